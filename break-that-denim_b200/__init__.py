@@ -1,0 +1,13 @@
+"""B200-native implicit cloth solve behind the reference's GpuSolver interface.
+
+The solve (projected Newton over the woven crossing lattice, Galerkin-multigrid-preconditioned PCG
+with exact yarn-line smoothers, line search, damage field and crossing slip) runs as CUDA kernels
+for sm_100a in libbtd.so; this package is the host-side mirror of the reference's
+`GpuSolver` (src/simulation/gpu/solver.ts) over the library's C ABI (include/btd.h).
+"""
+from . import _abi
+from .scene import (Scene, bundle_weave, compile_scene, default_spec, layer_spec, material_preset, SEG_BROKEN,
+                    SEG_EXISTS, SEG_INITIAL_DEFECT, SEG_SLIPPED)
+
+__all__ = ["Scene", "bundle_weave", "compile_scene", "default_spec", "layer_spec", "material_preset", "SEG_BROKEN",
+           "SEG_EXISTS", "SEG_INITIAL_DEFECT", "SEG_SLIPPED"]

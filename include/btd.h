@@ -1,0 +1,237 @@
+/*
+ * btd.h - C ABI of the B200-native implicit cloth solve.
+ *
+ * The solve replaces the reference's WebGPU `GpuSolver` (src/simulation/gpu/solver.ts:194-838):
+ * one projected-Newton substep over the woven crossing lattice, with the linear system solved by
+ * Galerkin-multigrid-preconditioned PCG whose smoother solves each yarn line exactly. Every entry
+ * point here corresponds to a member of `GpuSolver` (cited per function) or to the host-side scene
+ * compilation it is constructed from (`compileScene`, src/simulation/scene.ts:233-278).
+ *
+ * Conventions: every function returns 0 on success and a negative BTD_E* code on failure; no C++
+ * exception crosses this boundary. `btd_last_error` returns the message of the last failure on the
+ * calling thread. Arrays are plain host pointers with the sizes stated; positions and velocities are
+ * 4 floats per node (x, y, z, w), as the reference's vec4 buffers. A solver owns all its device
+ * memory and works on its own CUDA stream; one solver must not be used from two threads at once.
+ */
+#ifndef BTD_H
+#define BTD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BTD_OK 0
+#define BTD_E_INVALID (-1)     /* bad argument or unsupported size (the reference constructor throws) */
+#define BTD_E_CUDA (-2)        /* a CUDA call failed (device lost, out of memory, ...) */
+#define BTD_E_NO_DEVICE (-3)   /* no CUDA device: the library never falls back to the CPU */
+#define BTD_E_STATE (-4)       /* call out of order (e.g. a stage that needs an assembled system) */
+#define BTD_E_TIMEOUT (-5)     /* a bounded device-side wait ran out */
+
+/* ------------------------------------------------------------------------------------------------
+ * Scene description (src/simulation/material.ts:18-85, scene.ts:27-125)
+ * ---------------------------------------------------------------------------------------------- */
+
+/* YarnFamily (material.ts:18-54). yarns_per_span = 0 means "not bundled" (the field is absent). */
+typedef struct btd_yarn {
+  double linear_density, ea_low, ea_high, crimp_strain, ea_compress, axial_viscosity;
+  double bend_rigidity, bend_viscosity, strength, softening_opening, width, height, crimp_amplitude;
+  int32_t yarns_per_span;
+  int32_t pad_;
+} btd_yarn;
+
+/* WeaveMaterial (material.ts:56-85). */
+typedef struct btd_material {
+  int32_t id;
+  char name[60];
+  double pitch_u, pitch_v;
+  btd_yarn yarns[2];
+  int32_t twill_repeat, twill_warp_over;
+  double shear_stiffness, crossing_friction, crossing_normal0, crossing_wrap;
+  double thickness, cloth_friction, air_drag;
+} btd_material;
+
+/* WearSpec (scene.ts:27-46). */
+typedef struct btd_wear {
+  double center[2], axis[2], radii[2];
+  double amount, cell_size, feature_scale, defect_threshold, defect_density, sparse_from;
+} btd_wear;
+
+/* LayerSpec (scene.ts:48-71). bundle = {1, 1} when the reference leaves it undefined. */
+typedef struct btd_layer_spec {
+  btd_material material;
+  int32_t bundle[2];
+  double size_u, size_v, z, angle, compress_u, compress_v, shear;
+  int32_t collar_rows;
+  int32_t seed;
+  btd_wear wear;
+  double wear_strength_loss[2];
+  double perturbation;
+} btd_layer_spec;
+
+/* LayerInfo (scene.ts:73-89) plus its yarn-field layout (yarnField.ts:47-66). */
+typedef struct btd_layer_info {
+  int32_t index, nx, ny, node_offset, node_count;
+  int32_t bundle[2];
+  int32_t field_offset, field_k, field_m;
+  btd_material material; /* bundled (mechanical) */
+  btd_material weave;    /* individual yarns */
+  double map_a[4], map_origin[3], rest_center[2];
+} btd_layer_info;
+
+/*
+ * CompiledScene (scene.ts:91-125). N = node_count, C = crossing_count. Spans are indexed 2 n + f
+ * (f = 0: u-family span to (i + 1, j); f = 1: v-family span to (i, j + 1)); crossings 2 c + f.
+ * Either filled by btd_scene_compile (library-owned arrays, freed by btd_scene_free) or assembled
+ * by the caller over its own arrays.
+ */
+typedef struct btd_scene {
+  int32_t n_layers;
+  int32_t node_count;
+  int32_t crossing_count;
+  int32_t pad_;
+  btd_layer_info* layers;
+  double* rest_uv;          /* 2N */
+  double* position;         /* 3N */
+  double* mass;             /* N */
+  uint8_t* pinned;          /* N */
+  float* wear;              /* N */
+  float* structural_wear;   /* N */
+  double* rest_length;      /* 2N */
+  double* softening;        /* 2N */
+  uint16_t* seg_flags;      /* 2N: SEG_EXISTS 1, SEG_BROKEN 2, SEG_INITIAL_DEFECT 4, SEG_SLIPPED 8 */
+  double* intact;           /* 2N */
+  uint32_t* cut_mask;       /* 2N */
+  float* fail_site;         /* 2N */
+  float* field_strength;    /* 2C */
+  uint8_t* field_damage;    /* 2C */
+  uint8_t* field_area;      /* 2C */
+  double* crossing_normal0; /* N */
+  double* tails;            /* 4N */
+} btd_scene;
+
+/* compileScene (scene.ts:233-278): compile layer specs into a scene (host only, no GPU needed). */
+int btd_scene_compile(const btd_layer_spec* specs, int32_t n_specs, btd_scene** out);
+/* Free a scene returned by btd_scene_compile. */
+int btd_scene_free(btd_scene* scene);
+/* sceneHash (scene.ts:134-150): FNV-style content hash validating precomputed drapes. */
+int btd_scene_hash(const btd_scene* scene, uint32_t* out);
+/* The reference's materials DENIM / BACKING (material.ts:88-187); index 0 or 1. */
+int btd_material_preset(int32_t index, btd_material* out);
+/* bundleWeave (material.ts:198-226). */
+int btd_bundle_weave(const btd_material* m, int32_t bu, int32_t bv, btd_material* out);
+/* defaultSceneSpecs (scene.ts:438-469): the shipped 182 x 115 coupon. */
+int btd_default_scene_spec(btd_layer_spec* out);
+
+/* ------------------------------------------------------------------------------------------------
+ * Solver (GpuSolver, src/simulation/gpu/solver.ts:194-838)
+ * ---------------------------------------------------------------------------------------------- */
+
+/* GpuSolverParams (solver.ts:26-53) with the multigrid schedule (newtonMultigrid.ts:20-34). */
+typedef struct btd_params {
+  double h;
+  double gravity[3];
+  int32_t newton_iterations; /* always performed per substep */
+  int32_t newton_max;        /* gated upper bound (gate.wgsl) */
+  double newton_tolerance;   /* m, largest nodal update that ends the gated iterations */
+  double history_tolerance;  /* m, last update above which a node does not advance slip */
+  int32_t pcg_iterations;    /* PCG iterations (reference: a fixed count) or the cap with pcg_rel_tol */
+  int32_t coarse_sweeps;
+  int32_t max_coarsest_nodes;
+  int32_t self_contact;
+  double pcg_rel_tol;        /* extension: stop at ||r_k|| / ||r_0|| <= tol (0: fixed count) */
+  int32_t line_search;       /* choose the step among {1, 1/2, 1/4, 1/8} (energy.wgsl); 1 in the reference */
+  int32_t lag_coarse;        /* reuse the coarse levels after a substep's first Newton iteration; 1 */
+} btd_params;
+
+/* GPU_DEFAULTS (solver.ts:61-72). */
+int btd_default_params(btd_params* out);
+
+typedef struct btd_solver btd_solver;
+
+/* Counters (solver.ts:218-225): [0] ruptures, [1] pulled-out spans, [2] max speed (f32 bits),
+ * [3] line-search alpha (f32 bits), [4 + k] largest update of Newton iteration k (f32 bits),
+ * [12] rejected directions. Slots 16.. are solver statistics: [16] PCG iterations of the last
+ * Newton iteration, [17] PCG iterations summed since the last clear, [18] Newton iterations run,
+ * [19] relative residual of the last PCG solve (f32 bits), [20] device-side error flags. */
+#define BTD_COUNTERS 32
+
+/* GpuSolver constructor (solver.ts:275-385). Throws there on unsupported sizes; BTD_E_INVALID here. */
+int btd_create(const btd_scene* scene, const btd_params* params, btd_solver** out);
+int btd_destroy(btd_solver* s);
+
+/* encodeSubstep (solver.ts:737-760): predict, Newton iterations, commit, damage, slip. */
+int btd_substep(btd_solver* s, int32_t min_iterations, int32_t max_iterations);
+/* The engine's per-frame loop of substeps (worker.ts:664-674), stream-ordered, one launch each. */
+int btd_substeps(btd_solver* s, int32_t count);
+/* Wait for all submitted work (the reference's onSubmittedWorkDone). */
+int btd_synchronize(btd_solver* s);
+
+/* setState (solver.ts:833-837): positions (4 floats per node) and velocities (NULL: zero). */
+int btd_set_state(btd_solver* s, const float* position4, const float* velocity4);
+int btd_get_state(btd_solver* s, float* position4, float* velocity4);
+/* setSegments (solver.ts:821-824): per span rest length, intact fraction, cut mask, flags, fail
+ * site (2N each) and tails (4N). btd_get_segments reads them back (any pointer may be NULL). */
+int btd_set_segments(btd_solver* s, const float* rest_length, const float* intact, const uint32_t* cut_mask,
+                     const uint32_t* seg_flags, const float* fail_site, const float* tails);
+int btd_get_segments(btd_solver* s, float* rest_length, float* intact, uint32_t* cut_mask, uint32_t* seg_flags,
+                     float* fail_site, float* tails);
+/* setField (solver.ts:827-830): damage codes, 2 per crossing. */
+int btd_set_field(btd_solver* s, const uint8_t* damage);
+int btd_get_field(btd_solver* s, uint8_t* damage);
+/* resetState (solver.ts:810-818). */
+int btd_reset_state(btd_solver* s);
+
+/* setFloor (solver.ts:796-801): enabled = 0 removes the floor. */
+int btd_set_floor(btd_solver* s, int32_t enabled, float z);
+/* setTimestep (solver.ts:804-807). */
+int btd_set_timestep(btd_solver* s, float h);
+/* setHistoryEnabled (solver.ts:777-779). */
+int btd_set_history(btd_solver* s, int32_t enabled);
+/* setNewtonTolerance (solver.ts:782-785). */
+int btd_set_newton_tolerance(btd_solver* s, float tolerance);
+/* Extension: PCG cap and relative-residual stop (0 = fixed count as the reference). */
+int btd_set_pcg(btd_solver* s, int32_t max_iterations, double rel_tol);
+
+/* Counters (solver.ts:218-225); n <= BTD_COUNTERS. btd_clear_counters zeroes them. */
+int btd_read_counters(btd_solver* s, uint32_t* out, int32_t n);
+int btd_clear_counters(btd_solver* s);
+
+/* ---- stage encoders used by parity tests and profilers (solver.ts:574-728) ---- */
+int btd_stage_predict(btd_solver* s);                  /* encodePredict */
+int btd_stage_assemble(btd_solver* s, int32_t coarse); /* encodeAssemble(pass, coarse) */
+int btd_stage_vcycle(btd_solver* s);                   /* encodeVCycle(pass, 0): X0 = V(B0), X0 zeroed first */
+int btd_stage_pcg(btd_solver* s);                      /* encodePCG: delta = PCG(B0) */
+/* encodeLineSearch: energy changes e[4] and magnitude sums m[4] along delta, alpha chosen on device. */
+int btd_stage_linesearch(btd_solver* s, double* e4, double* m4);
+int btd_stage_apply(btd_solver* s, int32_t iteration); /* newtonApply */
+int btd_stage_newton(btd_solver* s, int32_t iteration);/* encodeNewtonIteration */
+int btd_stage_finalize(btd_solver* s);                 /* encodeFinalize: commit, damage, slip */
+int btd_stage_damage(btd_solver* s);                   /* encodeDamage */
+
+/* Multigrid levels (solver.ts:105-118, 333-352). */
+int btd_level_count(btd_solver* s, int32_t* out);
+int btd_level_nodes(btd_solver* s, int32_t level, int32_t* out);
+/* Operator of a level in the 25-offset layout of the CPU reference (newtonMultigrid.ts:38-48):
+ * N * 25 * 9 doubles, offset index (dj + 2) * 5 + (di + 2), row-major 3x3 blocks; fixed flags N. */
+int btd_read_operator(btd_solver* s, int32_t level, double* out, uint8_t* fixed);
+/* Vectors (4 floats per node): which = 0 X, 1 B, 2 R of a level; 3 delta, 4 dx, 5 pred, 6 ext (3 vec4/node). */
+#define BTD_VEC_X 0
+#define BTD_VEC_B 1
+#define BTD_VEC_R 2
+#define BTD_VEC_DELTA 3
+#define BTD_VEC_DX 4
+#define BTD_VEC_PRED 5
+int btd_read_vector(btd_solver* s, int32_t which, int32_t level, float* out4);
+int btd_write_vector(btd_solver* s, int32_t which, int32_t level, const float* in4);
+
+/* Last error message of the calling thread (always NUL-terminated when n > 0). */
+int btd_last_error(char* buf, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BTD_H */

@@ -1,0 +1,275 @@
+"""TEST INFRASTRUCTURE ONLY: Python binding of the FP64 oracle (oracle.cpp).
+
+The oracle restates the reference's own CPU solver (src/simulation/reference/solver.ts and
+newtonMultigrid.ts with laws.ts, axial.ts, lattice.ts, yarnField.ts) in C++. Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg use it, as the checker; the product never
+imports it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build():
+    """Compile liboracle.so with the committed Makefile (g++, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+class OraParams(C.Structure):
+    _fields_ = [
+        ("h", C.c_double),
+        ("gravity", C.c_double * 3),
+        ("newton_iterations", C.c_int32),
+        ("pcg_iterations", C.c_int32),
+        ("pcg_rel_tol", C.c_double),
+        ("max_coarsest_nodes", C.c_int32),
+        ("coarse_sweeps", C.c_int32),
+        ("line_colors", C.c_int32),
+        ("lag_coarse", C.c_int32),
+        ("line_search", C.c_int32),
+        ("threads", C.c_int32),
+    ]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        h = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        sig = {
+            "ora_create": ([vp, vp], vp),
+            "ora_destroy": ([vp], None),
+            "ora_last_error": ([], C.c_char_p),
+            "ora_potential": ([vp], C.c_double),
+            "ora_yarn_material_length": ([vp], C.c_double),
+            "ora_solve_penta": ([C.c_int32, vp, vp, vp, vp, vp, C.c_double], C.c_int),
+        }
+        for name, (a, r) in sig.items():
+            getattr(h, name).argtypes = a
+            getattr(h, name).restype = r
+        _lib = h
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _call(name, *args):
+    f = getattr(lib(), name)
+    rc = f(*args)
+    if isinstance(rc, int) and rc < 0:
+        raise RuntimeError(f"{name}: {lib().ora_last_error().decode()}")
+    return rc
+
+
+def solve_penta(D, E, F, r, shift=0.0):
+    """solvePenta (newtonMultigrid.ts:435-473) on (n, 3, 3) blocks."""
+    n = len(D)
+    x = np.zeros(3 * n)
+    _call("ora_solve_penta", n, _ptr(np.ascontiguousarray(D, np.float64)), _ptr(np.ascontiguousarray(E, np.float64)),
+          _ptr(np.ascontiguousarray(F, np.float64)), _ptr(np.ascontiguousarray(r, np.float64)), _ptr(x), C.c_double(shift))
+    return x.reshape(n, 3)
+
+
+class Oracle:
+    """ReferenceSolver (solver.ts(ref):41-749) with the multigrid of newtonMultigrid.ts.
+
+    Defaults follow the reference's own defaults (MG_DEFAULTS, no lag, no line search); pass the GPU
+    schedule explicitly to compare with the CUDA path.
+    """
+
+    def __init__(self, scene, h=1 / 240, gravity=(0, 0, -9.81), newton_iterations=2, pcg_iterations=4,
+                 pcg_rel_tol=0.0, max_coarsest_nodes=48, coarse_sweeps=6, line_colors=3, lag_coarse=False,
+                 line_search=False, threads=0):
+        p = OraParams()
+        p.h = h
+        p.gravity[0], p.gravity[1], p.gravity[2] = gravity
+        p.newton_iterations = newton_iterations
+        p.pcg_iterations = pcg_iterations
+        p.pcg_rel_tol = pcg_rel_tol
+        p.max_coarsest_nodes = max_coarsest_nodes
+        p.coarse_sweeps = coarse_sweeps
+        p.line_colors = line_colors
+        p.lag_coarse = int(lag_coarse)
+        p.line_search = int(line_search)
+        p.threads = threads
+        self.scene = scene
+        self.N = scene.N
+        self.params = p
+        self._h = _call("ora_create", C.byref(scene.c()), C.byref(p))
+        if not self._h:
+            raise RuntimeError(lib().ora_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ora_destroy(self._h)
+            self._h = None
+
+    # ---- state
+    def state(self):
+        n3 = 3 * self.N
+        x, v, dx, pred = (np.zeros(n3) for _ in range(4))
+        _call("ora_get_state", C.c_void_p(self._h), _ptr(x), _ptr(v), _ptr(dx), _ptr(pred))
+        return x.reshape(-1, 3), v.reshape(-1, 3), dx.reshape(-1, 3), pred.reshape(-1, 3)
+
+    @property
+    def x(self):
+        return self.state()[0]
+
+    @property
+    def v(self):
+        return self.state()[1]
+
+    def set_state(self, x, v=None):
+        x = np.ascontiguousarray(x, np.float64).reshape(-1)
+        v = None if v is None else np.ascontiguousarray(v, np.float64).reshape(-1)
+        _call("ora_set_state", C.c_void_p(self._h), _ptr(x), _ptr(v))
+
+    def set_dx(self, dx=None, pred=None):
+        dx = None if dx is None else np.ascontiguousarray(dx, np.float64).reshape(-1)
+        pred = None if pred is None else np.ascontiguousarray(pred, np.float64).reshape(-1)
+        _call("ora_set_dx", C.c_void_p(self._h), _ptr(dx), _ptr(pred))
+
+    def segments(self):
+        n2 = 2 * self.N
+        rest, intact, fail = np.zeros(n2), np.zeros(n2), np.zeros(n2)
+        cut = np.zeros(n2, np.uint32)
+        flags = np.zeros(n2, np.uint16)
+        tails = np.zeros(4 * self.N)
+        _call("ora_get_segments", C.c_void_p(self._h), _ptr(rest), _ptr(intact), _ptr(cut), _ptr(flags), _ptr(fail), _ptr(tails))
+        return dict(rest_length=rest, intact=intact, cut_mask=cut, seg_flags=flags, fail_site=fail, tails=tails)
+
+    def set_segments(self, rest_length=None, intact=None, cut_mask=None, seg_flags=None, fail_site=None, tails=None):
+        conv = lambda a, t: None if a is None else np.ascontiguousarray(a, t)
+        a = [conv(rest_length, np.float64), conv(intact, np.float64), conv(cut_mask, np.uint32),
+             conv(seg_flags, np.uint16), conv(fail_site, np.float64), conv(tails, np.float64)]
+        _call("ora_set_segments", C.c_void_p(self._h), *[_ptr(q) for q in a])
+
+    def field(self):
+        d = np.zeros(2 * self.scene.C, np.uint8)
+        _call("ora_get_field", C.c_void_p(self._h), _ptr(d))
+        return d
+
+    def set_field(self, damage):
+        _call("ora_set_field", C.c_void_p(self._h), _ptr(np.ascontiguousarray(damage, np.uint8)))
+
+    def set_history(self, on):
+        _call("ora_set_history", C.c_void_p(self._h), int(on))
+
+    def counts(self):
+        b, p = C.c_int32(), C.c_int32()
+        _call("ora_counts", C.c_void_p(self._h), C.byref(b), C.byref(p))
+        return b.value, p.value
+
+    # ---- grips and floor
+    def clear_grips(self):
+        _call("ora_clear_grips", C.c_void_p(self._h))
+
+    def add_grip(self, nodes, w, offset, goal, k):
+        nodes = np.ascontiguousarray(nodes, np.int32)
+        return _call("ora_add_grip", C.c_void_p(self._h), _ptr(nodes), _ptr(np.ascontiguousarray(w, np.float64)),
+                     _ptr(np.ascontiguousarray(offset, np.float64)), len(nodes), _ptr(np.ascontiguousarray(goal, np.float64)),
+                     C.c_double(k))
+
+    def set_grip_goal(self, grip, goal):
+        _call("ora_set_grip_goal", C.c_void_p(self._h), grip, _ptr(np.ascontiguousarray(goal, np.float64)))
+
+    def set_floor(self, z, bulge=0.3e-3, stiffness=1300.0, friction=0.35, friction_speed=0.002, enabled=True):
+        _call("ora_set_floor", C.c_void_p(self._h), int(enabled), C.c_double(z), C.c_double(bulge), C.c_double(stiffness),
+              C.c_double(friction), C.c_double(friction_speed))
+
+    # ---- stepping
+    def predict(self):
+        _call("ora_predict", C.c_void_p(self._h))
+
+    def newton_step(self):
+        m, rel, alpha = C.c_double(), C.c_double(), C.c_double()
+        it = C.c_int32()
+        _call("ora_newton_step", C.c_void_p(self._h), C.byref(m), C.byref(it), C.byref(rel), C.byref(alpha))
+        return dict(max_update=m.value, pcg_iterations=it.value, rel_residual=rel.value, alpha=alpha.value)
+
+    def finalize(self):
+        _call("ora_finalize", C.c_void_p(self._h))
+
+    def substep(self):
+        _call("ora_substep", C.c_void_p(self._h))
+
+    # ---- energies
+    def node_gradient(self, n):
+        g = np.zeros(3)
+        _call("ora_node_gradient", C.c_void_p(self._h), n, _ptr(g))
+        return g
+
+    def potential(self):
+        return lib().ora_potential(self._h)
+
+    def energy_change(self, d):
+        e, m = np.zeros(4), np.zeros(4)
+        _call("ora_energy_change", C.c_void_p(self._h), _ptr(np.ascontiguousarray(d, np.float64).reshape(-1)), _ptr(e), _ptr(m))
+        return e, m
+
+    def yarn_material_length(self):
+        return lib().ora_yarn_material_length(self._h)
+
+    # ---- multigrid stages
+    def assemble(self):
+        """(A (N, 25, 3, 3), fixed (N,), b (N, 3)) at the current iterate."""
+        A = np.zeros(self.N * 25 * 9)
+        fixed = np.zeros(self.N, np.uint8)
+        b = np.zeros(3 * self.N)
+        _call("ora_assemble", C.c_void_p(self._h), _ptr(A), _ptr(fixed), _ptr(b))
+        return A.reshape(self.N, 25, 3, 3), fixed, b.reshape(-1, 3)
+
+    def build_levels(self, A=None):
+        a = None if A is None else np.ascontiguousarray(A, np.float64).reshape(-1)
+        _call("ora_build_levels", C.c_void_p(self._h), _ptr(a))
+
+    def level_count(self):
+        return _call("ora_level_count", C.c_void_p(self._h))
+
+    def level(self, k):
+        n = _call("ora_level_nodes", C.c_void_p(self._h), k)
+        A = np.zeros(n * 25 * 9)
+        fixed = np.zeros(n, np.uint8)
+        _call("ora_read_level", C.c_void_p(self._h), k, _ptr(A), _ptr(fixed))
+        return A.reshape(n, 25, 3, 3), fixed
+
+    def prolongation(self, k):
+        n = _call("ora_level_nodes", C.c_void_p(self._h), k)
+        idx = np.zeros(4 * n, np.int32)
+        w = np.zeros(4 * n)
+        _call("ora_read_prolongation", C.c_void_p(self._h), k, _ptr(idx), _ptr(w))
+        return idx.reshape(n, 4), w.reshape(n, 4)
+
+    def apply(self, k, x):
+        x = np.ascontiguousarray(x, np.float64).reshape(-1)
+        y = np.zeros_like(x)
+        _call("ora_apply", C.c_void_p(self._h), k, _ptr(x), _ptr(y))
+        return y.reshape(-1, 3)
+
+    def smooth(self, k, x, b, reverse=False):
+        x = np.ascontiguousarray(x, np.float64).reshape(-1).copy()
+        _call("ora_smooth", C.c_void_p(self._h), k, _ptr(x), _ptr(np.ascontiguousarray(b, np.float64).reshape(-1)), int(reverse))
+        return x.reshape(-1, 3)
+
+    def vcycle(self, b):
+        b = np.ascontiguousarray(b, np.float64).reshape(-1)
+        z = np.zeros_like(b)
+        _call("ora_vcycle", C.c_void_p(self._h), _ptr(b), _ptr(z))
+        return z.reshape(-1, 3)
+
+    def pcg(self, b, iterations, rel_tol=0.0, x0=None):
+        b = np.ascontiguousarray(b, np.float64).reshape(-1)
+        x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, np.float64).reshape(-1).copy()
+        done, rel = C.c_int32(), C.c_double()
+        _call("ora_pcg", C.c_void_p(self._h), _ptr(b), _ptr(x), iterations, C.c_double(rel_tol), C.byref(done), C.byref(rel))
+        return x.reshape(-1, 3), done.value, rel.value

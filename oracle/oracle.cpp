@@ -1,0 +1,2070 @@
+// TEST INFRASTRUCTURE ONLY (see oracle.h): FP64 CPU restatement of the reference's solver. Each
+// function cites the reference file:line it restates; the reference is TypeScript, so this is a
+// restatement in C++ of its arithmetic, kept in the reference's operation order where that order
+// decides a branch.
+
+#include "oracle.h"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+constexpr double INF = std::numeric_limits<double>::infinity();
+
+double hyp3(double a, double b, double c) { return std::sqrt(a * a + b * b + c * c); }
+
+// ---------------------------------------------------------------------------- axial.ts
+
+struct Yarn {
+  double eaLow, eaHigh, crimpStrain, eaCompress, axialViscosity, bendRigidity, bendViscosity;
+  double softening;
+  int yarnsPerSpan;  // 1 when the reference leaves it undefined
+};
+
+// axialTension (axial.ts:16-22).
+double axialTension(const Yarn& p, double eps) {
+  if (eps <= 0) return p.eaCompress * eps;
+  double ec = p.crimpStrain, dk = p.eaHigh - p.eaLow;
+  if (eps <= ec) return p.eaLow * eps + (dk * eps * eps) / (2 * ec);
+  return p.eaLow * ec + (dk * ec) / 2 + p.eaHigh * (eps - ec);
+}
+// axialStiffness (axial.ts:25-30).
+double axialStiffness(const Yarn& p, double eps) {
+  if (eps <= 0) return p.eaCompress;
+  double ec = p.crimpStrain;
+  if (eps <= ec) return p.eaLow + ((p.eaHigh - p.eaLow) * eps) / ec;
+  return p.eaHigh;
+}
+// axialEnergyDensity (axial.ts:33-42).
+double axialEnergyDensity(const Yarn& p, double eps) {
+  if (eps <= 0) return 0.5 * p.eaCompress * eps * eps;
+  double ec = p.crimpStrain, dk = p.eaHigh - p.eaLow;
+  if (eps <= ec) return 0.5 * p.eaLow * eps * eps + (dk * eps * eps * eps) / (6 * ec);
+  double tc = p.eaLow * ec + (dk * ec) / 2;
+  double ecEnergy = 0.5 * p.eaLow * ec * ec + (dk * ec * ec) / 6;
+  double d = eps - ec;
+  return ecEnergy + tc * d + 0.5 * p.eaHigh * d * d;
+}
+// strainAtTension (axial.ts:45-53).
+double strainAtTension(const Yarn& p, double t) {
+  double ec = p.crimpStrain, dk = p.eaHigh - p.eaLow;
+  double tc = p.eaLow * ec + (dk * ec) / 2;
+  if (t >= tc) return ec + (t - tc) / p.eaHigh;
+  double a = dk / (2 * ec);
+  return (2 * t) / (p.eaLow + std::sqrt(p.eaLow * p.eaLow + 4 * a * t));
+}
+// yarnDamage (axial.ts:63-70).
+double yarnDamage(const Yarn& p, double yarns, double area, double peakYarn, double softStrain, double eps) {
+  double ep = strainAtTension(p, (peakYarn * yarns) / area);
+  if (eps <= ep) return 0;
+  if (eps >= ep + softStrain) return 1;
+  double tEnv = peakYarn * (1 - (eps - ep) / softStrain);
+  double tEl = (area * axialTension(p, eps)) / yarns;
+  return std::min(1.0, std::max(0.0, 1 - tEnv / std::max(tEl, 1e-12)));
+}
+
+// ---------------------------------------------------------------------------- laws.ts
+
+constexpr double BEND_S0 = 0.85;
+// bendPsi (laws.ts:17-30): [Psi, Psi', Psi''].
+void bendPsi(double q, double a, double* out) {
+  double s = q / a;
+  if (s < BEND_S0) {
+    double d = 1 - s;
+    out[0] = q / d;
+    out[1] = 1 / (d * d);
+    out[2] = 2 / (a * d * d * d);
+    return;
+  }
+  double d0 = 1 - BEND_S0, q0 = BEND_S0 * a;
+  double p1 = 1 / (d0 * d0), p2 = 2 / (a * d0 * d0 * d0);
+  double t = q - q0;
+  out[0] = q0 / d0 + p1 * t + 0.5 * p2 * t * t;
+  out[1] = p1 + p2 * t;
+  out[2] = p2;
+}
+struct BendGeometry {
+  double wa, wc, kPerB, fold;
+};
+// bendGeometry (laws.ts:54-58).
+BendGeometry bendGeometry(double La, double Lc) {
+  double s = La + Lc;
+  double lh = (2 * La * Lc) / s;
+  return {(2 * Lc) / s, (2 * La) / s, 1 / (lh * lh * 0.5 * s), 4 * lh * lh};
+}
+int popcount32(uint32_t v) { return __builtin_popcount(v); }
+// bendScale (laws.ts:67-74).
+double bendScale(double ia, double ic, uint32_t maskA, uint32_t maskC, int B) {
+  uint32_t full = B >= 32 ? 0xffffffffu : ((1u << B) - 1u);
+  int cont = popcount32(~(maskA | maskC) & full);
+  if (cont == 0) return 0;
+  int ua = popcount32(~maskA & full), uc = popcount32(~maskC & full);
+  return (static_cast<double>(cont) / B) * std::min(ua > 0 ? (ia * B) / ua : 0.0, uc > 0 ? (ic * B) / uc : 0.0);
+}
+// bendPsiDelta (laws.ts:89-103).
+double bendPsiDelta(double q0, double q1, double dq, double a) {
+  double s0 = q0 / a, s1 = q1 / a;
+  if (s0 < BEND_S0 && s1 < BEND_S0) return dq / ((1 - s0) * (1 - s1));
+  double qb = BEND_S0 * a, d0 = 1 - BEND_S0;
+  double p1 = 1 / (d0 * d0), p2 = 2 / (a * d0 * d0 * d0);
+  if (s0 >= BEND_S0 && s1 >= BEND_S0) return dq * (p1 + 0.5 * p2 * (q0 - qb + (q1 - qb)));
+  double lo = std::min(q0, q1);
+  double t = std::max(q0, q1) - qb;
+  double up = (qb - lo) / ((1 - lo / a) * d0) + t * (p1 + 0.5 * p2 * t);
+  return q1 >= q0 ? up : -up;
+}
+constexpr double SHEAR_JAM = 0.16, SHEAR_RAMP = 0.08, SHEAR_LOCK = 40;
+const double SHEAR_COS0 = std::sqrt(1 - std::pow(1 - (1 - SHEAR_JAM) * (1 - SHEAR_JAM), 2));
+// shearJam (laws.ts:126-129).
+double shearJam(double area) {
+  double c = SHEAR_COS0 * std::sqrt(std::min(1.0, std::max(0.02, area)));
+  return 1 - std::sqrt(1 - std::sqrt(1 - c * c));
+}
+double cellArea(double cu, double tu, double cv, double rv) { return std::max(0.5 * (cu + tu), 0.5 * (cv + rv)); }
+// shearLaw (laws.ts:140-159): [force, tangent, energy].
+void shearLaw(double ks, double Ld, double l, double jam, double* out) {
+  double d = l - Ld;
+  double f = ks * d, k = ks, e = 0.5 * ks * d * d;
+  double c = -d / Ld - jam;
+  if (c > 0) {
+    double extra = ks * (SHEAR_LOCK - 1);
+    if (c < SHEAR_RAMP) {
+      f -= (extra * Ld * c * c) / (2 * SHEAR_RAMP);
+      k += (extra * c) / SHEAR_RAMP;
+      e += (extra * Ld * Ld * c * c * c) / (6 * SHEAR_RAMP);
+    } else {
+      f -= extra * Ld * (c - 0.5 * SHEAR_RAMP);
+      k += extra;
+      e += extra * Ld * Ld *
+           ((SHEAR_RAMP * SHEAR_RAMP) / 6 + 0.5 * (c - SHEAR_RAMP) * (c - SHEAR_RAMP) + 0.5 * SHEAR_RAMP * (c - SHEAR_RAMP));
+    }
+  }
+  out[0] = f;
+  out[1] = k;
+  out[2] = e;
+}
+
+// ---------------------------------------------------------------------------- lattice.ts
+
+struct LatticeLayer {
+  int nx, ny, offset;
+};
+int coarseCount(int n) { return (n - 1 + 1) / 2 + 1; }  // Math.ceil((n - 1) / 2) + 1
+int coarseToFine(int I, int n) { return std::min(2 * I, n - 1); }
+// bracket (lattice.ts:30-41): up to two (coarse index, weight).
+int bracket(int i, int n, int* idx, double* w) {
+  int nc = coarseCount(n);
+  int lo = std::min(nc - 1, i >> 1);
+  if (coarseToFine(lo, n) > i) lo--;
+  int a = coarseToFine(lo, n);
+  if (a == i) {
+    idx[0] = lo;
+    w[0] = 1;
+    return 1;
+  }
+  int b = coarseToFine(lo + 1, n);
+  idx[0] = lo;
+  w[0] = static_cast<double>(b - i) / (b - a);
+  idx[1] = lo + 1;
+  w[1] = static_cast<double>(i - a) / (b - a);
+  return 2;
+}
+std::vector<LatticeLayer> coarsenLayers(const std::vector<LatticeLayer>& fine) {
+  std::vector<LatticeLayer> out;
+  int off = 0;
+  for (auto& L : fine) {
+    LatticeLayer C{coarseCount(L.nx), coarseCount(L.ny), off};
+    off += C.nx * C.ny;
+    out.push_back(C);
+  }
+  return out;
+}
+bool shouldCoarsen(const std::vector<LatticeLayer>& layers, int minNodes = 48) {
+  for (auto& L : layers)
+    if (!(L.nx * L.ny > minNodes && L.nx >= 5 && L.ny >= 5)) return false;
+  return true;
+}
+
+// ---------------------------------------------------------------------------- newtonMultigrid.ts
+
+constexpr int STENCIL = 25, CENTER = 12;
+int offsetIndex(int di, int dj) { return (dj + 2) * 5 + (di + 2); }
+
+struct Solver;
+
+// StencilOperator (newtonMultigrid.ts:44-125).
+struct StencilOperator {
+  int N = 0;
+  std::vector<LatticeLayer> layers;
+  std::vector<double> A;
+  std::vector<uint8_t> fixed;
+  std::vector<int> ij;
+  const Solver* linkSolver = nullptr;  // fine lattice: connectivity from the spans (A.link)
+  explicit StencilOperator(const std::vector<LatticeLayer>& L) : layers(L) {
+    for (auto& l : L) N += l.nx * l.ny;
+    A.assign(static_cast<size_t>(N) * STENCIL * 9, 0.0);
+    fixed.assign(N, 0);
+    ij.assign(3 * static_cast<size_t>(N), 0);
+    for (size_t l = 0; l < L.size(); ++l)
+      for (int j = 0; j < L[l].ny; ++j)
+        for (int i = 0; i < L[l].nx; ++i) {
+          int n = L[l].offset + j * L[l].nx + i;
+          ij[3 * n] = i;
+          ij[3 * n + 1] = j;
+          ij[3 * n + 2] = static_cast<int>(l);
+        }
+  }
+  int nbr(int n, int di, int dj) const {
+    int i = ij[3 * n] + di, j = ij[3 * n + 1] + dj;
+    const LatticeLayer& L = layers[ij[3 * n + 2]];
+    if (i < 0 || j < 0 || i >= L.nx || j >= L.ny) return -1;
+    return L.offset + j * L.nx + i;
+  }
+  void addBlock(int row, int o, double s, const double* B) {
+    double* p = &A[(static_cast<size_t>(row) * STENCIL + o) * 9];
+    for (int q = 0; q < 9; ++q) p[q] += s * B[q];
+  }
+  // y = A x, fixed rows give y = x (newtonMultigrid.ts:95-124).
+  void apply(const double* x, double* y) const {
+#pragma omp parallel for schedule(static)
+    for (int n = 0; n < N; ++n) {
+      if (fixed[n]) {
+        y[3 * n] = x[3 * n];
+        y[3 * n + 1] = x[3 * n + 1];
+        y[3 * n + 2] = x[3 * n + 2];
+        continue;
+      }
+      double a0 = 0, a1 = 0, a2 = 0;
+      for (int dj = -2; dj <= 2; ++dj)
+        for (int di = -2; di <= 2; ++di) {
+          int m = nbr(n, di, dj);
+          if (m < 0 || fixed[m]) continue;
+          const double* b = &A[(static_cast<size_t>(n) * STENCIL + offsetIndex(di, dj)) * 9];
+          double x0 = x[3 * m], x1 = x[3 * m + 1], x2 = x[3 * m + 2];
+          a0 += b[0] * x0 + b[1] * x1 + b[2] * x2;
+          a1 += b[3] * x0 + b[4] * x1 + b[5] * x2;
+          a2 += b[6] * x0 + b[7] * x1 + b[8] * x2;
+        }
+      y[3 * n] = a0;
+      y[3 * n + 1] = a1;
+      y[3 * n + 2] = a2;
+    }
+  }
+};
+
+struct Prolongation {
+  std::vector<int> idx;
+  std::vector<double> w;
+};
+struct MGLevel {
+  std::shared_ptr<StencilOperator> A;
+  std::shared_ptr<Prolongation> P;
+};
+
+constexpr double LINK_MIN_INTACT = 0.02;
+constexpr double PIVOT_SHIFT = 2e-6;
+const double LINE_ALPHAS[4] = {1, 0.5, 0.25, 0.125};
+constexpr double LINE_NOISE = 4e-6;
+
+// ---------------------------------------------------------------------------- yarnField.ts
+
+constexpr int DAMAGE_CUT = 255, DAMAGE_PULLED = 254, DAMAGE_SEPARATED = 254;
+constexpr int RECOIL_MAX = 12;
+constexpr double SHARE_FRACTION = 0.6, SHARE_REACH = 1.2e-3;
+constexpr int SHARE_MAXRUN = 6;
+constexpr uint16_t SEG_EXISTS = 1, SEG_BROKEN = 2, SEG_SLIPPED = 8;
+
+struct Layer {
+  int index, nx, ny, nodeOffset;
+  int fOffset, K, M, bu, bv;  // FieldLayer
+  Yarn yarns[2];
+  double pitchU, pitchV, weavePitchU, weavePitchV;
+  double shearStiffness, crossingFriction, crossingNormal0, crossingWrap, airDrag, thickness;
+};
+
+int bundleOf(const Layer& fl, int f) { return f == 1 ? fl.bu : fl.bv; }
+int spanLength(const Layer& fl, int f) { return f == 1 ? fl.bv : fl.bu; }
+double areaOf(int code) { return std::max(0.02, code / 255.0); }
+int damageCode(double d) { return d >= 1 ? DAMAGE_CUT : std::min(DAMAGE_PULLED - 1, static_cast<int>(std::floor(d * DAMAGE_CUT))); }
+
+// recoilLength (yarnField.ts:109-115).
+double recoilLength(const Yarn& y, double B, double area, double peak, double eps, double mu, double n0, double wrap,
+                    double tCross, double pitch) {
+  if (!(eps > 0)) return 0;
+  double share = area / B;
+  double e = std::min(eps, strainAtTension(y, peak / share));
+  double comp = share * (axialTension(y, e) * e - axialEnergyDensity(y, e));
+  return (comp * pitch) / (mu * (n0 + wrap * std::max(0.0, tCross)));
+}
+// breakDistance (yarnField.ts:158-177).
+int breakDistance(const Layer& fl, const uint8_t* damage, int f, int k, int m) {
+  int pos = f == 0 ? k : m, len = f == 0 ? fl.K : fl.M, stride = f == 0 ? 1 : fl.K;
+  int c = fl.fOffset + m * fl.K + k;
+  int best = -1;
+  for (int dir = -1; dir <= 1; dir += 2) {
+    for (int d = 1; d <= RECOIL_MAX; ++d) {
+      int p = pos + dir * d;
+      if (p < 0 || p >= len) break;
+      int code = damage[2 * (c + dir * d * stride) + f];
+      if (code == DAMAGE_CUT) {
+        if (best < 0 || d < best) best = d;
+        break;
+      }
+      if (code != DAMAGE_PULLED) break;
+    }
+  }
+  return best;
+}
+int nodeOfCrossing(const Layer& L, int k, int m) {
+  int i = std::min(L.nx - 1, k / L.bu), j = std::min(L.ny - 1, m / L.bv);
+  return L.nodeOffset + j * L.nx + i;
+}
+// spanCrossing (yarnField.ts:201-204).
+int spanCrossing(const Layer& fl, int i, int j, int f, int q, int p) {
+  if (f == 1) return fl.fOffset + (j * fl.bv + fl.bv / 2 + p) * fl.K + i * fl.bu + q;
+  return fl.fOffset + (j * fl.bv + q) * fl.K + i * fl.bu + fl.bu / 2 + p;
+}
+// interpolatedStrain (yarnField.ts:216-240).
+double interpolatedStrain(const Layer& L, int f, int k, int m, const double* strain) {
+  double s = f == 1 ? (k - (L.bu - 1) / 2.0) / L.bu : (k - (L.bu - 0.5)) / L.bu;
+  double t = f == 1 ? (m - (L.bv - 0.5)) / L.bv : (m - (L.bv - 1) / 2.0) / L.bv;
+  int i0 = static_cast<int>(std::floor(s)), j0 = static_cast<int>(std::floor(t));
+  double fu = s - i0, fv = t - j0;
+  int imax = f == 1 ? L.nx - 1 : L.nx - 2;
+  int jmax = f == 1 ? L.ny - 2 : L.ny - 1;
+  double num = 0, den = 0;
+  for (int dj = 0; dj < 2; ++dj)
+    for (int di = 0; di < 2; ++di) {
+      int i = i0 + di, j = j0 + dj;
+      if (i < 0 || j < 0 || i > imax || j > jmax) continue;
+      double e = strain[2 * (L.nodeOffset + j * L.nx + i) + f];
+      if (!std::isfinite(e)) continue;
+      double w = (di ? fu : 1 - fu) * (dj ? fv : 1 - fv);
+      num += w * e;
+      den += w;
+    }
+  return den > 1e-6 ? num / den : NAN;
+}
+int shareReach(const Layer& L, int f) {
+  return std::max(1, static_cast<int>(std::round(SHARE_REACH / (f == 1 ? L.weavePitchV : L.weavePitchU))));
+}
+double shareCap(int reach, double mu, double n0, double wrap, double tCross, double peak) {
+  return ((2 * reach + 1) * mu * (n0 + wrap * tCross)) / peak;
+}
+// shareFactor (yarnField.ts:303-321).
+double shareFactor(const Layer& fl, const uint8_t* sep, int f, int k, int m, int reach, double cap) {
+  int along = f == 1 ? m : k, lenAlong = f == 1 ? fl.M : fl.K;
+  int across = f == 1 ? k : m, lenAcross = f == 1 ? fl.K : fl.M;
+  auto at = [&](int y, int a) { return fl.fOffset + (f == 1 ? a * fl.K + y : y * fl.K + a); };
+  int runs = 0;
+  for (int dir = -1; dir <= 1; dir += 2) {
+    for (int d = 1; d <= SHARE_MAXRUN; ++d) {
+      int y = across + dir * d;
+      if (y < 0 || y >= lenAcross) break;
+      bool broken = false;
+      for (int a = std::max(0, along - reach); a <= std::min(lenAlong - 1, along + reach) && !broken; ++a)
+        broken = sep[2 * at(y, a) + f] == 1;
+      if (!broken) break;
+      runs++;
+    }
+  }
+  return 1 + std::min((SHARE_FRACTION * runs) / 2, cap);
+}
+// partSpanYarns (yarnField.ts:422-434).
+void partSpanYarns(const Layer& fl, uint8_t* damage, int i, int j, int f, int slipEnd) {
+  int P = spanLength(fl, f), half = P - P / 2;
+  for (int q = 0; q < bundleOf(fl, f); ++q) {
+    bool ofA = slipEnd != 0;
+    for (int p = 0; p < P; ++p) {
+      int e = 2 * spanCrossing(fl, i, j, f, q, p) + f;
+      if (damage[e] >= DAMAGE_SEPARATED) {
+        if (slipEnd < 0) ofA = false;
+      } else if (ofA != (p < half)) {
+        damage[e] = DAMAGE_PULLED;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------- solver.ts (reference)
+
+struct Grip {
+  std::vector<int> nodes;
+  std::vector<double> w, offset;
+  double goal[3];
+  double k;
+};
+
+struct FloorParams {
+  bool on = false;
+  double z = 0, bulge = 0.3e-3, stiffness = 1300, friction = 0.35, frictionSpeed = 0.002;
+};
+
+struct Solver {
+  ora_params prm;
+  int N = 0, C = 0;
+  std::vector<Layer> layers;
+  std::vector<double> mass, crossingNormal0, softening;
+  std::vector<uint8_t> pinned;
+  std::vector<float> fieldStrength;
+  std::vector<uint8_t> fieldArea;
+  std::vector<double> x, v, dx, pred, restLength, intact, failSite, strain, tails, lastUpdate;
+  std::vector<uint32_t> cutMask;
+  std::vector<uint16_t> segFlags;
+  std::vector<uint8_t> fieldDamage;
+  std::vector<int> nbr;
+  std::vector<int> layerOf;
+  std::vector<Grip> grips;
+  std::vector<std::vector<std::pair<int, int>>> gripOf;  // per node: (grip, entry)
+  FloorParams floor;
+  bool historyEnabled = true;
+  int brokenCount = 0, pulledOutCount = 0;
+  std::vector<MGLevel> lagged;      // lagged coarse levels (newtonMultigrid.ts:579)
+  std::vector<MGLevel> stageLevels; // levels built by ora_build_levels / the last Newton step
+
+  const Layer& layer(int n) const { return layers[layerOf[n]]; }
+  int seg(int n, int f, int dir) const {
+    if (dir > 0) return nbr[4 * n + 2 * f + 1] >= 0 ? 2 * n + f : -1;
+    int p = nbr[4 * n + 2 * f];
+    return p >= 0 ? 2 * p + f : -1;
+  }
+  bool segActive(int s) const { return s >= 0 && (segFlags[s] & (SEG_EXISTS | SEG_BROKEN)) == SEG_EXISTS; }
+  int segOther(int s) const { return nbr[4 * (s >> 1) + 2 * (s & 1) + 1]; }
+
+  // diagActive (solver.ts(ref):232-241).
+  bool diagActive(int c, int d) const {
+    int r = nbr[4 * c + 1], t = nbr[4 * c + 3];
+    if (r < 0 || t < 0) return false;
+    bool cu = segActive(2 * c), cv = segActive(2 * c + 1), rv = segActive(2 * r + 1), tu = segActive(2 * t);
+    return d == 0 ? (cu && rv) || (cv && tu) : (cu && cv) || (rv && tu);
+  }
+
+  // airDrag (solver.ts(ref):132-165): row-major 3x3.
+  void airDrag(int n, double* D) const {
+    std::fill(D, D + 9, 0.0);
+    const Layer& m = layer(n);
+    if (!(m.airDrag > 0)) return;
+    double k = (m.airDrag * m.pitchU * m.pitchV) / prm.h;
+    auto tangent = [&](int f, double* t) {
+      int a = n, b = n;
+      if (segActive(seg(n, f, -1))) a = nbr[4 * n + 2 * f];
+      if (segActive(seg(n, f, 1))) b = nbr[4 * n + 2 * f + 1];
+      for (int q = 0; q < 3; ++q) t[q] = x[3 * b + q] - x[3 * a + q];
+    };
+    double tu[3], tv[3];
+    tangent(0, tu);
+    tangent(1, tv);
+    double lu = hyp3(tu[0], tu[1], tu[2]), lv = hyp3(tv[0], tv[1], tv[2]);
+    auto outer = [&](const double* e, double kPar, double kPerp) {
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) D[3 * r + c] = (kPar - kPerp) * e[r] * e[c] + (r == c ? kPerp : 0);
+    };
+    if (lu > 0 && lv > 0) {
+      double c[3] = {tu[1] * tv[2] - tu[2] * tv[1], tu[2] * tv[0] - tu[0] * tv[2], tu[0] * tv[1] - tu[1] * tv[0]};
+      double lc = hyp3(c[0], c[1], c[2]);
+      if (lc > 1e-3 * lu * lv) {
+        double e[3] = {c[0] / lc, c[1] / lc, c[2] / lc};
+        outer(e, k, 0);
+        return;
+      }
+    }
+    if (lu > 0 || lv > 0) {
+      double t[3];
+      for (int q = 0; q < 3; ++q) t[q] = lu >= lv ? tu[q] / lu : tv[q] / lv;
+      outer(t, 0, k);
+      return;
+    }
+    double e[3] = {1, 0, 0};
+    outer(e, k, k);
+  }
+  static void dragMul(const double* D, const double* v, double* o) {
+    o[0] = D[0] * v[0] + D[1] * v[1] + D[2] * v[2];
+    o[1] = D[3] * v[0] + D[4] * v[1] + D[5] * v[2];
+    o[2] = D[6] * v[0] + D[7] * v[1] + D[8] * v[2];
+  }
+
+  // gripTerm (solver.ts(ref):173-180), summed over every grip holding the node.
+  double gripTerm(int n, double* g) const {
+    double ktot = 0;
+    for (auto& ge : gripOf[n]) {
+      const Grip& G = grips[ge.first];
+      int k = ge.second;
+      double kg = G.k * G.w[k];
+      for (int q = 0; q < 3; ++q) g[q] += kg * (x[3 * n + q] + dx[3 * n + q] - (G.goal[q] + G.offset[3 * k + q]));
+      ktot += kg;
+    }
+    return ktot;
+  }
+  double gripEnergy(int n) const {
+    double E = 0;
+    for (auto& ge : gripOf[n]) {
+      const Grip& G = grips[ge.first];
+      int k = ge.second;
+      double l2 = 0;
+      for (int q = 0; q < 3; ++q) {
+        double d = x[3 * n + q] + dx[3 * n + q] - (G.goal[q] + G.offset[3 * k + q]);
+        l2 += d * d;
+      }
+      E += 0.5 * G.k * G.w[k] * l2;
+    }
+    return E;
+  }
+
+  // response (solver.ts(ref):641-644) = spanResponse (axial.ts:78-80).
+  void response(int s, double eps, double* T, double* K) const {
+    const Yarn& y = layer(s >> 1).yarns[s & 1];
+    *T = intact[s] * axialTension(y, eps);
+    *K = intact[s] * axialStiffness(y, eps);
+  }
+
+  // segForce (solver.ts(ref):254-277): [fs, kPar, kPerp, l], e = unit vector owner -> far end.
+  void segForce(int s, double* out, double* e) const {
+    int a = s >> 1, f = s & 1, b = segOther(s);
+    double en[3], ee[3];
+    for (int q = 0; q < 3; ++q) {
+      en[q] = x[3 * b + q] - x[3 * a + q];
+      ee[q] = en[q] + (dx[3 * b + q] - dx[3 * a + q]);
+    }
+    double l = hyp3(ee[0], ee[1], ee[2]), ln = hyp3(en[0], en[1], en[2]);
+    for (int q = 0; q < 3; ++q) e[q] = ee[q] / l;
+    double L = restLength[s];
+    const Yarn& y = layer(a).yarns[f];
+    double T, K;
+    response(s, l / L - 1, &T, &K);
+    double c = y.axialViscosity / (L * prm.h);
+    double fs = T + c * (l - ln);
+    out[0] = fs;
+    out[1] = std::max(K, 0.0) / L + c;
+    out[2] = std::max(fs, 0.0) / l;
+    out[3] = l;
+  }
+
+  // bendCoeffs (solver.ts(ref):284-291): [kb, kd, fold, wa, wc].
+  void bendCoeffs(int b, int f, int s0, int s1, double* o) const {
+    const Yarn& y = layer(b).yarns[f];
+    BendGeometry geo = bendGeometry(restLength[s0], restLength[s1]);
+    double scale = bendScale(intact[s0], intact[s1], cutMask[s0], cutMask[s1], y.yarnsPerSpan);
+    double kb = y.bendRigidity * scale * geo.kPerB;
+    o[0] = kb;
+    o[1] = (kb * y.bendViscosity) / prm.h;
+    o[2] = geo.fold;
+    o[3] = geo.wa;
+    o[4] = geo.wc;
+  }
+  // triple (solver.ts(ref):311-316).
+  void triple(int a, int b, int c, double wa, double wc, double* r, double* rn) const {
+    for (int k = 0; k < 3; ++k) {
+      rn[k] = wa * x[3 * a + k] - 2 * x[3 * b + k] + wc * x[3 * c + k];
+      r[k] = rn[k] + wa * dx[3 * a + k] - 2 * dx[3 * b + k] + wc * dx[3 * c + k];
+    }
+  }
+  // bendGradCoeff + bendViscCoeff (solver.ts(ref):294-308).
+  static double bendCoeffSum(double kb, double kd, double fold, const double* r, const double* rn) {
+    double ps[3];
+    bendPsi(r[0] * r[0] + r[1] * r[1] + r[2] * r[2], fold, ps);
+    double ke = kb * ps[1];
+    double lr = hyp3(r[0], r[1], r[2]);
+    return ke + (kd * (lr - hyp3(rn[0], rn[1], rn[2]))) / std::max(lr, 1e-12);
+  }
+  // addBendingGradient (solver.ts(ref):319-352).
+  void addBendingGradient(int n, int f, double* g) const {
+    int prev = nbr[4 * n + 2 * f], nxt = nbr[4 * n + 2 * f + 1];
+    int sPrev = prev >= 0 ? 2 * prev + f : -1, sNext = nxt >= 0 ? 2 * n + f : -1;
+    double c[5], r[3], rn[3];
+    if (segActive(sPrev) && segActive(sNext)) {
+      bendCoeffs(n, f, sPrev, sNext, c);
+      triple(prev, n, nxt, c[3], c[4], r, rn);
+      double kv = bendCoeffSum(c[0], c[1], c[2], r, rn);
+      for (int k = 0; k < 3; ++k) g[k] += -2 * kv * r[k];
+    }
+    if (segActive(sNext)) {
+      int nxt2 = nbr[4 * nxt + 2 * f + 1];
+      int sNext2 = nxt2 >= 0 ? 2 * nxt + f : -1;
+      if (segActive(sNext2)) {
+        bendCoeffs(nxt, f, sNext, sNext2, c);
+        triple(n, nxt, nxt2, c[3], c[4], r, rn);
+        double kv = bendCoeffSum(c[0], c[1], c[2], r, rn);
+        for (int k = 0; k < 3; ++k) g[k] += c[3] * kv * r[k];
+      }
+    }
+    if (segActive(sPrev)) {
+      int prev2 = nbr[4 * prev + 2 * f];
+      int sPrev2 = prev2 >= 0 ? 2 * prev2 + f : -1;
+      if (segActive(sPrev2)) {
+        bendCoeffs(prev, f, sPrev2, sPrev, c);
+        triple(prev2, prev, n, c[3], c[4], r, rn);
+        double kv = bendCoeffSum(c[0], c[1], c[2], r, rn);
+        for (int k = 0; k < 3; ++k) g[k] += c[4] * kv * r[k];
+      }
+    }
+  }
+
+  // cellShear (solver.ts(ref):374-380): [ks, jam].
+  void cellShear(int cell, double* ks, double* jam) const {
+    int r = nbr[4 * cell + 1], t = nbr[4 * cell + 3];
+    auto io = [&](int s) { return segActive(s) ? intact[s] : 0.0; };
+    const Layer& m = layer(cell);
+    *ks = (m.shearStiffness * crossingNormal0[cell]) / m.crossingNormal0;
+    *jam = shearJam(cellArea(io(2 * cell), io(2 * t), io(2 * cell + 1), io(2 * r + 1)));
+  }
+  double shearRest(int cell) const {
+    double a = restLength[2 * cell], b = restLength[2 * cell + 1];
+    return std::sqrt(a * a + b * b);
+  }
+
+  // Floor terms of a node at its iterate (assemble.wgsl:191-209): gradient, diagonal Hessian,
+  // whether the node sits at the hard limit.
+  bool floorTerm(int n, double* g, double* H, bool* core) const {
+    *core = false;
+    if (!floor.on) return false;
+    double half = 0.5 * layer(n).thickness;
+    double delta = half + floor.bulge;
+    double zc = x[3 * n + 2] + dx[3 * n + 2];
+    double s = delta - (zc - floor.z);
+    if (!(s > 0)) return false;
+    double kc = floor.stiffness;
+    double lam = kc * s * s / delta;
+    double ut0 = dx[3 * n], ut1 = dx[3 * n + 1];
+    double kf = floor.friction * lam / std::max(std::sqrt(ut0 * ut0 + ut1 * ut1), floor.frictionSpeed * prm.h);
+    g[0] += kf * ut0;
+    g[1] += kf * ut1;
+    g[2] += -lam;
+    H[0] = kf;
+    H[1] = kf;
+    H[2] = 2 * kc * s / delta;
+    *core = zc <= floor.z + half * (1 + 1e-3);
+    return true;
+  }
+
+  // nodeGradient (solver.ts(ref):387-422).
+  void nodeGradient(int n, double* g) const {
+    g[0] = g[1] = g[2] = 0;
+    if (pinned[n]) return;
+    double h = prm.h;
+    double w = mass[n] / (h * h);
+    for (int q = 0; q < 3; ++q) g[q] += w * (dx[3 * n + q] - pred[3 * n + q]);
+    gripTerm(n, g);
+    double D[9], Dg[3];
+    airDrag(n, D);
+    dragMul(D, &dx[3 * n], Dg);
+    for (int q = 0; q < 3; ++q) g[q] += Dg[q];
+    double Hf[3];
+    bool core;
+    floorTerm(n, g, Hf, &core);
+    double sf[4], e[3];
+    for (int f = 0; f < 2; ++f) {
+      int sPrev = seg(n, f, -1), sNext = seg(n, f, 1);
+      if (segActive(sPrev)) {
+        segForce(sPrev, sf, e);
+        for (int q = 0; q < 3; ++q) g[q] += sf[0] * e[q];
+      }
+      if (segActive(sNext)) {
+        segForce(sNext, sf, e);
+        for (int q = 0; q < 3; ++q) g[q] -= sf[0] * e[q];
+      }
+      addBendingGradient(n, f, g);
+    }
+    // shearPartners (solver.ts(ref):355-367)
+    int left = nbr[4 * n], right = nbr[4 * n + 1], down = nbr[4 * n + 2], up = nbr[4 * n + 3];
+    int cand[4][3];
+    int nc = 0;
+    if (right >= 0 && up >= 0) cand[nc][0] = n, cand[nc][1] = nbr[4 * up + 1], cand[nc++][2] = 0;
+    if (left >= 0 && down >= 0) cand[nc][0] = nbr[4 * down], cand[nc][1] = nbr[4 * down], cand[nc++][2] = 0;
+    if (left >= 0 && up >= 0) cand[nc][0] = left, cand[nc][1] = nbr[4 * up], cand[nc++][2] = 1;
+    if (right >= 0 && down >= 0) cand[nc][0] = down, cand[nc][1] = nbr[4 * down + 1], cand[nc++][2] = 1;
+    for (int k = 0; k < nc; ++k) {
+      int cell = cand[k][0], partner = cand[k][1];
+      if (partner < 0 || !diagActive(cell, cand[k][2])) continue;
+      double ks, jam, sl[3];
+      cellShear(cell, &ks, &jam);
+      double d0 = (x[3 * partner] + dx[3 * partner]) - (x[3 * n] + dx[3 * n]);
+      double d1 = (x[3 * partner + 1] + dx[3 * partner + 1]) - (x[3 * n + 1] + dx[3 * n + 1]);
+      double d2 = (x[3 * partner + 2] + dx[3 * partner + 2]) - (x[3 * n + 2] + dx[3 * n + 2]);
+      double l = hyp3(d0, d1, d2);
+      shearLaw(ks, shearRest(cell), l, jam, sl);
+      g[0] -= (sl[0] * d0) / l;
+      g[1] -= (sl[0] * d1) / l;
+      g[2] -= (sl[0] * d2) / l;
+    }
+  }
+
+  // energyChange (solver.ts(ref):430-534), plus the floor's quadratic model (energy.wgsl:116-125).
+  void energyChange(const double* d, double* out, double* mag) const {
+    const int NA = 4;
+    double h = prm.h;
+    std::vector<double> eacc(static_cast<size_t>(N) * 8, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int n = 0; n < N; ++n) {
+      double* o = &eacc[8 * static_cast<size_t>(n)];
+      double* mg = o + 4;
+      auto add = [&](int k, double v) {
+        o[k] += v;
+        mg[k] += std::fabs(v);
+      };
+      auto quad = [&](double gd, double q) {
+        for (int k = 0; k < NA; ++k) {
+          double a = LINE_ALPHAS[k];
+          o[k] += a * gd + 0.5 * a * a * q;
+          mg[k] += std::fabs(a * gd) + std::fabs(0.5 * a * a * q);
+        }
+      };
+      auto dirOf = [&](int m, double* o3) {
+        for (int q = 0; q < 3; ++q) o3[q] = pinned[m] ? 0.0 : d[3 * m + q];
+      };
+      auto dot = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+      auto lenChange = [&](const double* e0, const double* de, double a, double l0, double* la) {
+        double ea[3] = {e0[0] + a * de[0], e0[1] + a * de[1], e0[2] + a * de[2]};
+        *la = hyp3(ea[0], ea[1], ea[2]);
+        return (2 * a * dot(e0, de) + a * a * dot(de, de)) / std::max(*la + l0, 1e-12);
+      };
+      double dn[3], d0[3] = {dx[3 * n], dx[3 * n + 1], dx[3 * n + 2]};
+      dirOf(n, dn);
+      if (!pinned[n]) {
+        double w = mass[n] / (h * h);
+        double dp[3] = {d0[0] - pred[3 * n], d0[1] - pred[3 * n + 1], d0[2] - pred[3 * n + 2]};
+        quad(w * dot(dn, dp), w * dot(dn, dn));
+        double g[3] = {0, 0, 0};
+        double kg = gripTerm(n, g);
+        if (kg > 0) quad(dot(g, dn), kg * dot(dn, dn));
+        double Dd[9], t1[3], t2[3];
+        airDrag(n, Dd);
+        dragMul(Dd, d0, t1);
+        dragMul(Dd, dn, t2);
+        quad(dot(t1, dn), dot(dn, t2));
+        double gf[3] = {0, 0, 0}, Hf[3];
+        bool core;
+        if (floorTerm(n, gf, Hf, &core)) quad(dot(gf, dn), Hf[0] * dn[0] * dn[0] + Hf[1] * dn[1] * dn[1] + Hf[2] * dn[2] * dn[2]);
+      }
+      const Layer& mat = layer(n);
+      for (int f = 0; f < 2; ++f) {
+        const Yarn& y = mat.yarns[f];
+        int next = nbr[4 * n + 2 * f + 1];
+        int s = 2 * n + f;
+        if (next >= 0 && segActive(s)) {
+          double L = restLength[s];
+          double en[3], ec[3], db[3], de[3];
+          for (int q = 0; q < 3; ++q) {
+            en[q] = x[3 * next + q] - x[3 * n + q];
+            ec[q] = en[q] + dx[3 * next + q] - d0[q];
+          }
+          dirOf(next, db);
+          for (int q = 0; q < 3; ++q) de[q] = db[q] - dn[q];
+          double l0 = hyp3(ec[0], ec[1], ec[2]), ln = hyp3(en[0], en[1], en[2]);
+          double T0, K0;
+          response(s, l0 / L - 1, &T0, &K0);
+          double c = y.axialViscosity / (L * h);
+          for (int k = 0; k < NA; ++k) {
+            double la;
+            double dl = lenChange(ec, de, LINE_ALPHAS[k], l0, &la);
+            double Ta, Ka;
+            response(s, la / L - 1, &Ta, &Ka);
+            add(k, 0.5 * (T0 + Ta) * dl);
+            add(k, 0.5 * c * dl * (la + l0 - 2 * ln));
+          }
+        }
+        int prev = nbr[4 * n + 2 * f];
+        if (prev >= 0 && next >= 0 && segActive(2 * prev + f) && segActive(s)) {
+          double cf[5];
+          bendCoeffs(n, f, 2 * prev + f, s, cf);
+          double kb = cf[0], kd = cf[1], ab = cf[2], wa = cf[3], wc = cf[4];
+          double rn[3], r0[3], dp[3], dq[3], dr[3];
+          for (int q = 0; q < 3; ++q) {
+            rn[q] = wa * x[3 * prev + q] - 2 * x[3 * n + q] + wc * x[3 * next + q];
+            r0[q] = rn[q] + wa * dx[3 * prev + q] - 2 * d0[q] + wc * dx[3 * next + q];
+          }
+          dirOf(prev, dp);
+          dirOf(next, dq);
+          for (int q = 0; q < 3; ++q) dr[q] = wa * dp[q] - 2 * dn[q] + wc * dq[q];
+          double q0 = dot(r0, r0), l0 = std::sqrt(q0), lrn = hyp3(rn[0], rn[1], rn[2]);
+          for (int k = 0; k < NA; ++k) {
+            double a = LINE_ALPHAS[k];
+            double dqa = 2 * a * dot(r0, dr) + a * a * dot(dr, dr);
+            add(k, 0.5 * kb * bendPsiDelta(q0, q0 + dqa, dqa, ab));
+            double la;
+            double dl = lenChange(r0, dr, a, l0, &la);
+            add(k, 0.5 * kd * dl * (la + l0 - 2 * lrn));
+          }
+        }
+      }
+      if (nbr[4 * n + 1] >= 0 && nbr[4 * n + 3] >= 0) {
+        int r = nbr[4 * n + 1], t = nbr[4 * n + 3], rt = nbr[4 * r + 3];
+        double Ld = shearRest(n), ks, jam;
+        cellShear(n, &ks, &jam);
+        int pq[2][3] = {{n, rt, 0}, {r, t, 1}};
+        for (auto& e : pq) {
+          int p = e[0], q = e[1];
+          if (!diagActive(n, e[2])) continue;
+          double ec[3], dq[3], dp[3], de[3];
+          for (int z = 0; z < 3; ++z) ec[z] = x[3 * q + z] + dx[3 * q + z] - x[3 * p + z] - dx[3 * p + z];
+          dirOf(q, dq);
+          dirOf(p, dp);
+          for (int z = 0; z < 3; ++z) de[z] = dq[z] - dp[z];
+          double l0 = hyp3(ec[0], ec[1], ec[2]), sl0[3], sla[3];
+          shearLaw(ks, Ld, l0, jam, sl0);
+          for (int k = 0; k < NA; ++k) {
+            double la;
+            double dl = lenChange(ec, de, LINE_ALPHAS[k], l0, &la);
+            shearLaw(ks, Ld, la, jam, sla);
+            add(k, 0.5 * (sl0[0] + sla[0]) * dl);
+          }
+        }
+      }
+    }
+    for (int k = 0; k < 4; ++k) out[k] = mag[k] = 0;
+    for (int n = 0; n < N; ++n)
+      for (int k = 0; k < 4; ++k) {
+        out[k] += eacc[8 * static_cast<size_t>(n) + k];
+        mag[k] += eacc[8 * static_cast<size_t>(n) + 4 + k];
+      }
+  }
+
+  double segLength(int s) const {
+    int a = s >> 1, b = segOther(s);
+    return hyp3(x[3 * b] - x[3 * a], x[3 * b + 1] - x[3 * a + 1], x[3 * b + 2] - x[3 * a + 2]);
+  }
+
+  // potential (solver.ts(ref):537-595): the undamaged (history-free) potential, for verification.
+  double potential() const {
+    double h = prm.h, E = 0;
+    for (int n = 0; n < N; ++n) {
+      if (pinned[n]) continue;
+      double w = mass[n] / (2 * h * h);
+      for (int q = 0; q < 3; ++q) {
+        double dd = dx[3 * n + q] - pred[3 * n + q];
+        E += w * dd * dd;
+      }
+      E += gripEnergy(n);
+      double D[9], Ddx[3];
+      airDrag(n, D);
+      dragMul(D, &dx[3 * n], Ddx);
+      E += 0.5 * (dx[3 * n] * Ddx[0] + dx[3 * n + 1] * Ddx[1] + dx[3 * n + 2] * Ddx[2]);
+    }
+    for (int s = 0; s < 2 * N; ++s) {
+      if (!segActive(s)) continue;
+      int a = s >> 1, f = s & 1, b = segOther(s);
+      double pa[3], pb[3];
+      for (int q = 0; q < 3; ++q) {
+        pa[q] = x[3 * a + q] + dx[3 * a + q];
+        pb[q] = x[3 * b + q] + dx[3 * b + q];
+      }
+      double l = hyp3(pb[0] - pa[0], pb[1] - pa[1], pb[2] - pa[2]);
+      double ln = segLength(s);
+      double L = restLength[s];
+      const Yarn& y = layer(a).yarns[f];
+      E += L * axialEnergyDensity(y, l / L - 1);
+      double c = y.axialViscosity / (L * h);
+      E += 0.5 * c * (l - ln) * (l - ln);
+      int nb = nbr[4 * b + 2 * f + 1];
+      if (nb >= 0 && segActive(2 * b + f)) {
+        double cf[5], r[3], rn[3], ps[3];
+        bendCoeffs(b, f, s, 2 * b + f, cf);
+        triple(a, b, nb, cf[3], cf[4], r, rn);
+        bendPsi(r[0] * r[0] + r[1] * r[1] + r[2] * r[2], cf[2], ps);
+        E += 0.5 * cf[0] * ps[0];
+        double dv = hyp3(r[0], r[1], r[2]) - hyp3(rn[0], rn[1], rn[2]);
+        E += 0.5 * cf[1] * dv * dv;
+      }
+    }
+    for (int n = 0; n < N; ++n) {
+      if (nbr[4 * n + 1] < 0 || nbr[4 * n + 3] < 0) continue;
+      int r = nbr[4 * n + 1], t = nbr[4 * n + 3], rt = nbr[4 * r + 3];
+      double ks, jam, sl[3];
+      cellShear(n, &ks, &jam);
+      double Ld = shearRest(n);
+      int pq[2][3] = {{n, rt, 0}, {r, t, 1}};
+      for (auto& e : pq) {
+        if (!diagActive(n, e[2])) continue;
+        int p = e[0], q = e[1];
+        double l = hyp3(x[3 * q] + dx[3 * q] - x[3 * p] - dx[3 * p], x[3 * q + 1] + dx[3 * q + 1] - x[3 * p + 1] - dx[3 * p + 1],
+                        x[3 * q + 2] + dx[3 * q + 2] - x[3 * p + 2] - dx[3 * p + 2]);
+        shearLaw(ks, Ld, l, jam, sl);
+        E += sl[2];
+      }
+    }
+    return E;
+  }
+
+  // predict (solver.ts(ref):602-613).
+  void predict() {
+    lagged.clear();
+    double h = prm.h;
+    for (int n = 0; n < N; ++n)
+      for (int q = 0; q < 3; ++q) {
+        double hv = pinned[n] ? 0 : h * v[3 * n + q];
+        pred[3 * n + q] = pinned[n] ? 0 : hv + h * h * prm.gravity[q];
+        dx[3 * n + q] = hv;
+      }
+  }
+
+  // segTension (solver.ts(ref):647-652).
+  void segTension(int s, double* T, double* k) const {
+    double L = restLength[s], l = segLength(s), K;
+    response(s, l / L - 1, T, &K);
+    *k = std::max(K, 0.0) * (l / (L * L));
+  }
+
+  void updateField();
+  int pullOut();
+  int coupleSpans();
+  void updateDamage();
+  void slipNode(int n, int f);
+  void updateSlip();
+  void finalize();
+
+  double yarnMaterialLength() const {
+    double total = 0;
+    for (int s = 0; s < 2 * N; ++s)
+      if (segActive(s)) total += restLength[s];
+    for (int q = 0; q < 4 * N; ++q) total += tails[q];
+    return total;
+  }
+
+  // multigrid
+  std::shared_ptr<StencilOperator> assembleFineOperator() const;
+  void rhs(double* b) const;
+  std::vector<MGLevel> buildHierarchy(std::shared_ptr<StencilOperator> fine) const;
+  void vcycle(const std::vector<MGLevel>& levels, int k, double* x, const double* b) const;
+  void pcg(const std::vector<MGLevel>& levels, const double* b, double* x, int iterations, double tol, int* done,
+           double* rel) const;
+  double newtonStep(int* pcgDone, double* rel, double* alphaOut);
+};
+
+// updateField (yarnField.ts:338-410).
+void Solver::updateField() {
+  std::vector<uint8_t> sep(fieldDamage.size());
+  for (size_t q = 0; q < fieldDamage.size(); ++q) sep[q] = fieldDamage[q] >= DAMAGE_SEPARATED ? 1 : 0;
+  for (const Layer& L : layers) {
+    for (int j = 0; j < L.ny; ++j)
+      for (int i = 0; i < L.nx; ++i)
+        for (int f = 0; f < 2; ++f) {
+          if ((f == 0 && i >= L.nx - 1) || (f == 1 && j >= L.ny - 1)) continue;
+          int s = 2 * (L.nodeOffset + j * L.nx + i) + f;
+          if (!segActive(s)) continue;
+          const Yarn& y = L.yarns[f];
+          int B = bundleOf(L, f), P = spanLength(L, f);
+          double soft = softening[s] / restLength[s];
+          int reach = shareReach(L, f);
+          for (int q = 0; q < B; ++q) {
+            if ((cutMask[s] >> q) & 1) continue;
+            int mid = spanCrossing(L, i, j, f, q, P >> 1) - L.fOffset;
+            double eps = interpolatedStrain(L, f, mid % L.K, mid / L.K, strain.data());
+            if (!std::isfinite(eps)) continue;
+            double minPeak = INF;
+            for (int p = 0; p < P; ++p) {
+              int c = spanCrossing(L, i, j, f, q, p);
+              minPeak = std::min(minPeak, strainAtTension(y, (static_cast<double>(fieldStrength[2 * c + f]) * B) / areaOf(fieldArea[2 * c + f])));
+            }
+            if (eps * (1 + SHARE_FRACTION * SHARE_MAXRUN) <= minPeak) continue;
+            int g = 1 - f;
+            int kM = mid % L.K, mM = mid / L.K;
+            double ec = interpolatedStrain(L, g, kM, mM, strain.data());
+            double tCross = std::isfinite(ec)
+                                ? (std::max(0.0, axialTension(L.yarns[g], ec)) * areaOf(fieldArea[2 * (mid + L.fOffset) + g])) / bundleOf(L, g)
+                                : 0;
+            double transfer = shareCap(reach, L.crossingFriction, crossingNormal0[s >> 1] / (L.bu * L.bv), L.crossingWrap, tCross, 1);
+            int best = -1, soft0 = -1, softCode = 0;
+            double bestScore = -INF, bestOmega = 1;
+            for (int p = 0; p < P; ++p) {
+              int c = spanCrossing(L, i, j, f, q, p);
+              int local = c - L.fOffset;
+              double omega = shareFactor(L, sep.data(), f, local % L.K, local / L.K, reach, transfer / fieldStrength[2 * c + f]);
+              double peak = strainAtTension(y, (static_cast<double>(fieldStrength[2 * c + f]) * B) / areaOf(fieldArea[2 * c + f]));
+              double score = omega / peak;
+              if (score > bestScore) best = c, bestScore = score, bestOmega = omega;
+              if (fieldDamage[2 * c + f] > softCode) soft0 = c, softCode = fieldDamage[2 * c + f];
+            }
+            if (soft0 >= 0) {
+              best = soft0;
+              int local = best - L.fOffset;
+              bestOmega = shareFactor(L, sep.data(), f, local % L.K, local / L.K, reach, transfer / fieldStrength[2 * best + f]);
+            }
+            int code = damageCode(yarnDamage(y, B, areaOf(fieldArea[2 * best + f]), fieldStrength[2 * best + f], soft, eps * bestOmega));
+            if (code > fieldDamage[2 * best + f]) fieldDamage[2 * best + f] = static_cast<uint8_t>(code);
+          }
+        }
+  }
+}
+
+// pullOut (yarnField.ts:125-152).
+int Solver::pullOut() {
+  std::vector<int> marked;
+  for (const Layer& L : layers)
+    for (int m = 0; m < L.M; ++m)
+      for (int k = 0; k < L.K; ++k) {
+        int c = L.fOffset + m * L.K + k;
+        for (int f = 0; f < 2; ++f) {
+          if (fieldDamage[2 * c + f] >= DAMAGE_SEPARATED) continue;
+          int d = breakDistance(L, fieldDamage.data(), f, k, m);
+          if (d < 0) continue;
+          double eps = interpolatedStrain(L, f, k, m, strain.data());
+          if (!std::isfinite(eps)) continue;
+          int g = 1 - f;
+          double ec = interpolatedStrain(L, g, k, m, strain.data());
+          double tCross = std::isfinite(ec) ? (std::max(0.0, axialTension(L.yarns[g], ec)) * areaOf(fieldArea[2 * c + g])) / bundleOf(L, g) : 0;
+          int n = nodeOfCrossing(L, k, m);
+          double pitch = f == 1 ? L.weavePitchV : L.weavePitchU;
+          double delta = recoilLength(L.yarns[f], bundleOf(L, f), areaOf(fieldArea[2 * c + f]), fieldStrength[2 * c + f], eps,
+                                      L.crossingFriction, crossingNormal0[n] / (L.bu * L.bv), L.crossingWrap, tCross, pitch);
+          if (delta >= (d - 0.5) * pitch) marked.push_back(2 * c + f);
+        }
+      }
+  for (int q : marked) fieldDamage[q] = DAMAGE_PULLED;
+  return static_cast<int>(marked.size());
+}
+
+// coupleSpans (yarnField.ts:443-499).
+int Solver::coupleSpans() {
+  int ruptures = 0;
+  for (const Layer& L : layers)
+    for (int j = 0; j < L.ny; ++j)
+      for (int i = 0; i < L.nx; ++i)
+        for (int f = 0; f < 2; ++f) {
+          if ((f == 0 && i >= L.nx - 1) || (f == 1 && j >= L.ny - 1)) continue;
+          int n = L.nodeOffset + j * L.nx + i;
+          int s = 2 * n + f;
+          if (segFlags[s] & SEG_SLIPPED) {
+            partSpanYarns(L, fieldDamage.data(), i, j, f, failSite[s] < 0.5 ? 0 : 1);
+            segFlags[s] &= static_cast<uint16_t>(~SEG_SLIPPED);
+            continue;
+          }
+          if (!segActive(s)) continue;
+          int B = bundleOf(L, f), P = spanLength(L, f);
+          double sum = 0, site = 0;
+          uint32_t mask = 0;
+          for (int q = 0; q < B; ++q) {
+            int dmax = 0, first = -1;
+            double compliance = 0;
+            for (int p = 0; p < P; ++p) {
+              int c = spanCrossing(L, i, j, f, q, p);
+              int d = fieldDamage[2 * c + f];
+              if (d > dmax) dmax = d;
+              if (d >= DAMAGE_SEPARATED && first < 0) first = p;
+              compliance += 1 / areaOf(fieldArea[2 * c + f]);
+            }
+            sum += (dmax >= DAMAGE_SEPARATED ? 0 : 1 - static_cast<double>(dmax) / DAMAGE_CUT) * (P / compliance);
+            if (dmax >= DAMAGE_SEPARATED) {
+              mask |= 1u << q;
+              site += (first + 0.5) / P;
+            }
+          }
+          intact[s] = sum / B;
+          cutMask[s] = mask;
+          uint32_t full = B >= 32 ? 0xffffffffu : ((1u << B) - 1u);
+          if (mask == full) {
+            double phi = site / B, rest = restLength[s];
+            int b = f == 0 ? n + 1 : n + L.nx;
+            segFlags[s] |= SEG_BROKEN;
+            failSite[s] = phi;
+            tails[4 * n + 2 * f + 1] += rest * phi;
+            tails[4 * b + 2 * f] += rest * (1 - phi);
+            ruptures++;
+            partSpanYarns(L, fieldDamage.data(), i, j, f, -1);
+          }
+        }
+  return ruptures;
+}
+
+// updateDamage (solver.ts(ref):659-666).
+void Solver::updateDamage() {
+  for (int q = 0; q < 2 * N; ++q) strain[q] = segActive(q) ? segLength(q) / restLength[q] - 1 : NAN;
+  updateField();
+  pullOut();
+  brokenCount += coupleSpans();
+}
+
+// slipNode (solver.ts(ref):685-740).
+void Solver::slipNode(int n, int f) {
+  if (pinned[n]) return;
+  int sL = seg(n, f, -1), sR = seg(n, f, 1);
+  if (sL < 0 || sR < 0) return;
+  bool actL = segActive(sL), actR = segActive(sR);
+  if (!actL && !actR) return;
+  int tailL = 4 * n + 2 * f, tailR = 4 * n + 2 * f + 1;
+  double TL = 0, kL = 0, TR = 0, kR = 0;
+  if (actL) segTension(sL, &TL, &kL);
+  if (actR) segTension(sR, &TR, &kR);
+  double tc = 0;
+  int cnt = 0;
+  for (int dir = -1; dir <= 1; dir += 2) {
+    int s = seg(n, 1 - f, dir);
+    if (segActive(s)) {
+      double T, k;
+      segTension(s, &T, &k);
+      tc += std::max(0.0, T);
+      cnt++;
+    }
+  }
+  if (cnt == 0) return;
+  tc /= cnt;
+  const Layer& mat = layer(n);
+  double Fc = mat.crossingFriction * (crossingNormal0[n] + mat.crossingWrap * mat.yarns[f].yarnsPerSpan * tc);
+  double dT = std::max(TR, 0.0) - std::max(TL, 0.0);
+  if (std::fabs(dT) <= Fc) return;
+  bool highR = dT > 0;
+  double kHigh = highR ? kR : kL;
+  bool lowActive = highR ? actL : actR;
+  double kLow = lowActive ? (highR ? kL : kR) : 0;
+  double dl = (std::fabs(dT) - Fc) / std::max(kHigh + kLow, 1e-9);
+  double pitch = f == 0 ? mat.pitchU : mat.pitchV;
+  int sHigh = highR ? sR : sL, sLow = highR ? sL : sR;
+  if (lowActive) {
+    dl = std::min(dl, std::max(0.0, restLength[sLow] - 0.55 * pitch));
+    restLength[sLow] -= dl;
+    restLength[sHigh] += dl;
+  } else {
+    int tIdx = highR ? tailL : tailR;
+    dl = std::min(dl, tails[tIdx]);
+    tails[tIdx] -= dl;
+    restLength[sHigh] += dl;
+    if (tails[tIdx] <= 1e-9) {
+      tails[tIdx] = 0;
+      int far = highR ? segOther(sHigh) : sHigh >> 1;
+      int farTail = highR ? 4 * far + 2 * f : 4 * far + 2 * f + 1;
+      tails[farTail] += restLength[sHigh];
+      segFlags[sHigh] |= SEG_BROKEN | SEG_SLIPPED;
+      failSite[sHigh] = highR ? 0 : 1;
+      pulledOutCount++;
+    }
+  }
+}
+
+// updateSlip (solver.ts(ref):669-683).
+void Solver::updateSlip() {
+  for (int f = 0; f < 2; ++f)
+    for (int parity = 0; parity < 2; ++parity)
+      for (const Layer& L : layers)
+        for (int j = 0; j < L.ny; ++j)
+          for (int i = 0; i < L.nx; ++i) {
+            int along = f == 0 ? i : j;
+            if ((along & 1) != parity) continue;
+            slipNode(L.nodeOffset + j * L.nx + i, f);
+          }
+}
+
+// finalize (solver.ts(ref):622-632).
+void Solver::finalize() {
+  double h = prm.h;
+  for (int q = 0; q < 3 * N; ++q) {
+    v[q] = dx[q] / h;
+    x[q] += dx[q];
+    dx[q] = 0;
+  }
+  if (!historyEnabled) return;
+  updateDamage();
+  updateSlip();
+}
+
+// ---------------------------------------------------------------------------- assembly
+
+void axialBlock(double kPar, double kPerp, const double* e, double* out) {
+  double d = kPar - kPerp;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) out[r * 3 + c] = d * e[r] * e[c] + (r == c ? kPerp : 0);
+}
+// scatterPair (newtonMultigrid.ts:133-146).
+void scatterPair(StencilOperator& A, int a, int b, const double* H) {
+  int ia = A.ij[3 * a], ja = A.ij[3 * a + 1], ib = A.ij[3 * b], jb = A.ij[3 * b + 1];
+  if (!A.fixed[a]) {
+    A.addBlock(a, CENTER, 1, H);
+    if (!A.fixed[b]) A.addBlock(a, offsetIndex(ib - ia, jb - ja), -1, H);
+  }
+  if (!A.fixed[b]) {
+    A.addBlock(b, CENTER, 1, H);
+    if (!A.fixed[a]) A.addBlock(b, offsetIndex(ia - ib, ja - jb), -1, H);
+  }
+}
+const double I3[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+
+// assembleFineOperator (newtonMultigrid.ts:169-274), plus the floor's diagonal Hessian and its hard
+// limit (assemble.wgsl:191-209, 318-322) when the floor is on.
+std::shared_ptr<StencilOperator> Solver::assembleFineOperator() const {
+  std::vector<LatticeLayer> ll;
+  for (auto& L : layers) ll.push_back({L.nx, L.ny, L.nodeOffset});
+  auto Ap = std::make_shared<StencilOperator>(ll);
+  StencilOperator& A = *Ap;
+  A.linkSolver = this;
+  double h = prm.h;
+  for (int n = 0; n < N; ++n)
+    if (pinned[n]) {
+      A.fixed[n] = 1;
+      A.addBlock(n, CENTER, 1, I3);
+    }
+  double gTmp[3];
+  for (int n = 0; n < N; ++n) {
+    if (A.fixed[n]) continue;
+    gTmp[0] = gTmp[1] = gTmp[2] = 0;
+    A.addBlock(n, CENTER, mass[n] / (h * h) + gripTerm(n, gTmp), I3);
+    double D[9];
+    airDrag(n, D);
+    A.addBlock(n, CENTER, 1, D);
+  }
+  double H[9], e[3];
+  for (int s = 0; s < 2 * N; ++s) {
+    if (!segActive(s)) continue;
+    int a = s >> 1, f = s & 1, b = segOther(s);
+    double l = 0;
+    for (int q = 0; q < 3; ++q) {
+      e[q] = x[3 * b + q] + dx[3 * b + q] - x[3 * a + q] - dx[3 * a + q];
+      l += e[q] * e[q];
+    }
+    l = std::sqrt(l);
+    for (int q = 0; q < 3; ++q) e[q] /= l;
+    double L = restLength[s];
+    const Yarn& y = layer(a).yarns[f];
+    double T, K;
+    response(s, l / L - 1, &T, &K);
+    double ln = segLength(s);
+    double c = y.axialViscosity / (L * h);
+    double fs = T + c * (l - ln);
+    axialBlock(std::max(K, 0.0) / L + c, std::max(fs, 0.0) / l, e, H);
+    scatterPair(A, a, b, H);
+  }
+  for (int b = 0; b < N; ++b)
+    for (int f = 0; f < 2; ++f) {
+      int a = nbr[4 * b + 2 * f], c = nbr[4 * b + 2 * f + 1];
+      if (a < 0 || c < 0) continue;
+      int s0 = 2 * a + f, s1 = 2 * b + f;
+      if (!segActive(s0) || !segActive(s1)) continue;
+      const Yarn& y = layer(b).yarns[f];
+      double cf[5];
+      bendCoeffs(b, f, s0, s1, cf);
+      double kb = cf[0], fold = cf[2], wa = cf[3], wc = cf[4];
+      double q2 = 0;
+      for (int z = 0; z < 3; ++z) {
+        double rz = wa * (x[3 * a + z] + dx[3 * a + z]) - 2 * (x[3 * b + z] + dx[3 * b + z]) + wc * (x[3 * c + z] + dx[3 * c + z]);
+        q2 += rz * rz;
+      }
+      double ps[3];
+      bendPsi(q2, fold, ps);
+      double k = kb * (ps[1] + 2 * ps[2] * q2) + (kb * y.bendViscosity) / h;
+      int nodes[3] = {a, b, c};
+      double w[3] = {wa, -2, wc};
+      for (int p = 0; p < 3; ++p) {
+        int r = nodes[p];
+        if (A.fixed[r]) continue;
+        for (int q = 0; q < 3; ++q) {
+          int m = nodes[q];
+          if (A.fixed[m]) continue;
+          int o = offsetIndex(A.ij[3 * m] - A.ij[3 * r], A.ij[3 * m + 1] - A.ij[3 * r + 1]);
+          A.addBlock(r, o, k * w[p] * w[q], I3);
+        }
+      }
+    }
+  for (int n = 0; n < N; ++n) {
+    int r = nbr[4 * n + 1], t = nbr[4 * n + 3];
+    if (r < 0 || t < 0) continue;
+    int rt = nbr[4 * r + 3];
+    double ks, jam;
+    cellShear(n, &ks, &jam);
+    double Ld = std::sqrt(restLength[2 * n] * restLength[2 * n] + restLength[2 * n + 1] * restLength[2 * n + 1]);
+    int pq[2][3] = {{n, rt, 0}, {r, t, 1}};
+    for (auto& pe : pq) {
+      int p = pe[0], q = pe[1];
+      if (!diagActive(n, pe[2])) continue;
+      double pa[3], l = 0, sl[3];
+      for (int z = 0; z < 3; ++z) {
+        pa[z] = x[3 * q + z] + dx[3 * q + z] - x[3 * p + z] - dx[3 * p + z];
+        l += pa[z] * pa[z];
+      }
+      l = std::sqrt(l);
+      for (int z = 0; z < 3; ++z) pa[z] /= l;
+      shearLaw(ks, Ld, l, jam, sl);
+      axialBlock(sl[1], std::max(sl[0], 0.0) / l, pa, H);
+      scatterPair(A, p, q, H);
+    }
+  }
+  if (floor.on) {
+    for (int n = 0; n < N; ++n) {
+      if (A.fixed[n]) continue;
+      double g[3], Hf[3];
+      nodeGradient(n, g);
+      double gg[3] = {0, 0, 0};
+      bool core;
+      if (!floorTerm(n, gg, Hf, &core)) continue;
+      double* Dn = &A.A[(static_cast<size_t>(n) * STENCIL + CENTER) * 9];
+      Dn[0] += Hf[0];
+      Dn[4] += Hf[1];
+      Dn[8] += Hf[2];
+      if (core && g[2] > 0) Dn[8] += 100.0 * (Dn[0] + Dn[4] + Dn[8]);
+    }
+  }
+  return Ap;
+}
+
+void Solver::rhs(double* b) const {
+#pragma omp parallel for schedule(static)
+  for (int n = 0; n < N; ++n) {
+    double g[3];
+    if (pinned[n]) {
+      b[3 * n] = b[3 * n + 1] = b[3 * n + 2] = 0;
+      continue;
+    }
+    nodeGradient(n, g);
+    b[3 * n] = -g[0];
+    b[3 * n + 1] = -g[1];
+    b[3 * n + 2] = -g[2];
+  }
+}
+
+// linked (newtonMultigrid.ts:287-295) with the fine lattice's A.link (newtonMultigrid.ts:172-175).
+bool linked(const StencilOperator& A, int a, int di, int dj) {
+  int b = A.nbr(a, di, dj);
+  if (b < 0) return false;
+  if (A.linkSolver) {
+    const Solver& S = *A.linkSolver;
+    int s = S.seg(a, di != 0 ? 0 : 1, di + dj > 0 ? 1 : -1);
+    return S.segActive(s) && S.intact[s] > LINK_MIN_INTACT;
+  }
+  if (A.fixed[b]) return true;
+  const double* p = &A.A[(static_cast<size_t>(a) * STENCIL + offsetIndex(di, dj)) * 9];
+  for (int q = 0; q < 9; ++q)
+    if (p[q] != 0) return true;
+  return false;
+}
+
+// buildProlongation (newtonMultigrid.ts:305-342).
+std::shared_ptr<Prolongation> buildProlongation(const StencilOperator& fine, std::vector<LatticeLayer>* coarseOut) {
+  std::vector<LatticeLayer> coarse = coarsenLayers(fine.layers);
+  auto P = std::make_shared<Prolongation>();
+  P->idx.assign(4 * static_cast<size_t>(fine.N), -1);
+  P->w.assign(4 * static_cast<size_t>(fine.N), 0.0);
+  for (size_t l = 0; l < fine.layers.size(); ++l) {
+    const LatticeLayer& L = fine.layers[l];
+    const LatticeLayer& C = coarse[l];
+    for (int j = 0; j < L.ny; ++j) {
+      int bjI[2];
+      double bjW[2];
+      int nbj = bracket(j, L.ny, bjI, bjW);
+      for (int i = 0; i < L.nx; ++i) {
+        int f = L.offset + j * L.nx + i;
+        if (fine.fixed[f]) continue;
+        int biI[2];
+        double biW[2];
+        int nbi = bracket(i, L.nx, biI, biW);
+        int k = 0;
+        double sum = 0;
+        for (int a = 0; a < nbj; ++a) {
+          int J = bjI[a];
+          double wj = bjW[a];
+          int dj = coarseToFine(J, L.ny) - j;
+          for (int b = 0; b < nbi; ++b) {
+            int I = biI[b];
+            double wi = biW[b];
+            int di = coarseToFine(I, L.nx) - i;
+            bool ok = true;
+            if (di != 0 && dj != 0) {
+              int m1 = fine.nbr(f, di, 0), m2 = fine.nbr(f, 0, dj);
+              ok = (linked(fine, f, di, 0) && linked(fine, m1, 0, dj)) || (linked(fine, f, 0, dj) && linked(fine, m2, di, 0));
+            } else if (di != 0 || dj != 0) {
+              ok = linked(fine, f, di, dj);
+            }
+            P->idx[4 * f + k] = C.offset + J * C.nx + I;
+            P->w[4 * f + k] = ok ? wi * wj : 0;
+            sum += P->w[4 * f + k];
+            k++;
+          }
+        }
+        for (int q = 0; q < k; ++q) P->w[4 * f + q] = sum > 0 ? P->w[4 * f + q] / sum : 0;
+      }
+    }
+  }
+  *coarseOut = coarse;
+  return P;
+}
+
+// galerkin (newtonMultigrid.ts:345-387).
+std::shared_ptr<StencilOperator> galerkin(const StencilOperator& A, const std::vector<LatticeLayer>& coarseLayers,
+                                          const Prolongation& P) {
+  auto Cp = std::make_shared<StencilOperator>(coarseLayers);
+  StencilOperator& C = *Cp;
+  double blk[9];
+  for (int a = 0; a < A.N; ++a) {
+    if (A.fixed[a]) continue;
+    for (int dj = -2; dj <= 2; ++dj)
+      for (int di = -2; di <= 2; ++di) {
+        int b = A.nbr(a, di, dj);
+        if (b < 0 || A.fixed[b]) continue;
+        const double* src = &A.A[(static_cast<size_t>(a) * STENCIL + offsetIndex(di, dj)) * 9];
+        bool nz = false;
+        for (int q = 0; q < 9; ++q) {
+          blk[q] = src[q];
+          nz = nz || blk[q] != 0;
+        }
+        if (!nz) continue;
+        for (int ka = 0; ka < 4; ++ka) {
+          int I = P.idx[4 * a + ka];
+          if (I < 0) continue;
+          double wa = P.w[4 * a + ka];
+          for (int kb = 0; kb < 4; ++kb) {
+            int J = P.idx[4 * b + kb];
+            if (J < 0) continue;
+            double w = wa * P.w[4 * b + kb];
+            int oi = C.ij[3 * J] - C.ij[3 * I], oj = C.ij[3 * J + 1] - C.ij[3 * I + 1];
+            if (std::abs(oi) > 2 || std::abs(oj) > 2) throw std::runtime_error("Galerkin stencil exceeds radius 2");
+            C.addBlock(I, offsetIndex(oi, oj), w, blk);
+          }
+        }
+      }
+  }
+  for (int I = 0; I < C.N; ++I) {
+    double* base = &C.A[(static_cast<size_t>(I) * STENCIL + CENTER) * 9];
+    if (base[0] + base[4] + base[8] <= 0) {
+      C.fixed[I] = 1;
+      std::fill(&C.A[static_cast<size_t>(I) * STENCIL * 9], &C.A[static_cast<size_t>(I + 1) * STENCIL * 9], 0.0);
+      base[0] = base[4] = base[8] = 1;
+    }
+  }
+  return Cp;
+}
+
+// inv3 / pivotInv3 (newtonMultigrid.ts:391-423).
+void inv3(const double* a, double* out) {
+  double a00 = a[0], a01 = a[1], a02 = a[2], a10 = a[3], a11 = a[4], a12 = a[5], a20 = a[6], a21 = a[7], a22 = a[8];
+  double c00 = a11 * a22 - a12 * a21, c01 = a12 * a20 - a10 * a22, c02 = a10 * a21 - a11 * a20;
+  double det = a00 * c00 + a01 * c01 + a02 * c02;
+  double id = 1 / det;
+  out[0] = c00 * id;
+  out[1] = (a02 * a21 - a01 * a22) * id;
+  out[2] = (a01 * a12 - a02 * a11) * id;
+  out[3] = c01 * id;
+  out[4] = (a00 * a22 - a02 * a20) * id;
+  out[5] = (a02 * a10 - a00 * a12) * id;
+  out[6] = c02 * id;
+  out[7] = (a01 * a20 - a00 * a21) * id;
+  out[8] = (a00 * a11 - a01 * a10) * id;
+}
+void pivotInv3(const double* a, double* out, double shift) {
+  double e = shift * std::max(std::max(std::fabs(a[0]), std::fabs(a[4])), std::fabs(a[8]));
+  double sh[9];
+  for (int q = 0; q < 9; ++q) sh[q] = a[q];
+  sh[0] += e;
+  sh[4] += e;
+  sh[8] += e;
+  inv3(sh, out);
+}
+void mul3(const double* a, const double* b, double* out) {
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) out[r * 3 + c] = a[r * 3] * b[c] + a[r * 3 + 1] * b[3 + c] + a[r * 3 + 2] * b[6 + c];
+}
+
+// solvePenta (newtonMultigrid.ts:435-473).
+void solvePenta(int n, const double* D, const double* E, const double* F, const double* r, double* x, double shift) {
+  std::vector<double> Dk(D, D + 9 * n), U1(E, E + 9 * n), L1(9 * static_cast<size_t>(n), 0.0), rk(r, r + 3 * n);
+  for (int k = 1; k < n; ++k)
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) L1[9 * k + a * 3 + b] = E[9 * (k - 1) + b * 3 + a];
+  double inv[9], Lm[9], t[9], Amk[9];
+  for (int k = 0; k < n; ++k) {
+    pivotInv3(&Dk[9 * k], inv, shift);
+    for (int m = k + 1; m <= k + 2 && m < n; ++m) {
+      if (m == k + 1)
+        std::memcpy(Amk, &L1[9 * m], sizeof Amk);
+      else
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) Amk[a * 3 + b] = F[9 * k + b * 3 + a];
+      mul3(Amk, inv, Lm);
+      if (k + 1 < n) {
+        mul3(Lm, &U1[9 * k], t);
+        double* dst = m == k + 1 ? Dk.data() : L1.data();
+        for (int q = 0; q < 9; ++q) dst[9 * m + q] -= t[q];
+      }
+      if (k + 2 < n) {
+        mul3(Lm, &F[9 * k], t);
+        double* dst = m == k + 1 ? U1.data() : Dk.data();
+        for (int q = 0; q < 9; ++q) dst[9 * m + q] -= t[q];
+      }
+      for (int q = 0; q < 3; ++q) rk[3 * m + q] -= Lm[q * 3] * rk[3 * k] + Lm[q * 3 + 1] * rk[3 * k + 1] + Lm[q * 3 + 2] * rk[3 * k + 2];
+    }
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    double b0[3] = {rk[3 * k], rk[3 * k + 1], rk[3 * k + 2]};
+    for (int q = 0; q < 3; ++q) {
+      if (k + 1 < n) b0[q] -= U1[9 * k + q * 3] * x[3 * (k + 1)] + U1[9 * k + q * 3 + 1] * x[3 * (k + 1) + 1] + U1[9 * k + q * 3 + 2] * x[3 * (k + 1) + 2];
+      if (k + 2 < n) b0[q] -= F[9 * k + q * 3] * x[3 * (k + 2)] + F[9 * k + q * 3 + 1] * x[3 * (k + 2) + 1] + F[9 * k + q * 3 + 2] * x[3 * (k + 2) + 2];
+    }
+    pivotInv3(&Dk[9 * k], inv, shift);
+    for (int q = 0; q < 3; ++q) x[3 * k + q] = inv[q * 3] * b0[0] + inv[q * 3 + 1] * b0[1] + inv[q * 3 + 2] * b0[2];
+  }
+}
+
+// smoothLines (newtonMultigrid.ts:659-733).
+void smoothLines(const StencilOperator& A, double* x, const double* b, bool reverse, int colors) {
+  int maxLen = 0;
+  for (auto& L : A.layers) maxLen = std::max(maxLen, std::max(L.nx, L.ny));
+  std::vector<std::pair<int, int>> order;
+  for (int family : {1, 0})
+    for (int c = 0; c < colors; ++c) order.push_back({family, c});
+  if (reverse) std::reverse(order.begin(), order.end());
+  std::vector<double> xOld(3 * static_cast<size_t>(A.N));
+  for (auto& fc : order) {
+    int family = fc.first, color = fc.second;
+    std::copy(x, x + 3 * static_cast<size_t>(A.N), xOld.begin());
+    for (const LatticeLayer& L : A.layers) {
+      int lines = family == 0 ? L.ny : L.nx;
+      int len = family == 0 ? L.nx : L.ny;
+      int nlines = lines > color ? (lines - color + colors - 1) / colors : 0;
+#pragma omp parallel
+      {
+        std::vector<double> D(9 * static_cast<size_t>(maxLen)), E(D.size()), F(D.size()), r(3 * static_cast<size_t>(maxLen)),
+            sol(r.size());
+#pragma omp for schedule(dynamic, 1)
+        for (int li = 0; li < nlines; ++li) {
+          int line = color + li * colors;
+          auto node = [&](int k) { return family == 0 ? L.offset + line * L.nx + k : L.offset + k * L.nx + line; };
+          std::fill(D.begin(), D.begin() + 9 * len, 0.0);
+          std::fill(E.begin(), E.begin() + 9 * len, 0.0);
+          for (int k = 0; k < len; ++k) {
+            int n = node(k);
+            r[3 * k] = b[3 * n];
+            r[3 * k + 1] = b[3 * n + 1];
+            r[3 * k + 2] = b[3 * n + 2];
+            if (A.fixed[n]) {
+              D[9 * k] = D[9 * k + 4] = D[9 * k + 8] = 1;
+              continue;
+            }
+            double maj = 0;
+            for (int dj = -2; dj <= 2; ++dj)
+              for (int di = -2; di <= 2; ++di) {
+                int m = A.nbr(n, di, dj);
+                if (m < 0 || (A.fixed[m] && !(di == 0 && dj == 0))) continue;
+                const double* B = &A.A[(static_cast<size_t>(n) * STENCIL + offsetIndex(di, dj)) * 9];
+                int along = family == 0 ? di : dj, across = family == 0 ? dj : di;
+                if (across == 0 && along == 0) {
+                  for (int q = 0; q < 9; ++q) D[9 * k + q] += B[q];
+                  continue;
+                }
+                if (across == 0 && along == 1) {
+                  for (int q = 0; q < 9; ++q) E[9 * k + q] = B[q];
+                  continue;
+                }
+                if (across == 0 && along == -1) continue;
+                if (across == 0 || std::abs(across) == colors) {
+                  double s = 0;
+                  for (int q = 0; q < 9; ++q) s += B[q] * B[q];
+                  maj += std::sqrt(s);
+                }
+                double x0 = xOld[3 * m], x1 = xOld[3 * m + 1], x2 = xOld[3 * m + 2];
+                r[3 * k] -= B[0] * x0 + B[1] * x1 + B[2] * x2;
+                r[3 * k + 1] -= B[3] * x0 + B[4] * x1 + B[5] * x2;
+                r[3 * k + 2] -= B[6] * x0 + B[7] * x1 + B[8] * x2;
+              }
+            D[9 * k] += maj;
+            D[9 * k + 4] += maj;
+            D[9 * k + 8] += maj;
+            r[3 * k] += maj * xOld[3 * n];
+            r[3 * k + 1] += maj * xOld[3 * n + 1];
+            r[3 * k + 2] += maj * xOld[3 * n + 2];
+          }
+          std::fill(F.begin(), F.begin() + 9 * len, 0.0);
+          solvePenta(len, D.data(), E.data(), F.data(), r.data(), sol.data(), PIVOT_SHIFT);
+          for (int k = 0; k < len; ++k) {
+            int n = node(k);
+            if (A.fixed[n]) continue;
+            x[3 * n] = sol[3 * k];
+            x[3 * n + 1] = sol[3 * k + 1];
+            x[3 * n + 2] = sol[3 * k + 2];
+          }
+        }
+      }
+    }
+  }
+}
+
+// buildHierarchy (newtonMultigrid.ts:480-491).
+std::vector<MGLevel> Solver::buildHierarchy(std::shared_ptr<StencilOperator> fine) const {
+  std::vector<MGLevel> levels;
+  levels.push_back({fine, nullptr});
+  std::shared_ptr<StencilOperator> cur = fine;
+  while (cur->N > prm.max_coarsest_nodes && shouldCoarsen(cur->layers)) {
+    std::vector<LatticeLayer> coarse;
+    auto P = buildProlongation(*cur, &coarse);
+    auto C = galerkin(*cur, coarse, *P);
+    levels.back().P = P;
+    levels.push_back({C, nullptr});
+    cur = C;
+  }
+  return levels;
+}
+
+// vcycle (newtonMultigrid.ts:495-528).
+void Solver::vcycle(const std::vector<MGLevel>& levels, int k, double* x, const double* b) const {
+  const StencilOperator& A = *levels[k].A;
+  int colors = prm.line_colors;
+  if (!levels[k].P) {
+    for (int s = 0; s < prm.coarse_sweeps; ++s) smoothLines(A, x, b, (s & 1) == 1, colors);
+    return;
+  }
+  const Prolongation& P = *levels[k].P;
+  smoothLines(A, x, b, false, colors);
+  std::vector<double> Ax(3 * static_cast<size_t>(A.N));
+  A.apply(x, Ax.data());
+  const StencilOperator& C = *levels[k + 1].A;
+  std::vector<double> rc(3 * static_cast<size_t>(C.N), 0.0);
+  for (int f = 0; f < A.N; ++f) {
+    if (A.fixed[f]) continue;
+    for (int kk = 0; kk < 4; ++kk) {
+      int c = P.idx[4 * f + kk];
+      if (c < 0) continue;
+      double w = P.w[4 * f + kk];
+      for (int q = 0; q < 3; ++q) rc[3 * c + q] += w * (b[3 * f + q] - Ax[3 * f + q]);
+    }
+  }
+  for (int c = 0; c < C.N; ++c)
+    if (C.fixed[c]) rc[3 * c] = rc[3 * c + 1] = rc[3 * c + 2] = 0;
+  std::vector<double> xc(3 * static_cast<size_t>(C.N), 0.0);
+  vcycle(levels, k + 1, xc.data(), rc.data());
+  for (int f = 0; f < A.N; ++f) {
+    if (A.fixed[f]) continue;
+    for (int kk = 0; kk < 4; ++kk) {
+      int c = P.idx[4 * f + kk];
+      if (c < 0) continue;
+      double w = P.w[4 * f + kk];
+      for (int q = 0; q < 3; ++q) x[3 * f + q] += w * xc[3 * c + q];
+    }
+  }
+  smoothLines(A, x, b, true, colors);
+}
+
+// Deterministic dot product: fixed 64 chunks summed in order, independent of the thread count.
+double dotv(const double* a, const double* b, size_t n) {
+  const int CH = 64;
+  double part[CH];
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < CH; ++c) {
+    size_t lo = n * c / CH, hi = n * (c + 1) / CH;
+    double s = 0;
+    for (size_t q = lo; q < hi; ++q) s += a[q] * b[q];
+    part[c] = s;
+  }
+  double s = 0;
+  for (int c = 0; c < CH; ++c) s += part[c];
+  return s;
+}
+
+// pcg (newtonMultigrid.ts:537-576) with the relative-residual stop (extension).
+void Solver::pcg(const std::vector<MGLevel>& levels, const double* b, double* x, int iterations, double tol, int* done,
+                 double* relOut) const {
+  const StencilOperator& A = *levels[0].A;
+  size_t n = 3 * static_cast<size_t>(A.N);
+  std::vector<double> r(n), Ap(n), z(n, 0.0), p(n);
+  A.apply(x, Ap.data());
+  for (size_t q = 0; q < n; ++q) r[q] = b[q] - Ap[q];
+  for (int m = 0; m < A.N; ++m)
+    if (A.fixed[m]) r[3 * m] = r[3 * m + 1] = r[3 * m + 2] = 0;
+  double r0 = std::sqrt(dotv(r.data(), r.data(), n));
+  double rel = 1;
+  int it = 0;
+  if (tol > 0 && !(r0 > 0)) {
+    if (done) *done = 0;
+    if (relOut) *relOut = 0;
+    return;
+  }
+  vcycle(levels, 0, z.data(), r.data());
+  p = z;
+  double rz = dotv(r.data(), z.data(), n);
+  for (it = 0; it < iterations; ++it) {
+    A.apply(p.data(), Ap.data());
+    for (int m = 0; m < A.N; ++m)
+      if (A.fixed[m]) Ap[3 * m] = Ap[3 * m + 1] = Ap[3 * m + 2] = 0;
+    double pAp = dotv(p.data(), Ap.data(), n);
+    if (!(pAp > 0)) break;
+    double alpha = rz / pAp;
+    for (size_t q = 0; q < n; ++q) {
+      x[q] += alpha * p[q];
+      r[q] -= alpha * Ap[q];
+    }
+    if (tol > 0) {
+      rel = std::sqrt(dotv(r.data(), r.data(), n)) / r0;
+      if (rel <= tol) {
+        it++;
+        break;
+      }
+    }
+    if (it + 1 == iterations) {
+      it++;
+      break;
+    }
+    std::fill(z.begin(), z.end(), 0.0);
+    vcycle(levels, 0, z.data(), r.data());
+    double rz2 = dotv(r.data(), z.data(), n);
+    double beta = rz2 / rz;
+    rz = rz2;
+    for (size_t q = 0; q < n; ++q) p[q] = z[q] + beta * p[q];
+  }
+  if (tol <= 0 && r0 > 0) rel = std::sqrt(dotv(r.data(), r.data(), n)) / r0;
+  if (done) *done = it;
+  if (relOut) *relOut = rel;
+}
+
+// chooseStep (newtonMultigrid.ts:597-603).
+double chooseStep(const double* e, const double* m) {
+  int best = 0;
+  for (int k = 1; k < 4; ++k)
+    if (e[k] < e[best]) best = k;
+  if (e[best] < -LINE_NOISE * m[best]) return LINE_ALPHAS[best];
+  bool all = true;
+  for (int k = 0; k < 4; ++k) all = all && e[k] > LINE_NOISE * m[k];
+  if (all) return 0;
+  return 1;
+}
+
+// newtonStepPCG (newtonMultigrid.ts:610-645).
+double Solver::newtonStep(int* pcgDone, double* rel, double* alphaOut) {
+  auto A = assembleFineOperator();
+  std::vector<double> b(3 * static_cast<size_t>(N));
+  rhs(b.data());
+  std::vector<MGLevel> levels;
+  if (prm.lag_coarse && !lagged.empty()) {
+    levels = lagged;
+    levels[0] = {A, lagged[0].P};
+  } else {
+    levels = buildHierarchy(A);
+    if (prm.lag_coarse) lagged = levels;
+  }
+  stageLevels = levels;
+  std::vector<double> d(3 * static_cast<size_t>(N), 0.0);
+  pcg(levels, b.data(), d.data(), prm.pcg_iterations, prm.pcg_rel_tol, pcgDone, rel);
+  double alpha = 1;
+  if (prm.line_search) {
+    double e[4], mag[4];
+    energyChange(d.data(), e, mag);
+    alpha = chooseStep(e, mag);
+  }
+  double m = 0;
+  for (size_t q = 0; q < d.size(); ++q) {
+    d[q] *= alpha;
+    dx[q] += d[q];
+    m = std::max(m, std::fabs(d[q]));
+  }
+  for (int n = 0; n < N; ++n) lastUpdate[n] = hyp3(d[3 * n], d[3 * n + 1], d[3 * n + 2]);
+  if (alphaOut) *alphaOut = alpha;
+  return m;
+}
+
+Yarn toYarn(const btd_yarn& y) {
+  return {y.ea_low, y.ea_high, y.crimp_strain, y.ea_compress, y.axial_viscosity, y.bend_rigidity, y.bend_viscosity,
+          y.softening_opening, y.yarns_per_span > 0 ? y.yarns_per_span : 1};
+}
+
+}  // namespace
+
+struct ora_solver {
+  Solver s;
+};
+
+extern "C" {
+
+const char* ora_last_error(void) { return g_err.c_str(); }
+
+ora_solver* ora_create(const btd_scene* sc, const ora_params* p) {
+  try {
+    if (!sc || !p) throw std::runtime_error("null scene or params");
+    auto* o = new ora_solver();
+    Solver& S = o->s;
+    S.prm = *p;
+    if (p->threads > 0) omp_set_num_threads(p->threads);
+    int N = sc->node_count, C = sc->crossing_count;
+    S.N = N;
+    S.C = C;
+    for (int l = 0; l < sc->n_layers; ++l) {
+      const btd_layer_info& L = sc->layers[l];
+      Layer o2{};
+      o2.index = L.index;
+      o2.nx = L.nx;
+      o2.ny = L.ny;
+      o2.nodeOffset = L.node_offset;
+      o2.fOffset = L.field_offset;
+      o2.K = L.field_k;
+      o2.M = L.field_m;
+      o2.bu = L.bundle[0];
+      o2.bv = L.bundle[1];
+      o2.yarns[0] = toYarn(L.material.yarns[0]);
+      o2.yarns[1] = toYarn(L.material.yarns[1]);
+      o2.pitchU = L.material.pitch_u;
+      o2.pitchV = L.material.pitch_v;
+      o2.weavePitchU = L.weave.pitch_u;
+      o2.weavePitchV = L.weave.pitch_v;
+      o2.shearStiffness = L.material.shear_stiffness;
+      o2.crossingFriction = L.material.crossing_friction;
+      o2.crossingNormal0 = L.material.crossing_normal0;
+      o2.crossingWrap = L.material.crossing_wrap;
+      o2.airDrag = L.material.air_drag;
+      o2.thickness = L.material.thickness;
+      S.layers.push_back(o2);
+    }
+    S.mass.assign(sc->mass, sc->mass + N);
+    S.crossingNormal0.assign(sc->crossing_normal0, sc->crossing_normal0 + N);
+    S.softening.assign(sc->softening, sc->softening + 2 * size_t(N));
+    S.pinned.assign(sc->pinned, sc->pinned + N);
+    S.fieldStrength.assign(sc->field_strength, sc->field_strength + 2 * size_t(C));
+    S.fieldArea.assign(sc->field_area, sc->field_area + 2 * size_t(C));
+    S.fieldDamage.assign(sc->field_damage, sc->field_damage + 2 * size_t(C));
+    S.x.assign(sc->position, sc->position + 3 * size_t(N));
+    S.v.assign(3 * size_t(N), 0.0);
+    S.dx.assign(3 * size_t(N), 0.0);
+    S.pred.assign(3 * size_t(N), 0.0);
+    S.restLength.assign(sc->rest_length, sc->rest_length + 2 * size_t(N));
+    S.intact.assign(sc->intact, sc->intact + 2 * size_t(N));
+    S.cutMask.assign(sc->cut_mask, sc->cut_mask + 2 * size_t(N));
+    S.failSite.assign(sc->fail_site, sc->fail_site + 2 * size_t(N));
+    S.segFlags.assign(sc->seg_flags, sc->seg_flags + 2 * size_t(N));
+    S.tails.assign(sc->tails, sc->tails + 4 * size_t(N));
+    S.strain.assign(2 * size_t(N), 0.0);
+    S.lastUpdate.assign(N, 0.0);
+    S.nbr.assign(4 * size_t(N), -1);
+    S.layerOf.assign(N, 0);
+    S.gripOf.assign(N, {});
+    for (size_t l = 0; l < S.layers.size(); ++l) {
+      const Layer& L = S.layers[l];
+      for (int j = 0; j < L.ny; ++j)
+        for (int i = 0; i < L.nx; ++i) {
+          int n = L.nodeOffset + j * L.nx + i;
+          S.layerOf[n] = static_cast<int>(l);
+          if (i > 0) S.nbr[4 * n + 0] = n - 1;
+          if (i < L.nx - 1) S.nbr[4 * n + 1] = n + 1;
+          if (j > 0) S.nbr[4 * n + 2] = n - L.nx;
+          if (j < L.ny - 1) S.nbr[4 * n + 3] = n + L.nx;
+        }
+    }
+    return o;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return nullptr;
+  }
+}
+
+void ora_destroy(ora_solver* s) { delete s; }
+
+int ora_set_state(ora_solver* o, const double* x, const double* v) {
+  Solver& S = o->s;
+  if (x) std::copy(x, x + 3 * size_t(S.N), S.x.begin());
+  if (v)
+    std::copy(v, v + 3 * size_t(S.N), S.v.begin());
+  else
+    std::fill(S.v.begin(), S.v.end(), 0.0);
+  return 0;
+}
+int ora_get_state(ora_solver* o, double* x, double* v, double* dx, double* pred) {
+  Solver& S = o->s;
+  if (x) std::copy(S.x.begin(), S.x.end(), x);
+  if (v) std::copy(S.v.begin(), S.v.end(), v);
+  if (dx) std::copy(S.dx.begin(), S.dx.end(), dx);
+  if (pred) std::copy(S.pred.begin(), S.pred.end(), pred);
+  return 0;
+}
+int ora_set_dx(ora_solver* o, const double* dx, const double* pred) {
+  Solver& S = o->s;
+  if (dx) std::copy(dx, dx + 3 * size_t(S.N), S.dx.begin());
+  if (pred) std::copy(pred, pred + 3 * size_t(S.N), S.pred.begin());
+  return 0;
+}
+int ora_set_segments(ora_solver* o, const double* rest, const double* intact, const uint32_t* cut, const uint16_t* flags,
+                     const double* fail, const double* tails) {
+  Solver& S = o->s;
+  size_t n2 = 2 * size_t(S.N);
+  if (rest) std::copy(rest, rest + n2, S.restLength.begin());
+  if (intact) std::copy(intact, intact + n2, S.intact.begin());
+  if (cut) std::copy(cut, cut + n2, S.cutMask.begin());
+  if (flags) std::copy(flags, flags + n2, S.segFlags.begin());
+  if (fail) std::copy(fail, fail + n2, S.failSite.begin());
+  if (tails) std::copy(tails, tails + 4 * size_t(S.N), S.tails.begin());
+  return 0;
+}
+int ora_get_segments(ora_solver* o, double* rest, double* intact, uint32_t* cut, uint16_t* flags, double* fail,
+                     double* tails) {
+  Solver& S = o->s;
+  if (rest) std::copy(S.restLength.begin(), S.restLength.end(), rest);
+  if (intact) std::copy(S.intact.begin(), S.intact.end(), intact);
+  if (cut) std::copy(S.cutMask.begin(), S.cutMask.end(), cut);
+  if (flags) std::copy(S.segFlags.begin(), S.segFlags.end(), flags);
+  if (fail) std::copy(S.failSite.begin(), S.failSite.end(), fail);
+  if (tails) std::copy(S.tails.begin(), S.tails.end(), tails);
+  return 0;
+}
+int ora_set_field(ora_solver* o, const uint8_t* d) {
+  std::copy(d, d + o->s.fieldDamage.size(), o->s.fieldDamage.begin());
+  return 0;
+}
+int ora_get_field(ora_solver* o, uint8_t* d) {
+  std::copy(o->s.fieldDamage.begin(), o->s.fieldDamage.end(), d);
+  return 0;
+}
+int ora_set_history(ora_solver* o, int32_t on) {
+  o->s.historyEnabled = on != 0;
+  return 0;
+}
+int ora_counts(ora_solver* o, int32_t* broken, int32_t* pulled) {
+  if (broken) *broken = o->s.brokenCount;
+  if (pulled) *pulled = o->s.pulledOutCount;
+  return 0;
+}
+int ora_clear_grips(ora_solver* o) {
+  o->s.grips.clear();
+  for (auto& g : o->s.gripOf) g.clear();
+  return 0;
+}
+int ora_add_grip(ora_solver* o, const int32_t* nodes, const double* w, const double* offset, int32_t count, const double* goal,
+                 double k) {
+  Solver& S = o->s;
+  Grip G;
+  G.nodes.assign(nodes, nodes + count);
+  G.w.assign(w, w + count);
+  G.offset.assign(offset, offset + 3 * size_t(count));
+  for (int q = 0; q < 3; ++q) G.goal[q] = goal[q];
+  G.k = k;
+  int gi = static_cast<int>(S.grips.size());
+  for (int e = 0; e < count; ++e) {
+    if (nodes[e] < 0 || nodes[e] >= S.N) return -1;
+    S.gripOf[nodes[e]].push_back({gi, e});
+  }
+  S.grips.push_back(G);
+  return gi;
+}
+int ora_set_grip_goal(ora_solver* o, int32_t grip, const double* goal) {
+  if (grip < 0 || grip >= static_cast<int>(o->s.grips.size())) return -1;
+  for (int q = 0; q < 3; ++q) o->s.grips[grip].goal[q] = goal[q];
+  return 0;
+}
+int ora_set_floor(ora_solver* o, int32_t enabled, double z, double bulge, double stiffness, double friction,
+                  double friction_speed) {
+  FloorParams& F = o->s.floor;
+  F.on = enabled != 0;
+  F.z = z;
+  F.bulge = bulge;
+  F.stiffness = stiffness;
+  F.friction = friction;
+  F.frictionSpeed = friction_speed;
+  return 0;
+}
+int ora_predict(ora_solver* o) {
+  o->s.predict();
+  return 0;
+}
+int ora_newton_step(ora_solver* o, double* maxUpdate, int32_t* pcgIt, double* rel, double* alpha) {
+  try {
+    int done = 0;
+    double r = 0, a = 1;
+    double m = o->s.newtonStep(&done, &r, &a);
+    if (maxUpdate) *maxUpdate = m;
+    if (pcgIt) *pcgIt = done;
+    if (rel) *rel = r;
+    if (alpha) *alpha = a;
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+int ora_finalize(ora_solver* o) {
+  o->s.finalize();
+  return 0;
+}
+int ora_substep(ora_solver* o) {
+  try {
+    o->s.predict();
+    for (int it = 0; it < o->s.prm.newton_iterations; ++it) {
+      int d;
+      double r, a;
+      o->s.newtonStep(&d, &r, &a);
+    }
+    o->s.finalize();
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+int ora_node_gradient(ora_solver* o, int32_t n, double* g) {
+  o->s.nodeGradient(n, g);
+  return 0;
+}
+double ora_potential(ora_solver* o) { return o->s.potential(); }
+int ora_energy_change(ora_solver* o, const double* d, double* e4, double* m4) {
+  o->s.energyChange(d, e4, m4);
+  return 0;
+}
+double ora_yarn_material_length(ora_solver* o) { return o->s.yarnMaterialLength(); }
+
+int ora_assemble(ora_solver* o, double* A, uint8_t* fixed, double* b) {
+  try {
+    auto op = o->s.assembleFineOperator();
+    if (A) std::copy(op->A.begin(), op->A.end(), A);
+    if (fixed) std::copy(op->fixed.begin(), op->fixed.end(), fixed);
+    if (b) o->s.rhs(b);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+int ora_build_levels(ora_solver* o, const double* A) {
+  try {
+    auto op = o->s.assembleFineOperator();
+    if (A) std::copy(A, A + op->A.size(), op->A.begin());
+    o->s.stageLevels = o->s.buildHierarchy(op);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+int ora_level_count(ora_solver* o) { return static_cast<int>(o->s.stageLevels.size()); }
+int ora_level_nodes(ora_solver* o, int32_t k) {
+  if (k < 0 || k >= static_cast<int>(o->s.stageLevels.size())) return -1;
+  return o->s.stageLevels[k].A->N;
+}
+int ora_read_level(ora_solver* o, int32_t k, double* A, uint8_t* fixed) {
+  if (k < 0 || k >= static_cast<int>(o->s.stageLevels.size())) return -1;
+  const StencilOperator& op = *o->s.stageLevels[k].A;
+  if (A) std::copy(op.A.begin(), op.A.end(), A);
+  if (fixed) std::copy(op.fixed.begin(), op.fixed.end(), fixed);
+  return 0;
+}
+int ora_read_prolongation(ora_solver* o, int32_t k, int32_t* idx, double* w) {
+  if (k < 0 || k >= static_cast<int>(o->s.stageLevels.size()) || !o->s.stageLevels[k].P) return -1;
+  const Prolongation& P = *o->s.stageLevels[k].P;
+  if (idx) std::copy(P.idx.begin(), P.idx.end(), idx);
+  if (w) std::copy(P.w.begin(), P.w.end(), w);
+  return 0;
+}
+int ora_apply(ora_solver* o, int32_t k, const double* x, double* y) {
+  if (k < 0 || k >= static_cast<int>(o->s.stageLevels.size())) return -1;
+  o->s.stageLevels[k].A->apply(x, y);
+  return 0;
+}
+int ora_smooth(ora_solver* o, int32_t k, double* x, const double* b, int32_t reverse) {
+  if (k < 0 || k >= static_cast<int>(o->s.stageLevels.size())) return -1;
+  smoothLines(*o->s.stageLevels[k].A, x, b, reverse != 0, o->s.prm.line_colors);
+  return 0;
+}
+int ora_vcycle(ora_solver* o, const double* b, double* z) {
+  if (o->s.stageLevels.empty()) return -1;
+  o->s.vcycle(o->s.stageLevels, 0, z, b);
+  return 0;
+}
+int ora_pcg(ora_solver* o, const double* b, double* x, int32_t iterations, double tol, int32_t* done, double* rel) {
+  if (o->s.stageLevels.empty()) return -1;
+  int d = 0;
+  double r = 0;
+  o->s.pcg(o->s.stageLevels, b, x, iterations, tol, &d, &r);
+  if (done) *done = d;
+  if (rel) *rel = r;
+  return 0;
+}
+int ora_solve_penta(int32_t n, const double* D, const double* E, const double* F, const double* r, double* x, double shift) {
+  solvePenta(n, D, E, F, r, x, shift);
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,104 @@
+/*
+ * oracle.h - TEST INFRASTRUCTURE ONLY. The FP64 CPU restatement of the reference's own solver
+ * (src/simulation/reference/{solver,newtonMultigrid}.ts with laws.ts, axial.ts, lattice.ts and
+ * yarnField.ts). It is the correctness oracle for the CUDA path and the timed CPU baseline; only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it. The product library
+ * never links or calls it.
+ *
+ * Parity is pinned by restating the reference's own property tests (tests/unit/newtonMultigrid.test.ts,
+ * referenceSolver.test.ts, yarnField.test.ts, laws.test.ts, axial.test.ts) against this code; the
+ * reference ships no golden vectors for the solve.
+ *
+ * Extensions flagged as not in the reference: a PCG relative-residual stop, several grips, the
+ * floor contact of the GPU shaders restated on the CPU.
+ */
+#ifndef BTD_ORACLE_H
+#define BTD_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "btd.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ora_params {
+  double h;
+  double gravity[3];
+  int32_t newton_iterations;
+  int32_t pcg_iterations;    /* fixed count, or the cap when pcg_rel_tol > 0 */
+  double pcg_rel_tol;        /* extension: stop at ||r_k|| / ||r_0|| <= tol */
+  int32_t max_coarsest_nodes;/* MGConfig (newtonMultigrid.ts:20-34) */
+  int32_t coarse_sweeps;
+  int32_t line_colors;
+  int32_t lag_coarse;
+  int32_t line_search;
+  int32_t threads;           /* OpenMP threads (0: all) */
+} ora_params;
+
+typedef struct ora_solver ora_solver;
+
+ora_solver* ora_create(const btd_scene* scene, const ora_params* params);
+void ora_destroy(ora_solver* s);
+const char* ora_last_error(void);
+
+/* ReferenceSolver state (solver.ts(ref):41-119); 3 doubles per node. */
+int ora_set_state(ora_solver* s, const double* x, const double* v);
+int ora_get_state(ora_solver* s, double* x, double* v, double* dx, double* pred);
+int ora_set_dx(ora_solver* s, const double* dx, const double* pred);
+int ora_set_segments(ora_solver* s, const double* rest, const double* intact, const uint32_t* cut_mask,
+                     const uint16_t* flags, const double* fail_site, const double* tails);
+int ora_get_segments(ora_solver* s, double* rest, double* intact, uint32_t* cut_mask, uint16_t* flags,
+                     double* fail_site, double* tails);
+int ora_set_field(ora_solver* s, const uint8_t* damage);
+int ora_get_field(ora_solver* s, uint8_t* damage);
+int ora_set_history(ora_solver* s, int32_t on);
+int ora_counts(ora_solver* s, int32_t* broken, int32_t* pulled);
+
+/* Grips (ReferenceGrip, solver.ts(ref):29-37), any number (extension: the reference has one). */
+int ora_clear_grips(ora_solver* s);
+int ora_add_grip(ora_solver* s, const int32_t* nodes, const double* w, const double* offset, int32_t count,
+                 const double* goal, double k);
+int ora_set_grip_goal(ora_solver* s, int32_t grip, const double* goal);
+/* Floor (GPU shader math, common.wgsl:251-270, restated; extension). */
+int ora_set_floor(ora_solver* s, int32_t enabled, double z, double bulge, double stiffness, double friction,
+                  double friction_speed);
+
+/* Substep and its parts (solver.ts(ref):602-632, newtonMultigrid.ts:610-645). */
+int ora_predict(ora_solver* s);
+int ora_newton_step(ora_solver* s, double* max_update, int32_t* pcg_iterations, double* rel_residual,
+                    double* alpha);
+int ora_finalize(ora_solver* s);
+int ora_substep(ora_solver* s);
+
+/* Energies (solver.ts(ref):387-595). */
+int ora_node_gradient(ora_solver* s, int32_t n, double* g3);
+double ora_potential(ora_solver* s);
+int ora_energy_change(ora_solver* s, const double* d, double* e4, double* m4);
+double ora_yarn_material_length(ora_solver* s);
+
+/* Multigrid stages on the solver's current system (newtonMultigrid.ts:169-576). A: N*25*9. */
+int ora_assemble(ora_solver* s, double* A, uint8_t* fixed, double* b);
+/* Build the hierarchy from a given fine operator (the current state's links), as correctness.ts does. */
+int ora_build_levels(ora_solver* s, const double* A_fine);
+int ora_level_count(ora_solver* s);
+int ora_level_nodes(ora_solver* s, int32_t level);
+int ora_read_level(ora_solver* s, int32_t level, double* A, uint8_t* fixed);
+int ora_read_prolongation(ora_solver* s, int32_t level, int32_t* idx, double* w);
+int ora_apply(ora_solver* s, int32_t level, const double* x, double* y);
+int ora_smooth(ora_solver* s, int32_t level, double* x, const double* b, int32_t reverse);
+int ora_vcycle(ora_solver* s, const double* b, double* z);
+int ora_pcg(ora_solver* s, const double* b, double* x, int32_t iterations, double rel_tol, int32_t* done,
+            double* rel_residual);
+
+/* Block pentadiagonal solve (newtonMultigrid.ts:435-473). */
+int ora_solve_penta(int32_t n, const double* D, const double* E, const double* F, const double* r, double* x,
+                    double shift);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
