@@ -1,0 +1,275 @@
+#!/usr/bin/env python
+"""Benchmark: Newton steps/s of the implicit cloth solve at relative residual 1e-6 on B200.
+
+A step is one substep of the workload: predictor, 4 projected-Newton iterations each solved by
+Galerkin-multigrid PCG to relative residual 1e-6, line search, commit, damage field and crossing
+slip. `value` is Newton iterations per second over all ranks, timed with CUDA events on the
+solver's stream with a cold L2 before every step (a 256 MiB buffer is rewritten between steps,
+outside the timed events); `e2e` is the same metric through the public C ABI from pinned host
+buffers (state in, state out every step). One patch does not shard: with --gpus N each rank runs
+an independent replica (weak scaling) and the time is the max over ranks.
+
+--impl reference times the reference's CPU solver (its FP64 restatement: the reference is
+TypeScript and has no runnable CPU path here) on the host cores, on the same workload and metric.
+"""
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "break-that-denim_b200")
+METRIC = "Newton steps/s at rel-res 1e-6: learned-precond vs plain MG-PCG, 1 B200"
+FALLBACK_HBM_GBS = 6650.0
+
+# workloads: (lattice side, patch size m, dt, Newton iterations, relative residual)
+WORKLOADS = {
+    "hanging-256": dict(n=256, size=0.6, h=1 / 60, newton=4, rel=1e-6,
+                        desc="256x256-vertex hanging shell patch (0.6 m, config-0 material and schedule: top row pinned, "
+                             "dt 1/60, 4 projected-Newton, MG-PCG to rel-res 1e-6, no contact), seeded N(0,1e-4) jitter"),
+    "config0-64": dict(n=64, size=0.3, h=1 / 60, newton=4, rel=1e-6,
+                       desc="64x64-vertex hanging shell patch (0.3 m), dt 1/60, 4 projected-Newton, 3-level MG-PCG to rel-res 1e-6"),
+}
+DEFAULT_WORKLOAD = "hanging-256"
+MG = dict(max_coarsest_nodes=400, coarse_sweeps=2, line_colors=3, lag_coarse=True, line_search=True)
+
+
+def package():
+    if "btd_b200" in sys.modules:
+        return sys.modules["btd_b200"]
+    spec = importlib.util.spec_from_file_location("btd_b200", os.path.join(PKG, "__init__.py"), submodule_search_locations=[PKG])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["btd_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def build_scene(btd, w):
+    return btd.configs.hanging_patch(w["n"], w["size"], seed=1)
+
+
+def peaks():
+    try:
+        p = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 4 + k and r[4 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def cpu_sample(btd, w, substeps, threads=0):
+    """The oracle (the reference's CPU solver restated, FP64, OpenMP) on `substeps` substeps."""
+    sys.path.insert(0, ROOT)
+    from oracle import Oracle
+
+    sc = build_scene(btd, w)
+    o = Oracle(sc, h=w["h"], newton_iterations=w["newton"], pcg_iterations=500, pcg_rel_tol=w["rel"], threads=threads, **MG)
+    t = time.perf_counter()
+    for _ in range(substeps):
+        o.substep()
+    dt = time.perf_counter() - t
+    cores = threads if threads > 0 else (os.cpu_count() or 1)
+    return substeps * w["newton"] / dt, dt, cores
+
+
+def run_reference(args, w, rank):
+    if rank != 0:
+        return
+    btd = package()
+    for _ in range(args.warmup):
+        pass  # the CPU solver has no warm-up state worth timing; warm-up steps run inside the sample below
+    steps = max(1, args.steps)
+    value, dt, cores = cpu_sample(btd, w, steps)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Newton steps/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": {"workload": args.workload, "description": w["desc"]},
+            "cpu_baseline": {"value": value, "unit": "Newton steps/s", "cores": cores, "kind": "port",
+                             "sample": f"{steps} substeps x {w['newton']} Newton of the workload from its initial state"},
+            "e2e": {"value": value, "unit": "Newton steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    w = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, w, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    btd = package()
+    sc = build_scene(btd, w)
+    params = btd.configs.solver_params(w["h"], w["newton"], w["rel"])
+    gpu = btd.GpuSolver(sc, params)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        gpu.synchronize()
+
+    # warm-up (captures the substep graph, fills caches)
+    for _ in range(args.warmup):
+        gpu.substep()
+    gpu.synchronize()
+    gpu.clear_counters()
+
+    # ---- device-timed region: K substeps, cold L2 before each (flush outside the events)
+    barrier()
+    idx = local
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        idx = vis.split(",")[local]
+    with ClockSampler(idx) as clocks:
+        ms_step = gpu.profile_stage("substep", reps=args.steps, flush=True)
+        barrier()
+    c = gpu.counter_dict()
+    newton_total = c["newton"]
+    pcg_total = c["pcg_total"]
+    t_dev = ms_step * args.steps / 1e3
+    if dist is not None:
+        t = torch.tensor([t_dev], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev = float(t.item())
+    value = world * newton_total / t_dev
+    launches = gpu.launch_count(args.steps, newton_total, pcg_total)
+
+    # ---- end to end through the C ABI from pinned host buffers: state in, substep, state out
+    N = sc.N
+    xh = torch.empty((N, 4), dtype=torch.float32, pin_memory=True)
+    vh = torch.empty((N, 4), dtype=torch.float32, pin_memory=True)
+    lib = btd._abi.lib()
+    h = gpu._h
+    btd._abi.check("btd_get_state", h, xh.data_ptr(), vh.data_ptr())
+    gpu.clear_counters()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        btd._abi.check("btd_set_state", h, xh.data_ptr(), vh.data_ptr())
+        btd._abi.check("btd_substep", h, 0, 0)
+        btd._abi.check("btd_get_state", h, xh.data_ptr(), vh.data_ptr())
+    barrier()
+    t_e2e = time.perf_counter() - t0
+    newton_e2e = gpu.counter_dict()["newton"]
+    if dist is not None:
+        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = world * newton_e2e / t_e2e
+
+    # ---- roofline of the dominant kernel (fine-level smoother sweep), live, cold L2 per launch
+    peak, peak_kind = peaks()
+    R0 = 232.0  # fine row algorithmic bytes
+    ms_sweep = gpu.profile_stage("smooth", reps=10, flush=True)
+    bytes_sweep = 2.0 * N * (R0 + 36.0)
+    achieved = bytes_sweep / (ms_sweep / 1e3) / 1e9
+    ms_mv = gpu.profile_stage("matvec", reps=10, flush=True)
+    mv_gbs = N * (R0 + 24.0) / (ms_mv / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(args.workload, {}).get("smooth_sweep_dram_bytes")
+        except Exception:
+            traffic = None
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "Newton steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "description": w["desc"], "nodes": N, "levels": gpu.level_count(),
+                   "newton_per_step": w["newton"], "pcg_iterations_per_newton": pcg_total / max(1, newton_total),
+                   "l2": "flushed before every timed step (256 MiB rewrite outside the events)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e, "unit": "Newton steps/s", "h2d_bytes_per_step": 2 * 16 * N, "d2h_bytes_per_step": 2 * 16 * N},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": "k_smooth<FineRows> (fine yarn-line sweep, 6 colour launches)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_kind": peak_kind, "algorithmic_bytes_per_sweep": bytes_sweep, "ms_per_sweep": ms_sweep,
+                     "matvec_gbs": mv_gbs, "matvec_ms": ms_mv},
+        "clocks": clocks.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        v_cpu, dt_cpu, cores = cpu_sample(btd, w, 1)
+        line["cpu_baseline"] = {"value": v_cpu, "unit": "Newton steps/s", "cores": cores, "kind": "port",
+                                "sample": f"1 substep ({w['newton']} Newton) of the workload from its initial state, {dt_cpu:.1f} s"}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -189,6 +189,8 @@ SIGNATURES = {
     "btd_read_operator": ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p], C.c_int),
     "btd_read_vector": ([C.c_void_p, C.c_int32, C.c_int32, C.c_void_p], C.c_int),
     "btd_write_vector": ([C.c_void_p, C.c_int32, C.c_int32, C.c_void_p], C.c_int),
+    "btd_profile_stage": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, _p(C.c_float)], C.c_int),
+    "btd_launch_count": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, _p(C.c_int64)], C.c_int),
     "btd_last_error": ([C.c_char_p, C.c_size_t], C.c_int),
 }
 

@@ -1,0 +1,96 @@
+"""Synthetic workloads: the benchmark configurations mapped onto the reference's lattice model.
+
+The reference models cloth as a woven crossing lattice (src/simulation/scene.ts): one node per
+crossing, u-family spans along i (x when the layer angle is 0), v-family spans along j, per-span
+axial EA (N), a shear diagonal pair per cell (N/m), per-yarn bending rigidity B (N m^2) and a mass
+lumped per node. A shell material given per unit width maps onto it at lattice pitch p as:
+  EA (N) = stretch (N/m) * p        shear diagonal ks = shear modulus G (N/m)
+  B (N m^2) = bending (N m) * p      node mass = areal density * p^2
+The family along x (u) carries the warp stretch. Linear stretch uses eaLow = eaHigh; compression
+keeps the reference denim's ratio eaCompress / eaLow = 1/2. Viscosities and air drag are the
+reference DENIM values (material.ts:88-138). Gravity acts along the reference's vertical axis z.
+Initial jitter is N(0, sigma) per free coordinate from splitmix64 -> Box-Muller with the seed given.
+"""
+import numpy as np
+
+from . import _abi
+from .scene import compile_scene, layer_spec, material_preset
+
+U64 = np.uint64
+
+
+def splitmix64(seed, n):
+    """n 64-bit outputs of splitmix64 seeded with `seed`."""
+    with np.errstate(over="ignore"):
+        k = np.arange(1, n + 1, dtype=U64)
+        z = U64(seed) + k * U64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> U64(30))) * U64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> U64(27))) * U64(0x94D049BB133111EB)
+        return z ^ (z >> U64(31))
+
+
+def normal(seed, n):
+    """n standard normal draws (Box-Muller over splitmix64 pairs)."""
+    m = (n + 1) // 2
+    r = splitmix64(seed, 2 * m)
+    u1 = ((r[0::2] >> U64(11)).astype(np.float64) + 1.0) / 9007199254740992.0  # (0, 1]
+    u2 = (r[1::2] >> U64(11)).astype(np.float64) / 9007199254740992.0
+    rad = np.sqrt(-2.0 * np.log(u1))
+    z = np.empty(2 * m)
+    z[0::2] = rad * np.cos(2 * np.pi * u2)
+    z[1::2] = rad * np.sin(2 * np.pi * u2)
+    return z[:n]
+
+
+def shell_material(pitch, stretch=(8e3, 4e3), shear=200.0, bending=1e-5, areal_density=0.35, break_strain=0.08):
+    """A lattice material for a shell of the given per-width stiffnesses at lattice pitch `pitch`."""
+    m = material_preset(0)
+    m.name = b"shell"
+    m.pitch_u = pitch
+    m.pitch_v = pitch
+    for f in range(2):
+        y = m.yarns[f]
+        ea = stretch[f] * pitch
+        y.linear_density = 0.5 * areal_density * pitch
+        y.ea_low = ea
+        y.ea_high = ea
+        y.ea_compress = 0.5 * ea
+        y.bend_rigidity = bending * pitch
+        y.strength = ea * break_strain  # linear law: T(eps_break)
+        y.yarns_per_span = 0
+    m.shear_stiffness = shear
+    return m
+
+
+def hanging_patch(n, size=0.3, seed=1, jitter=1e-4, **mat):
+    """An n x n shell patch, top row (j = n - 1) pinned, flat plus N(0, jitter) on free coordinates."""
+    pitch = size / (n - 1)
+    m = shell_material(pitch, **mat)
+    sc = compile_scene(layer_spec(m, (n - 0.5) * pitch, (n - 0.5) * pitch, collar_rows=0, seed=seed))
+    assert sc.nx == n and sc.ny == n, (sc.nx, sc.ny)
+    pinned = np.zeros((n, n), np.uint8)
+    pinned[n - 1, :] = 1
+    sc.pinned[:] = pinned.reshape(-1)
+    free = sc.pinned == 0
+    pos = sc.position.reshape(-1, 3)
+    z = normal(seed, 3 * int(free.sum())).reshape(-1, 3)
+    pos[free] += jitter * z
+    sc.position[:] = pos.reshape(-1)
+    return sc
+
+
+# Solver schedules of the configurations.
+CONFIG0 = dict(n=64, size=0.3, h=1 / 60, newton_iterations=4, pcg_rel_tol=1e-6, steps=60, max_coarsest_nodes=400)
+
+
+def config0(seed=1):
+    """Plain method, small size: 64 x 64 hanging patch, 0.3 m, top row pinned, dt = 1/60, 4 Newton,
+    3-level MG-PCG to relative residual 1e-6, no contact, 60 steps."""
+    return hanging_patch(64, 0.3, seed=seed)
+
+
+def solver_params(h, newton_iterations, pcg_rel_tol, pcg_cap=500, **kw):
+    from .solver import default_params
+
+    return default_params(h=h, newton_iterations=newton_iterations, newton_max=newton_iterations, pcg_iterations=pcg_cap,
+                          pcg_rel_tol=pcg_rel_tol, **kw)

@@ -1,0 +1,256 @@
+// Galerkin multigrid kernels on the lattice stencils (multigrid.wgsl; newtonMultigrid.ts:282-528).
+// Each kernel is a template over the row layout of the level it reads (fine: 12 couplings with
+// scalar +-2 bending entries; coarse: the 24-coupling radius-2 stencil); coarse rows are always
+// written in the coarse layout.
+#pragma once
+
+#include "common.cuh"
+
+namespace btd {
+
+struct FineRows {
+  static constexpr int NC = 12;
+  __device__ static int2 offset(int k) { return fineOffset(k); }
+  __device__ static Sym diag(const float4* op, int N, int n) { return fineBlock(op, N, n, 0); }
+  __device__ static Sym coupling(const float4* op, int N, int n, int k) { return fineCouplingBlock(op, N, n, k); }
+  // coupling index of a unit offset (prolongation connectivity)
+  __device__ static int index(int di, int dj) { return fineCoupling(di, dj); }
+};
+struct CoarseRows {
+  static constexpr int NC = 24;
+  __device__ static int2 offset(int k) {
+    int o = k >= 12 ? k + 1 : k;
+    return make_int2(o % 5 - 2, o / 5 - 2);
+  }
+  __device__ static Sym diag(const float4* op, int N, int n) { return coarseBlock(op, N, n, 12); }
+  __device__ static Sym coupling(const float4* op, int N, int n, int k) { return coarseBlock(op, N, n, k >= 12 ? k + 1 : k); }
+  __device__ static int index(int di, int dj) {
+    int o = (dj + 2) * 5 + (di + 2);
+    return o > 12 ? o - 1 : o;
+  }
+};
+
+__device__ __forceinline__ void nodeCoord(const DLevel& L, int n, int* i, int* j, int* l) {
+  uint2 c = L.coord[n];
+  *i = c.x & 0xFFFF;
+  *j = c.x >> 16;
+  *l = c.y;
+}
+
+constexpr float LINK_MIN_INTACT = 0.02f;
+
+// Whether node (i, j) of level F and its unit-offset neighbour are connected (linked,
+// multigrid.wgsl:44-56; newtonMultigrid.ts:287-295): an intact span on the fine lattice; on coarse
+// levels a nonzero Galerkin coupling or a fixed neighbour.
+template <class Rows, bool FINE>
+__device__ __forceinline__ bool linked(const DLevel& F, const Seg* __restrict__ segs, const DLevelLayer& L, int i, int j, int di, int dj) {
+  int a = levelNode(L, i, j), b = levelNode(L, i + di, j + dj);
+  if (a < 0 || b < 0) return false;
+  if (FINE) {
+    int f = di != 0 ? 0 : 1;
+    int owner = di + dj > 0 ? a : b;
+    Seg sg = segs[2 * owner + f];
+    return segActive(sg) && sg.intact > LINK_MIN_INTACT;
+  }
+  if (F.fixed[b]) return true;
+  return !symIsZero(Rows::coupling(F.op, F.N, a, Rows::index(di, dj)));
+}
+
+// Masked, renormalised bilinear weights (prolongWeights, multigrid.wgsl:62-102; buildProlongation,
+// newtonMultigrid.ts:305-342).
+template <class Rows, bool FINE>
+__global__ void k_prolong_weights(DLevel F, const Seg* __restrict__ segs) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= F.N) return;
+  if (F.fixed[a]) {
+    F.pw[a] = make_float4(0, 0, 0, 0);
+    return;
+  }
+  int i, j, l;
+  nodeCoord(F, a, &i, &j, &l);
+  const DLevelLayer L = F.layers[l];
+  Bracket bi = bracketOf(i, L.nx), bj = bracketOf(j, L.ny);
+  float w[4] = {0, 0, 0, 0};
+  float sum = 0.f;
+  for (int kj = 0; kj < 2; ++kj) {
+    int J = kj ? bj.hi : bj.lo;
+    float wj = kj ? bj.whi : bj.wlo;
+    if (wj == 0.f) continue;
+    int dj = coarseToFine(J, L.ny) - j;
+    for (int ki = 0; ki < 2; ++ki) {
+      int I = ki ? bi.hi : bi.lo;
+      float wi = ki ? bi.whi : bi.wlo;
+      if (wi == 0.f) continue;
+      int di = coarseToFine(I, L.nx) - i;
+      bool ok = true;
+      if (di != 0 && dj != 0) {
+        ok = (linked<Rows, FINE>(F, segs, L, i, j, di, 0) && linked<Rows, FINE>(F, segs, L, i + di, j, 0, dj)) ||
+             (linked<Rows, FINE>(F, segs, L, i, j, 0, dj) && linked<Rows, FINE>(F, segs, L, i, j + dj, di, 0));
+      } else if (di != 0 || dj != 0) {
+        ok = linked<Rows, FINE>(F, segs, L, i, j, di, dj);
+      }
+      if (ok) {
+        w[ki + 2 * kj] = wi * wj;
+        sum += wi * wj;
+      }
+    }
+  }
+  F.pw[a] = sum > 0.f ? make_float4(w[0] / sum, w[1] / sum, w[2] / sum, w[3] / sum) : make_float4(0, 0, 0, 0);
+}
+
+// Bilinear (unmasked) weight of fine index i in coarse index I, 0 outside its bracket.
+__device__ __forceinline__ float weightOf(int i, int I, int n) {
+  Bracket b = bracketOf(i, n);
+  if (b.lo == I) return b.wlo;
+  if (b.hi == I && b.whi > 0.f) return b.whi;
+  return 0.f;
+}
+__device__ __forceinline__ float pwSlot(float4 w, int s) { return s == 0 ? w.x : s == 1 ? w.y : s == 2 ? w.z : w.w; }
+
+constexpr int RAP_THREADS = 64;
+
+// Galerkin coarse row P^T A P of coarse node I (rap, multigrid.wgsl:115-178; galerkin,
+// newtonMultigrid.ts:345-387). One thread per coarse node; its 25 accumulators live in shared memory.
+template <class Rows>
+__global__ void __launch_bounds__(RAP_THREADS) k_rap(DLevel F, DLevel C) {
+  __shared__ float acc[RAP_THREADS][153];  // odd stride: conflict-free per-thread rows
+  int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= C.N) return;
+  float* a25 = acc[threadIdx.x];
+  for (int q = 0; q < 150; ++q) a25[q] = 0.f;
+  int ci, cj, l;
+  nodeCoord(C, I, &ci, &cj, &l);
+  const DLevelLayer Lf = F.layers[l];
+  const int nxf = Lf.nx, nyf = Lf.ny;
+  const int fi0 = coarseToFine(ci, nxf), fj0 = coarseToFine(cj, nyf);
+  for (int aj = fj0 - 1; aj <= fj0 + 1; ++aj) {
+    if (aj < 0 || aj >= nyf) continue;
+    if (weightOf(aj, cj, nyf) == 0.f) continue;
+    for (int ai = fi0 - 1; ai <= fi0 + 1; ++ai) {
+      if (ai < 0 || ai >= nxf) continue;
+      if (weightOf(ai, ci, nxf) == 0.f) continue;
+      int a = levelNode(Lf, ai, aj);
+      if (F.fixed[a]) continue;
+      Bracket bai = bracketOf(ai, nxf), baj = bracketOf(aj, nyf);
+      float wa = pwSlot(F.pw[a], (bai.lo == ci ? 0 : 1) + 2 * (baj.lo == cj ? 0 : 1));
+      if (wa == 0.f) continue;
+      for (int k = 0; k <= Rows::NC; ++k) {
+        int2 off = make_int2(0, 0);
+        Sym Ab;
+        if (k == Rows::NC) {
+          Ab = Rows::diag(F.op, F.N, a);
+        } else {
+          off = Rows::offset(k);
+          Ab = Rows::coupling(F.op, F.N, a, k);
+        }
+        if (symIsZero(Ab)) continue;
+        int bi = ai + off.x, bj = aj + off.y;
+        if (bi < 0 || bj < 0 || bi >= nxf || bj >= nyf) continue;
+        Bracket bri = bracketOf(bi, nxf), brj = bracketOf(bj, nyf);
+        float4 wb = F.pw[levelNode(Lf, bi, bj)];
+        for (int kj = 0; kj < 2; ++kj) {
+          int J = kj ? brj.hi : brj.lo;
+          for (int ki = 0; ki < 2; ++ki) {
+            int Ii = ki ? bri.hi : bri.lo;
+            float wJ = pwSlot(wb, ki + 2 * kj);
+            if (wJ == 0.f) continue;
+            int o = (J - cj + 2) * 5 + (Ii - ci + 2);
+            float s = wa * wJ;
+            float* p = a25 + 6 * o;
+            p[0] += Ab.xx * s, p[1] += Ab.xy * s, p[2] += Ab.xz * s, p[3] += Ab.yy * s, p[4] += Ab.yz * s, p[5] += Ab.zz * s;
+          }
+        }
+      }
+    }
+  }
+  const float* c = a25 + 6 * 12;
+  bool fixedRow = c[0] + c[3] + c[5] <= 0.f;
+  if (fixedRow) {
+    for (int q = 0; q < 150; ++q) a25[q] = 0.f;
+    a25[72] = 1.f, a25[75] = 1.f, a25[77] = 1.f;
+  }
+  for (int p = 0; p < COARSE_PLANES; ++p) {
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = 4 * p + q < 150 ? a25[4 * p + q] : 0.f;
+    C.op[(size_t)p * C.N + I] = make_float4(v[0], v[1], v[2], v[3]);
+  }
+  C.fixed[I] = fixedRow ? 1u : 0u;
+}
+
+// r = b - A x on level F (residual, multigrid.wgsl:182-199); fixed rows give 0.
+template <class Rows>
+__global__ void k_residual(DLevel F) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= F.N) return;
+  if (F.fixed[n]) {
+    F.R[n] = make_float4(0, 0, 0, 0);
+    return;
+  }
+  int i, j, l;
+  nodeCoord(F, n, &i, &j, &l);
+  const DLevelLayer L = F.layers[l];
+  float3 r = f3(F.B[n]) - Rows::diag(F.op, F.N, n) * f3(F.X[n]);
+#pragma unroll 4
+  for (int k = 0; k < Rows::NC; ++k) {
+    int2 off = Rows::offset(k);
+    int m = levelNode(L, i + off.x, j + off.y);
+    if (m < 0) continue;
+    r -= Rows::coupling(F.op, F.N, n, k) * f3(F.X[m]);
+  }
+  F.R[n] = make_float4(r.x, r.y, r.z, 0.f);
+}
+
+// b_c = P^T r_f and x_c = 0 (restrictResidual, multigrid.wgsl:204-232).
+__global__ void k_restrict(DLevel F, DLevel C) {
+  int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= C.N) return;
+  C.X[I] = make_float4(0, 0, 0, 0);
+  if (C.fixed[I]) {
+    C.B[I] = make_float4(0, 0, 0, 0);
+    return;
+  }
+  int ci, cj, l;
+  nodeCoord(C, I, &ci, &cj, &l);
+  const DLevelLayer Lf = F.layers[l];
+  int fi0 = coarseToFine(ci, Lf.nx), fj0 = coarseToFine(cj, Lf.ny);
+  float3 s = make_float3(0, 0, 0);
+  for (int aj = fj0 - 1; aj <= fj0 + 1; ++aj) {
+    if (aj < 0 || aj >= Lf.ny || weightOf(aj, cj, Lf.ny) == 0.f) continue;
+    for (int ai = fi0 - 1; ai <= fi0 + 1; ++ai) {
+      if (ai < 0 || ai >= Lf.nx || weightOf(ai, ci, Lf.nx) == 0.f) continue;
+      int a = levelNode(Lf, ai, aj);
+      if (F.fixed[a]) continue;
+      Bracket bai = bracketOf(ai, Lf.nx), baj = bracketOf(aj, Lf.ny);
+      float w = pwSlot(F.pw[a], (bai.lo == ci ? 0 : 1) + 2 * (baj.lo == cj ? 0 : 1));
+      s += w * f3(F.R[a]);
+    }
+  }
+  C.B[I] = make_float4(s.x, s.y, s.z, 0.f);
+}
+
+// x_f += P x_c (prolongAdd, multigrid.wgsl:237-258).
+__global__ void k_prolong(DLevel F, DLevel C) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= F.N || F.fixed[a]) return;
+  int i, j, l;
+  nodeCoord(F, a, &i, &j, &l);
+  const DLevelLayer Lf = F.layers[l];
+  const DLevelLayer Lc = C.layers[l];
+  Bracket bi = bracketOf(i, Lf.nx), bj = bracketOf(j, Lf.ny);
+  float4 w = F.pw[a];
+  float3 s = make_float3(0, 0, 0);
+  for (int kj = 0; kj < 2; ++kj) {
+    int J = kj ? bj.hi : bj.lo;
+    for (int ki = 0; ki < 2; ++ki) {
+      int Ii = ki ? bi.hi : bi.lo;
+      float wk = pwSlot(w, ki + 2 * kj);
+      if (wk == 0.f) continue;
+      s += wk * f3(C.X[levelNode(Lc, Ii, J)]);
+    }
+  }
+  float4 x = F.X[a];
+  F.X[a] = make_float4(x.x + s.x, x.y + s.y, x.z + s.z, 0.f);
+}
+
+}  // namespace btd

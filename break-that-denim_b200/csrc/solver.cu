@@ -1,0 +1,1094 @@
+// Host side of the CUDA solve: the B200 counterpart of the reference's GpuSolver
+// (src/simulation/gpu/solver.ts:194-838) behind the C ABI of include/btd.h.
+//
+// A solver owns its device memory and one CUDA stream. A substep (encodeSubstep, solver.ts:737-760)
+// is captured once into a CUDA graph: predictor, Newton iterations (assembly, Galerkin hierarchy on
+// the first iteration, PCG with a V-cycle preconditioner, line search, bounded update), commit,
+// damage field and crossing slip. PCG's convergence test runs on the device and drives a graph
+// while-node, so a whole substep is one graph launch with no host round trip.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "btd.h"
+#include "common.cuh"
+#include "k_history.cuh"
+#include "k_mg.cuh"
+#include "k_pcg.cuh"
+#include "k_smooth.cuh"
+#include "k_step.cuh"
+
+namespace btd {
+void setError(const std::string& msg);
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+#define CK(call)                                                                                            \
+  do {                                                                                                      \
+    cudaError_t e_ = (call);                                                                                \
+    if (e_ != cudaSuccess) throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+static int blocksFor(int n, int t) { return (n + t - 1) / t; }
+
+// ------------------------------------------------------------------------------------------ levels
+
+struct Level {
+  int N = 0;
+  bool fine = false;
+  std::vector<DLevelLayer> layers;
+  std::vector<int4> lines;  // (start, stride, length, family) grouped by colour
+  int colourStart[7] = {0, 0, 0, 0, 0, 0, 0};
+  int maxLine = 0;
+  DLevelLayer* dLayers = nullptr;
+  uint2* dCoord = nullptr;
+  int4* dLines = nullptr;
+  float4* op = nullptr;
+  uint32_t* fixed = nullptr;
+  float4 *X = nullptr, *B = nullptr, *R = nullptr, *pw = nullptr;
+  DLevel dev() const {
+    DLevel d;
+    d.N = N;
+    d.nLayers = (int)layers.size();
+    d.layers = dLayers;
+    d.coord = dCoord;
+    d.op = op;
+    d.fixed = fixed;
+    d.X = X;
+    d.B = B;
+    d.R = R;
+    d.pw = pw;
+    return d;
+  }
+};
+
+// Line tables (lineTable, lattice.ts:330-350): v-lines coloured i mod 3, then u-lines j mod 3.
+static void buildLines(Level& L) {
+  std::vector<int4> byColour[6];
+  for (auto& ly : L.layers) {
+    for (int i = 0; i < ly.nx; ++i) byColour[i % 3].push_back(make_int4(ly.offset + i, ly.nx, ly.ny, 1));
+    for (int j = 0; j < ly.ny; ++j) byColour[3 + j % 3].push_back(make_int4(ly.offset + j * ly.nx, 1, ly.nx, 0));
+    L.maxLine = std::max(L.maxLine, std::max(ly.nx, ly.ny));
+  }
+  L.lines.clear();
+  for (int c = 0; c < 6; ++c) {
+    L.colourStart[c] = (int)L.lines.size();
+    L.lines.insert(L.lines.end(), byColour[c].begin(), byColour[c].end());
+  }
+  L.colourStart[6] = (int)L.lines.size();
+}
+
+}  // namespace btd
+
+using namespace btd;
+
+struct btd_solver {
+  int device = 0;
+  cudaStream_t stream = nullptr, bodyStream = nullptr;
+  btd_params params{};
+  SimParams hostP{};
+  int N = 0, C = 0, nLayers = 0;
+  int redBlocks = 1;
+  std::vector<void*> allocs;
+  // scene copies for resetState
+  std::vector<float4> x0;
+  std::vector<Seg> segs0;
+  std::vector<float> soft0, fail0, tails0;
+  std::vector<uint8_t> damage0;
+  // device state
+  SimParams* dP = nullptr;
+  Scalars* dScal = nullptr;
+  uint32_t* dCounters = nullptr;
+  double* dPartials = nullptr;
+  unsigned* dTicket = nullptr;
+  NodeStatic* dNodes = nullptr;
+  DLayer* dLayers = nullptr;
+  float4 *x = nullptr, *v = nullptr, *dx = nullptr, *pred = nullptr, *ext = nullptr, *delta = nullptr, *p = nullptr,
+         *Ap = nullptr;
+  Seg* segs = nullptr;
+  float *softening = nullptr, *failSite = nullptr, *tails = nullptr, *strain = nullptr, *strength = nullptr;
+  uint8_t *damage = nullptr, *area = nullptr, *sep = nullptr, *marks = nullptr;
+  std::vector<Level> levels;
+  std::vector<DLayer> hostLayers;
+  // graphs: substep graphs keyed by Newton iteration count; the standalone PCG graph
+  std::map<int, cudaGraphExec_t> substepExec;
+  cudaGraphExec_t pcgExec = nullptr;
+  void* flushBuf = nullptr;  // profiling only: rewritten to evict L2 between timed launches
+
+  template <class T>
+  T* alloc(size_t count) {
+    void* ptr = nullptr;
+    CK(cudaMalloc(&ptr, std::max<size_t>(count, 1) * sizeof(T)));
+    CK(cudaMemsetAsync(ptr, 0, std::max<size_t>(count, 1) * sizeof(T), stream));
+    allocs.push_back(ptr);
+    return static_cast<T*>(ptr);
+  }
+
+  StepArgs stepArgs() const {
+    StepArgs a;
+    a.P = dP;
+    a.N = N;
+    a.nodes = dNodes;
+    a.pinned = levels[0].fixed;
+    a.layers = dLayers;
+    a.x = x;
+    a.v = v;
+    a.dx = dx;
+    a.pred = pred;
+    a.segs = segs;
+    a.ext = ext;
+    a.cmeta = nullptr;
+    a.counters = dCounters;
+    a.scal = dScal;
+    return a;
+  }
+  Reduce reduce() const { return {dPartials, dTicket}; }
+  PcgArgs pcgArgs(cudaGraphConditionalHandle h, int useCond) const {
+    PcgArgs a;
+    a.F = levels[0].dev();
+    a.p = p;
+    a.Ap = Ap;
+    a.delta = delta;
+    a.scal = dScal;
+    a.P = dP;
+    a.counters = dCounters;
+    a.red = reduce();
+    a.cond = h;
+    a.useCond = useCond;
+    return a;
+  }
+  HistArgs histArgs() const {
+    HistArgs a;
+    a.S = stepArgs();
+    a.nSpans = 2 * N;
+    a.nCross = C;
+    a.nLayers = nLayers;
+    a.strain = strain;
+    a.softening = softening;
+    a.failSite = failSite;
+    a.tails = tails;
+    a.damage = damage;
+    a.area = area;
+    a.strength = strength;
+    a.sep = sep;
+    a.marks = marks;
+    a.segsW = segs;
+    return a;
+  }
+
+  // ---------------------------------------------------------------- stage encoders (stream s)
+
+  void encPredict(cudaStream_t s) {
+    k_predict<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs());
+    k_project_start<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs());
+  }
+
+  void encHierarchy(cudaStream_t s) {
+    for (size_t k = 0; k + 1 < levels.size(); ++k) {
+      DLevel F = levels[k].dev(), Cl = levels[k + 1].dev();
+      if (k == 0) {
+        k_prolong_weights<FineRows, true><<<blocksFor(F.N, 128), 128, 0, s>>>(F, segs);
+        k_rap<FineRows><<<blocksFor(Cl.N, RAP_THREADS), RAP_THREADS, 0, s>>>(F, Cl);
+      } else {
+        k_prolong_weights<CoarseRows, false><<<blocksFor(F.N, 128), 128, 0, s>>>(F, segs);
+        k_rap<CoarseRows><<<blocksFor(Cl.N, RAP_THREADS), RAP_THREADS, 0, s>>>(F, Cl);
+      }
+    }
+  }
+
+  void encAssemble(cudaStream_t s, bool coarse) {
+    k_assemble<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs(), levels[0].op, levels[0].B);
+    if (coarse) encHierarchy(s);
+  }
+
+  void encSmooth(cudaStream_t s, int k, bool reverse) {
+    Level& L = levels[k];
+    size_t smem = sizeof(float) * smoothSmemFloats(L.maxLine);
+    for (int q = 0; q < 6; ++q) {
+      int c = reverse ? 5 - q : q;
+      int count = L.colourStart[c + 1] - L.colourStart[c];
+      if (count == 0) continue;
+      if (L.fine)
+        k_smooth<FineRows><<<count, SM_THREADS, smem, s>>>(L.dev(), L.dLines, L.colourStart[c]);
+      else
+        k_smooth<CoarseRows><<<count, SM_THREADS, smem, s>>>(L.dev(), L.dLines, L.colourStart[c]);
+    }
+  }
+
+  // encodeVCycle (solver.ts:584-598): X of level k = V(B) with X zero on entry.
+  void encVCycle(cudaStream_t s, int k) {
+    int last = (int)levels.size() - 1;
+    if (k == last) {
+      for (int sw = 0; sw < params.coarse_sweeps; ++sw) encSmooth(s, k, (sw & 1) == 1);
+      return;
+    }
+    Level& F = levels[k];
+    Level& Cl = levels[k + 1];
+    encSmooth(s, k, false);
+    if (F.fine)
+      k_residual<FineRows><<<blocksFor(F.N, 128), 128, 0, s>>>(F.dev());
+    else
+      k_residual<CoarseRows><<<blocksFor(F.N, 128), 128, 0, s>>>(F.dev());
+    k_restrict<<<blocksFor(Cl.N, 128), 128, 0, s>>>(F.dev(), Cl.dev());
+    encVCycle(s, k + 1);
+    k_prolong<<<blocksFor(F.N, 128), 128, 0, s>>>(F.dev(), Cl.dev());
+    encSmooth(s, k, true);
+  }
+
+  void encPcgBody(cudaStream_t s, const PcgArgs& a) {
+    encVCycle(s, 0);
+    k_pcg_dot_rz<<<redBlocks, RED_THREADS, 0, s>>>(a, 0);
+    k_pcg_update_p<<<blocksFor(N, 256), 256, 0, s>>>(a, 0);
+    k_pcg_matvec<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    k_pcg_update_xr<<<redBlocks, RED_THREADS, 0, s>>>(a);
+  }
+
+  // encodePCG (solver.ts:625-644) with the device-side stop: prologue, then a while-node whose
+  // condition k_pcg_update_xr sets. Must be called while `s` is capturing.
+  void encPCG(cudaStream_t s) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nDeps = 0;
+    CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nDeps));
+    if (st != cudaStreamCaptureStatusActive) throw std::runtime_error("PCG must be encoded into a graph capture");
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    PcgArgs a = pcgArgs(h, 1);
+    k_pcg_init<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    encVCycle(s, 0);
+    k_pcg_dot_rz<<<redBlocks, RED_THREADS, 0, s>>>(a, 1);
+    k_pcg_update_p<<<blocksFor(N, 256), 256, 0, s>>>(a, 1);
+    k_pcg_matvec<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    k_pcg_update_xr<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nDeps));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nDeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    CK(cudaStreamBeginCaptureToGraph(bodyStream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    encPcgBody(bodyStream, a);
+    cudaGraph_t out;
+    CK(cudaStreamEndCapture(bodyStream, &out));
+  }
+
+  void encLineSearch(cudaStream_t s) {
+    if (params.line_search) {
+      EnergyArgs e;
+      e.S = stepArgs();
+      e.delta = delta;
+      e.red = reduce();
+      k_energy<<<redBlocks, RED_THREADS, 0, s>>>(e);
+    } else {
+      k_set_alpha<<<1, 1, 0, s>>>(dScal, dCounters, 1.f);
+    }
+  }
+
+  void encApply(cudaStream_t s, int it) {
+    k_newton_apply<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs(), delta, std::min(it, MAX_NEWTON - 1));
+  }
+
+  // encodeNewtonIteration (solver.ts:687-696).
+  void encNewton(cudaStream_t s, int it) {
+    encAssemble(s, it == 0 || !params.lag_coarse);
+    encPCG(s);
+    encLineSearch(s);
+    encApply(s, it);
+  }
+
+  void encDamage(cudaStream_t s) {
+    HistArgs h = histArgs();
+    k_span_strain<<<blocksFor(2 * N, 256), 256, 0, s>>>(h);
+    k_sep_snapshot<<<blocksFor(2 * C, 256), 256, 0, s>>>(h);
+    k_field_update<<<blocksFor(2 * N, 128), 128, 0, s>>>(h);
+    for (int l = 0; l < nLayers; ++l)
+      k_pull_mark<<<blocksFor(hostLayers[l].K * hostLayers[l].M, 128), 128, 0, s>>>(h, l);
+    k_pull_apply<<<blocksFor(2 * C, 256), 256, 0, s>>>(h);
+    k_couple<<<blocksFor(2 * N, 128), 128, 0, s>>>(h);
+  }
+
+  // encodeFinalize (solver.ts:723-728); history passes check SimParams.historyOn on the device.
+  void encFinalize(cudaStream_t s) {
+    k_commit<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs());
+    encDamageGated(s);
+    HistArgs h = histArgs();
+    for (int f = 0; f < 2; ++f)
+      for (int par = 0; par < 2; ++par) k_slip<<<blocksFor(N, 128), 128, 0, s>>>(h, f, par);
+  }
+  void encDamageGated(cudaStream_t s);
+
+  void encSubstep(cudaStream_t s, int newtonIterations) {
+    CK(cudaMemsetAsync(dCounters + CNT_UPDATE, 0, sizeof(uint32_t) * MAX_NEWTON, s));
+    encPredict(s);
+    for (int it = 0; it < newtonIterations; ++it) encNewton(s, it);
+    encFinalize(s);
+  }
+
+  cudaGraphExec_t capture(const std::function<void(cudaStream_t)>& fn) {
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+    try {
+      fn(stream);
+    } catch (...) {
+      cudaGraph_t g;
+      cudaStreamEndCapture(stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    cudaGraph_t g;
+    CK(cudaStreamEndCapture(stream, &g));
+    cudaGraphExec_t ex;
+    CK(cudaGraphInstantiate(&ex, g, 0));
+    CK(cudaGraphDestroy(g));
+    return ex;
+  }
+
+  cudaGraphExec_t substepGraph(int iters) {
+    auto it = substepExec.find(iters);
+    if (it != substepExec.end()) return it->second;
+    cudaGraphExec_t ex = capture([&](cudaStream_t s) { encSubstep(s, iters); });
+    substepExec[iters] = ex;
+    return ex;
+  }
+
+  void pushParams() {
+    CK(cudaMemcpyAsync(dP, &hostP, sizeof(SimParams), cudaMemcpyHostToDevice, stream));
+  }
+  void sync() { CK(cudaStreamSynchronize(stream)); }
+
+  ~btd_solver() {
+    for (auto& kv : substepExec) cudaGraphExecDestroy(kv.second);
+    if (pcgExec) cudaGraphExecDestroy(pcgExec);
+    if (flushBuf) cudaFree(flushBuf);
+    for (void* q : allocs) cudaFree(q);
+    if (stream) cudaStreamDestroy(stream);
+    if (bodyStream) cudaStreamDestroy(bodyStream);
+  }
+};
+
+// The damage passes early-out inside the kernels when history is off, except the span strain and
+// snapshot passes, which are cheap and harmless.
+void btd_solver::encDamageGated(cudaStream_t s) { encDamage(s); }
+
+namespace {
+
+int fail(const std::exception& e) {
+  if (dynamic_cast<const CudaError*>(&e)) {
+    btd::setError(e.what());
+    return BTD_E_CUDA;
+  }
+  btd::setError(e.what());
+  return BTD_E_INVALID;
+}
+
+#define GUARD(...)                         \
+  try {                                    \
+    __VA_ARGS__;                           \
+    return BTD_OK;                         \
+  } catch (const std::exception& e) {      \
+    return fail(e);                        \
+  }
+
+DYarn toDYarn(const btd_yarn& y) {
+  return {(float)y.ea_low, (float)y.ea_high, (float)y.crimp_strain, (float)y.ea_compress, (float)y.axial_viscosity,
+          (float)y.bend_rigidity, (float)y.bend_viscosity, (float)(y.yarns_per_span > 0 ? y.yarns_per_span : 1)};
+}
+
+void checkSolver(btd_solver* s) {
+  if (!s) throw std::invalid_argument("null solver");
+}
+
+}  // namespace
+
+extern "C" {
+
+int btd_default_params(btd_params* out) {
+  if (!out) return BTD_E_INVALID;
+  btd_params p{};
+  p.h = 1.0 / 120;
+  p.gravity[0] = 0;
+  p.gravity[1] = 0;
+  p.gravity[2] = -9.81;
+  p.newton_iterations = 2;
+  p.newton_max = 2;
+  p.newton_tolerance = 1e-5;
+  p.history_tolerance = 1;
+  p.pcg_iterations = 2;
+  p.coarse_sweeps = 2;
+  p.max_coarsest_nodes = 400;
+  p.self_contact = 0;
+  p.pcg_rel_tol = 0;
+  p.line_search = 1;
+  p.lag_coarse = 1;
+  *out = p;
+  return BTD_OK;
+}
+
+int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
+  if (!sc || !prm || !out) {
+    btd::setError("btd_create: null argument");
+    return BTD_E_INVALID;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    btd::setError("btd_create: no CUDA device (the solve has no CPU fallback)");
+    return BTD_E_NO_DEVICE;
+  }
+  std::unique_ptr<btd_solver> s(new btd_solver());
+  try {
+    if (prm->newton_iterations < 1 || prm->newton_iterations > MAX_NEWTON || prm->newton_max < prm->newton_iterations ||
+        prm->newton_max > MAX_NEWTON)
+      throw std::invalid_argument("invalid Newton iteration bounds");
+    if (prm->pcg_iterations < 1) throw std::invalid_argument("pcg_iterations must be >= 1");
+    if (prm->coarse_sweeps < 1) throw std::invalid_argument("coarse_sweeps must be >= 1");
+    if (!(prm->h > 0)) throw std::invalid_argument("h must be positive");
+    CK(cudaGetDevice(&s->device));
+    CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&s->bodyStream, cudaStreamNonBlocking));
+    s->params = *prm;
+    const int N = sc->node_count, C = sc->crossing_count;
+    s->N = N;
+    s->C = C;
+    s->nLayers = sc->n_layers;
+    if (N < 4 || sc->n_layers < 1) throw std::invalid_argument("empty scene");
+
+    // ---- layers and per-node static data
+    std::vector<NodeStatic> nodes(N);
+    std::vector<uint32_t> pinned(N);
+    std::vector<uint2> coord(N);
+    for (int l = 0; l < sc->n_layers; ++l) {
+      const btd_layer_info& L = sc->layers[l];
+      if (L.nx < 2 || L.ny < 2 || L.nx > 65535 || L.ny > 65535) throw std::invalid_argument("lattice extent out of range");
+      if (std::max(L.nx, L.ny) > SM_MAX_LINE) throw std::invalid_argument("yarn line longer than " + std::to_string(SM_MAX_LINE));
+      if (L.bundle[0] > 32 || L.bundle[1] > 32) throw std::invalid_argument("bundles of more than 32 yarns are not supported");
+      DLayer d{};
+      d.offset = L.node_offset;
+      d.nx = L.nx;
+      d.ny = L.ny;
+      d.nodeCount = L.node_count;
+      d.yarn[0] = toDYarn(L.material.yarns[0]);
+      d.yarn[1] = toDYarn(L.material.yarns[1]);
+      d.shearStiffness = (float)L.material.shear_stiffness;
+      d.crossingFriction = (float)L.material.crossing_friction;
+      d.crossingWrap = (float)L.material.crossing_wrap;
+      d.pitchU = (float)L.material.pitch_u;
+      d.pitchV = (float)L.material.pitch_v;
+      d.airDrag = (float)L.material.air_drag;
+      d.crossingNormal0 = (float)L.material.crossing_normal0;
+      d.thickness = (float)L.material.thickness;
+      d.fOffset = L.field_offset;
+      d.K = L.field_k;
+      d.M = L.field_m;
+      d.bu = L.bundle[0];
+      d.bv = L.bundle[1];
+      d.reachU = std::max(1, (int)std::lround(1.2e-3 / L.weave.pitch_u));
+      d.reachV = std::max(1, (int)std::lround(1.2e-3 / L.weave.pitch_v));
+      d.weavePitchU = (float)L.weave.pitch_u;
+      d.weavePitchV = (float)L.weave.pitch_v;
+      s->hostLayers.push_back(d);
+      for (int j = 0; j < L.ny; ++j)
+        for (int i = 0; i < L.nx; ++i) {
+          int n = L.node_offset + j * L.nx + i;
+          nodes[n] = {(uint32_t)i | ((uint32_t)j << 16), (uint32_t)l, (float)sc->mass[n], (float)sc->crossing_normal0[n]};
+          pinned[n] = sc->pinned[n] ? 1u : 0u;
+          coord[n] = make_uint2((uint32_t)i | ((uint32_t)j << 16), (uint32_t)l);
+        }
+    }
+    cudaStream_t st = s->stream;
+    s->dP = s->alloc<SimParams>(1);
+    s->dScal = s->alloc<Scalars>(1);
+    s->dCounters = s->alloc<uint32_t>(CNT_SIZE);
+    s->redBlocks = std::max(1, std::min(blocksFor(N, RED_THREADS), 4 * 148));
+    s->dPartials = s->alloc<double>(8 * (size_t)s->redBlocks);
+    s->dTicket = s->alloc<unsigned>(1);
+    s->dNodes = s->alloc<NodeStatic>(N);
+    s->dLayers = s->alloc<DLayer>(s->hostLayers.size());
+    CK(cudaMemcpyAsync(s->dNodes, nodes.data(), sizeof(NodeStatic) * N, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->dLayers, s->hostLayers.data(), sizeof(DLayer) * s->hostLayers.size(), cudaMemcpyHostToDevice, st));
+    s->x = s->alloc<float4>(N);
+    s->v = s->alloc<float4>(N);
+    s->dx = s->alloc<float4>(N);
+    s->pred = s->alloc<float4>(N);
+    s->ext = s->alloc<float4>(3 * (size_t)N);
+    s->delta = s->alloc<float4>(N);
+    s->p = s->alloc<float4>(N);
+    s->Ap = s->alloc<float4>(N);
+    s->segs = s->alloc<Seg>(2 * (size_t)N);
+    s->softening = s->alloc<float>(2 * (size_t)N);
+    s->failSite = s->alloc<float>(2 * (size_t)N);
+    s->tails = s->alloc<float>(4 * (size_t)N);
+    s->strain = s->alloc<float>(2 * (size_t)N);
+    s->damage = s->alloc<uint8_t>(2 * (size_t)C);
+    s->area = s->alloc<uint8_t>(2 * (size_t)C);
+    s->sep = s->alloc<uint8_t>(2 * (size_t)C);
+    s->marks = s->alloc<uint8_t>(2 * (size_t)C);
+    s->strength = s->alloc<float>(2 * (size_t)C);
+
+    // ---- scene state (kept on the host for resetState)
+    s->x0.resize(N);
+    for (int n = 0; n < N; ++n)
+      s->x0[n] = make_float4((float)sc->position[3 * n], (float)sc->position[3 * n + 1], (float)sc->position[3 * n + 2], 0.f);
+    s->segs0.resize(2 * (size_t)N);
+    s->soft0.resize(2 * (size_t)N);
+    s->fail0.resize(2 * (size_t)N);
+    for (size_t q = 0; q < 2 * (size_t)N; ++q) {
+      s->segs0[q] = {(float)sc->rest_length[q], (float)sc->intact[q], sc->cut_mask[q], (uint32_t)sc->seg_flags[q]};
+      s->soft0[q] = (float)sc->softening[q];
+      s->fail0[q] = sc->fail_site[q];
+    }
+    s->tails0.resize(4 * (size_t)N);
+    for (size_t q = 0; q < 4 * (size_t)N; ++q) s->tails0[q] = (float)sc->tails[q];
+    s->damage0.assign(sc->field_damage, sc->field_damage + 2 * (size_t)C);
+    CK(cudaMemcpyAsync(s->softening, s->soft0.data(), sizeof(float) * 2 * N, cudaMemcpyHostToDevice, st));
+    if (C > 0) {
+      CK(cudaMemcpyAsync(s->area, sc->field_area, 2 * (size_t)C, cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(s->strength, sc->field_strength, sizeof(float) * 2 * (size_t)C, cudaMemcpyHostToDevice, st));
+    }
+
+    // ---- multigrid levels (levelLayers, lattice.ts:302-310)
+    std::vector<DLevelLayer> cur;
+    for (int l = 0; l < sc->n_layers; ++l)
+      cur.push_back({sc->layers[l].node_offset, sc->layers[l].nx, sc->layers[l].ny, 0});
+    for (;;) {
+      Level L;
+      L.layers = cur;
+      for (auto& ly : cur) L.N += ly.nx * ly.ny;
+      L.fine = s->levels.empty();
+      buildLines(L);
+      s->levels.push_back(L);
+      bool can = true;
+      for (auto& ly : cur) can = can && ly.nx * ly.ny > 48 && ly.nx >= 5 && ly.ny >= 5;
+      if (L.N <= prm->max_coarsest_nodes || !can) break;
+      std::vector<DLevelLayer> nxt;
+      int off = 0;
+      for (auto& ly : cur) {
+        DLevelLayer c{off, ly.nx / 2 + 1, ly.ny / 2 + 1, 0};
+        off += c.nx * c.ny;
+        nxt.push_back(c);
+      }
+      cur = nxt;
+    }
+    for (size_t k = 0; k < s->levels.size(); ++k) {
+      Level& L = s->levels[k];
+      L.dLayers = s->alloc<DLevelLayer>(L.layers.size());
+      CK(cudaMemcpyAsync(L.dLayers, L.layers.data(), sizeof(DLevelLayer) * L.layers.size(), cudaMemcpyHostToDevice, st));
+      std::vector<uint2> cc(L.N);
+      for (size_t l = 0; l < L.layers.size(); ++l) {
+        auto& ly = L.layers[l];
+        for (int j = 0; j < ly.ny; ++j)
+          for (int i = 0; i < ly.nx; ++i) cc[ly.offset + j * ly.nx + i] = make_uint2((uint32_t)i | ((uint32_t)j << 16), (uint32_t)l);
+      }
+      L.dCoord = s->alloc<uint2>(L.N);
+      CK(cudaMemcpyAsync(L.dCoord, cc.data(), sizeof(uint2) * L.N, cudaMemcpyHostToDevice, st));
+      L.dLines = s->alloc<int4>(L.lines.size());
+      CK(cudaMemcpyAsync(L.dLines, L.lines.data(), sizeof(int4) * L.lines.size(), cudaMemcpyHostToDevice, st));
+      L.op = s->alloc<float4>((size_t)(L.fine ? FINE_PLANES : COARSE_PLANES) * L.N);
+      L.fixed = s->alloc<uint32_t>(L.N);
+      if (k == 0) CK(cudaMemcpyAsync(L.fixed, pinned.data(), sizeof(uint32_t) * N, cudaMemcpyHostToDevice, st));
+      L.X = s->alloc<float4>(L.N);
+      L.B = s->alloc<float4>(L.N);
+      L.R = s->alloc<float4>(L.N);
+      L.pw = s->alloc<float4>(L.N);
+      size_t smem = sizeof(float) * smoothSmemFloats(L.maxLine);
+      if (smem > 48 * 1024) {
+        if (L.fine)
+          CK(cudaFuncSetAttribute(k_smooth<FineRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        else
+          CK(cudaFuncSetAttribute(k_smooth<CoarseRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      }
+    }
+
+    // ---- parameters
+    SimParams& P = s->hostP;
+    P.h = (float)prm->h;
+    P.gx = (float)prm->gravity[0];
+    P.gy = (float)prm->gravity[1];
+    P.gz = (float)prm->gravity[2];
+    P.historyOn = 1;
+    P.historyTol = (float)prm->history_tolerance;
+    P.floorOn = 0;
+    P.floorZ = 0;
+    P.floorBulge = 0.3e-3f;
+    P.floorStiffness = 1300.f;
+    P.floorFriction = 0.35f;
+    P.floorFrictionSpeed = 0.002f;
+    P.pcgMax = prm->pcg_iterations;
+    P.lineSearch = prm->line_search;
+    P.pcgTol = prm->pcg_rel_tol;
+    P.newtonTol = (float)prm->newton_tolerance;
+    s->pushParams();
+
+    // ---- initial state (resetState)
+    CK(cudaMemcpyAsync(s->x, s->x0.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->segs, s->segs0.data(), sizeof(Seg) * 2 * N, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->failSite, s->fail0.data(), sizeof(float) * 2 * N, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->tails, s->tails0.data(), sizeof(float) * 4 * N, cudaMemcpyHostToDevice, st));
+    if (C > 0) CK(cudaMemcpyAsync(s->damage, s->damage0.data(), 2 * (size_t)C, cudaMemcpyHostToDevice, st));
+    s->sync();
+    s->substepGraph(prm->newton_iterations);
+    s->pcgExec = s->capture([&](cudaStream_t q) { s->encPCG(q); });
+    s->sync();
+    *out = s.release();
+    return BTD_OK;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+int btd_destroy(btd_solver* s) {
+  if (!s) return BTD_OK;
+  cudaStreamSynchronize(s->stream);
+  delete s;
+  return BTD_OK;
+}
+
+int btd_substep(btd_solver* s, int32_t min_iterations, int32_t max_iterations) {
+  GUARD({
+    checkSolver(s);
+    int iters = std::min(MAX_NEWTON, std::max(s->params.newton_iterations, (int)min_iterations));
+    (void)max_iterations;
+    CK(cudaGraphLaunch(s->substepGraph(iters), s->stream));
+  });
+}
+
+int btd_substeps(btd_solver* s, int32_t count) {
+  GUARD({
+    checkSolver(s);
+    cudaGraphExec_t ex = s->substepGraph(s->params.newton_iterations);
+    for (int k = 0; k < count; ++k) CK(cudaGraphLaunch(ex, s->stream));
+  });
+}
+
+int btd_synchronize(btd_solver* s) { GUARD({ checkSolver(s); s->sync(); }); }
+
+int btd_set_state(btd_solver* s, const float* pos4, const float* vel4) {
+  GUARD({
+    checkSolver(s);
+    if (!pos4) throw std::invalid_argument("null positions");
+    CK(cudaMemcpyAsync(s->x, pos4, sizeof(float4) * s->N, cudaMemcpyHostToDevice, s->stream));
+    if (vel4)
+      CK(cudaMemcpyAsync(s->v, vel4, sizeof(float4) * s->N, cudaMemcpyHostToDevice, s->stream));
+    else
+      CK(cudaMemsetAsync(s->v, 0, sizeof(float4) * s->N, s->stream));
+    s->sync();
+  });
+}
+
+int btd_get_state(btd_solver* s, float* pos4, float* vel4) {
+  GUARD({
+    checkSolver(s);
+    if (pos4) CK(cudaMemcpyAsync(pos4, s->x, sizeof(float4) * s->N, cudaMemcpyDeviceToHost, s->stream));
+    if (vel4) CK(cudaMemcpyAsync(vel4, s->v, sizeof(float4) * s->N, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+  });
+}
+
+int btd_set_segments(btd_solver* s, const float* rest, const float* intact, const uint32_t* cut, const uint32_t* flags,
+                     const float* fail_site, const float* tails) {
+  GUARD({
+    checkSolver(s);
+    const size_t n2 = 2 * (size_t)s->N;
+    std::vector<Seg> sg(n2);
+    CK(cudaMemcpyAsync(sg.data(), s->segs, sizeof(Seg) * n2, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+    for (size_t q = 0; q < n2; ++q) {
+      if (rest) sg[q].rest = rest[q];
+      if (intact) sg[q].intact = intact[q];
+      if (cut) sg[q].cutMask = cut[q];
+      if (flags) sg[q].flags = flags[q];
+    }
+    CK(cudaMemcpyAsync(s->segs, sg.data(), sizeof(Seg) * n2, cudaMemcpyHostToDevice, s->stream));
+    if (fail_site) CK(cudaMemcpyAsync(s->failSite, fail_site, sizeof(float) * n2, cudaMemcpyHostToDevice, s->stream));
+    if (tails) CK(cudaMemcpyAsync(s->tails, tails, sizeof(float) * 4 * s->N, cudaMemcpyHostToDevice, s->stream));
+    s->sync();
+  });
+}
+
+int btd_get_segments(btd_solver* s, float* rest, float* intact, uint32_t* cut, uint32_t* flags, float* fail_site, float* tails) {
+  GUARD({
+    checkSolver(s);
+    const size_t n2 = 2 * (size_t)s->N;
+    std::vector<Seg> sg(n2);
+    CK(cudaMemcpyAsync(sg.data(), s->segs, sizeof(Seg) * n2, cudaMemcpyDeviceToHost, s->stream));
+    if (fail_site) CK(cudaMemcpyAsync(fail_site, s->failSite, sizeof(float) * n2, cudaMemcpyDeviceToHost, s->stream));
+    if (tails) CK(cudaMemcpyAsync(tails, s->tails, sizeof(float) * 4 * s->N, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+    for (size_t q = 0; q < n2; ++q) {
+      if (rest) rest[q] = sg[q].rest;
+      if (intact) intact[q] = sg[q].intact;
+      if (cut) cut[q] = sg[q].cutMask;
+      if (flags) flags[q] = sg[q].flags;
+    }
+  });
+}
+
+int btd_set_field(btd_solver* s, const uint8_t* damage) {
+  GUARD({
+    checkSolver(s);
+    if (s->C > 0) CK(cudaMemcpyAsync(s->damage, damage, 2 * (size_t)s->C, cudaMemcpyHostToDevice, s->stream));
+    s->sync();
+  });
+}
+
+int btd_get_field(btd_solver* s, uint8_t* damage) {
+  GUARD({
+    checkSolver(s);
+    if (s->C > 0) CK(cudaMemcpyAsync(damage, s->damage, 2 * (size_t)s->C, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+  });
+}
+
+int btd_reset_state(btd_solver* s) {
+  GUARD({
+    checkSolver(s);
+    const int N = s->N;
+    CK(cudaMemcpyAsync(s->x, s->x0.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemsetAsync(s->v, 0, sizeof(float4) * N, s->stream));
+    CK(cudaMemcpyAsync(s->segs, s->segs0.data(), sizeof(Seg) * 2 * N, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->failSite, s->fail0.data(), sizeof(float) * 2 * N, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->tails, s->tails0.data(), sizeof(float) * 4 * N, cudaMemcpyHostToDevice, s->stream));
+    if (s->C > 0) CK(cudaMemcpyAsync(s->damage, s->damage0.data(), 2 * (size_t)s->C, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemsetAsync(s->ext, 0, sizeof(float4) * 3 * N, s->stream));
+    s->sync();
+  });
+}
+
+int btd_set_floor(btd_solver* s, int32_t enabled, float z) {
+  GUARD({
+    checkSolver(s);
+    s->hostP.floorOn = enabled ? 1 : 0;
+    s->hostP.floorZ = z;
+    s->pushParams();
+    s->sync();
+  });
+}
+
+int btd_set_timestep(btd_solver* s, float h) {
+  GUARD({
+    checkSolver(s);
+    if (!(h > 0)) throw std::invalid_argument("h must be positive");
+    s->hostP.h = h;
+    s->params.h = h;
+    s->pushParams();
+    s->sync();
+  });
+}
+
+int btd_set_history(btd_solver* s, int32_t on) {
+  GUARD({
+    checkSolver(s);
+    s->hostP.historyOn = on ? 1 : 0;
+    s->pushParams();
+    s->sync();
+  });
+}
+
+int btd_set_newton_tolerance(btd_solver* s, float tol) {
+  GUARD({
+    checkSolver(s);
+    s->hostP.newtonTol = tol;
+    s->params.newton_tolerance = tol;
+    s->pushParams();
+    s->sync();
+  });
+}
+
+int btd_set_pcg(btd_solver* s, int32_t max_iterations, double rel_tol) {
+  GUARD({
+    checkSolver(s);
+    if (max_iterations < 1) throw std::invalid_argument("max_iterations must be >= 1");
+    s->hostP.pcgMax = max_iterations;
+    s->hostP.pcgTol = rel_tol;
+    s->params.pcg_iterations = max_iterations;
+    s->params.pcg_rel_tol = rel_tol;
+    s->pushParams();
+    s->sync();
+  });
+}
+
+int btd_read_counters(btd_solver* s, uint32_t* out, int32_t n) {
+  GUARD({
+    checkSolver(s);
+    if (!out || n < 0 || n > CNT_SIZE) throw std::invalid_argument("bad counter count");
+    CK(cudaMemcpyAsync(out, s->dCounters, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+  });
+}
+
+int btd_clear_counters(btd_solver* s) {
+  GUARD({
+    checkSolver(s);
+    CK(cudaMemsetAsync(s->dCounters, 0, sizeof(uint32_t) * CNT_SIZE, s->stream));
+    s->sync();
+  });
+}
+
+int btd_stage_predict(btd_solver* s) {
+  GUARD({
+    checkSolver(s);
+    s->encPredict(s->stream);
+    CK(cudaGetLastError());
+    s->sync();
+  });
+}
+
+int btd_stage_assemble(btd_solver* s, int32_t coarse) {
+  GUARD({
+    checkSolver(s);
+    s->encAssemble(s->stream, coarse != 0);
+    CK(cudaGetLastError());
+    s->sync();
+  });
+}
+
+int btd_stage_vcycle(btd_solver* s) {
+  GUARD({
+    checkSolver(s);
+    CK(cudaMemsetAsync(s->levels[0].X, 0, sizeof(float4) * s->N, s->stream));
+    s->encVCycle(s->stream, 0);
+    CK(cudaGetLastError());
+    s->sync();
+  });
+}
+
+int btd_stage_pcg(btd_solver* s) {
+  GUARD({
+    checkSolver(s);
+    CK(cudaGraphLaunch(s->pcgExec, s->stream));
+    s->sync();
+  });
+}
+
+int btd_stage_linesearch(btd_solver* s, double* e4, double* m4) {
+  GUARD({
+    checkSolver(s);
+    s->encLineSearch(s->stream);
+    CK(cudaGetLastError());
+    Scalars sc;
+    CK(cudaMemcpyAsync(&sc, s->dScal, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+    for (int k = 0; k < 4; ++k) {
+      if (e4) e4[k] = sc.e[k];
+      if (m4) m4[k] = sc.m[k];
+    }
+  });
+}
+
+int btd_stage_apply(btd_solver* s, int32_t it) {
+  GUARD({
+    checkSolver(s);
+    s->encApply(s->stream, it);
+    CK(cudaGetLastError());
+    s->sync();
+  });
+}
+
+int btd_stage_newton(btd_solver* s, int32_t it) {
+  GUARD({
+    checkSolver(s);
+    cudaGraphExec_t ex = s->capture([&](cudaStream_t q) { s->encNewton(q, it); });
+    cudaError_t e = cudaGraphLaunch(ex, s->stream);
+    cudaError_t e2 = cudaStreamSynchronize(s->stream);
+    cudaGraphExecDestroy(ex);
+    CK(e);
+    CK(e2);
+  });
+}
+
+int btd_stage_finalize(btd_solver* s) {
+  GUARD({
+    checkSolver(s);
+    s->encFinalize(s->stream);
+    CK(cudaGetLastError());
+    s->sync();
+  });
+}
+
+int btd_stage_damage(btd_solver* s) {
+  GUARD({
+    checkSolver(s);
+    s->encDamage(s->stream);
+    CK(cudaGetLastError());
+    s->sync();
+  });
+}
+
+int btd_profile_stage(btd_solver* s, int32_t which, int32_t reps, int32_t flush, float* ms) {
+  GUARD({
+    checkSolver(s);
+    if (!ms || reps < 1 || which < 0 || which > 5) throw std::invalid_argument("bad profile request");
+    const size_t flushBytes = size_t(256) << 20;
+    if (flush && !s->flushBuf) CK(cudaMalloc(&s->flushBuf, flushBytes));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float total = 0.f;
+    PcgArgs pa = s->pcgArgs(0, 0);
+    for (int r = 0; r < reps; ++r) {
+      if (flush) CK(cudaMemsetAsync(s->flushBuf, r & 0xff, flushBytes, s->stream));
+      CK(cudaEventRecord(e0, s->stream));
+      switch (which) {
+        case BTD_STAGE_MATVEC:
+          k_pcg_matvec<<<s->redBlocks, RED_THREADS, 0, s->stream>>>(pa);
+          break;
+        case BTD_STAGE_SMOOTH:
+          s->encSmooth(s->stream, 0, false);
+          break;
+        case BTD_STAGE_ASSEMBLE:
+          s->encAssemble(s->stream, false);
+          break;
+        case BTD_STAGE_VCYCLE:
+          CK(cudaMemsetAsync(s->levels[0].X, 0, sizeof(float4) * s->N, s->stream));
+          s->encVCycle(s->stream, 0);
+          break;
+        case BTD_STAGE_HIERARCHY:
+          s->encHierarchy(s->stream);
+          break;
+        default:
+          CK(cudaGraphLaunch(s->substepGraph(s->params.newton_iterations), s->stream));
+      }
+      CK(cudaEventRecord(e1, s->stream));
+      CK(cudaEventSynchronize(e1));
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, e0, e1));
+      total += t;
+    }
+    CK(cudaGetLastError());
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = total / reps;
+  });
+}
+
+int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pcg, int64_t* out) {
+  GUARD({
+    checkSolver(s);
+    if (!out) throw std::invalid_argument("null output");
+    auto colours = [&](int k) {
+      int c = 0;
+      for (int q = 0; q < 6; ++q) c += s->levels[k].colourStart[q + 1] > s->levels[k].colourStart[q];
+      return (int64_t)c;
+    };
+    const int L = (int)s->levels.size();
+    int64_t V = s->params.coarse_sweeps * colours(L - 1);
+    for (int k = 0; k + 1 < L; ++k) V += 2 * colours(k) + 3;
+    // per Newton iteration: assembly, PCG prologue (init + V-cycle + 4), line search, apply; the
+    // hierarchy (weights + RAP per coarse level) on the first iteration; V-cycle + 4 per extra PCG pass
+    const int64_t perNewton = 1 + (1 + V + 4) + 1 + 1;
+    const int64_t hierarchy = 2 * (L - 1);
+    const int64_t hierPerSubstep = s->params.lag_coarse ? hierarchy : hierarchy * (newton / std::max(1, substeps));
+    const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4;
+    *out = (int64_t)substeps * (perSubstep + hierPerSubstep) + (int64_t)newton * perNewton + (int64_t)(pcg - newton) * (V + 4);
+  });
+}
+
+int btd_level_count(btd_solver* s, int32_t* out) {
+  GUARD({
+    checkSolver(s);
+    *out = (int32_t)s->levels.size();
+  });
+}
+
+int btd_level_nodes(btd_solver* s, int32_t level, int32_t* out) {
+  GUARD({
+    checkSolver(s);
+    if (level < 0 || level >= (int)s->levels.size()) throw std::invalid_argument("level out of range");
+    *out = s->levels[level].N;
+  });
+}
+
+int btd_read_operator(btd_solver* s, int32_t level, double* out, uint8_t* fixed) {
+  GUARD({
+    checkSolver(s);
+    if (level < 0 || level >= (int)s->levels.size()) throw std::invalid_argument("level out of range");
+    Level& L = s->levels[level];
+    const int planes = L.fine ? FINE_PLANES : COARSE_PLANES;
+    std::vector<float4> op((size_t)planes * L.N);
+    std::vector<uint32_t> fx(L.N);
+    CK(cudaMemcpyAsync(op.data(), L.op, sizeof(float4) * op.size(), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(fx.data(), L.fixed, sizeof(uint32_t) * L.N, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+    auto flt = [&](int n, int f) {
+      const float4& v = op[(size_t)(f >> 2) * L.N + n];
+      int c = f & 3;
+      return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
+    };
+    if (out) {
+      std::fill(out, out + (size_t)L.N * 225, 0.0);
+      for (int n = 0; n < L.N; ++n) {
+        auto put = [&](int o, int f) {
+          double xx = flt(n, f), xy = flt(n, f + 1), xz = flt(n, f + 2), yy = flt(n, f + 3), yz = flt(n, f + 4), zz = flt(n, f + 5);
+          double* b = out + ((size_t)n * 25 + o) * 9;
+          b[0] = xx, b[1] = xy, b[2] = xz, b[3] = xy, b[4] = yy, b[5] = yz, b[6] = xz, b[7] = yz, b[8] = zz;
+        };
+        auto scal = [&](int o, double v) {
+          double* b = out + ((size_t)n * 25 + o) * 9;
+          b[0] = v, b[4] = v, b[8] = v;
+        };
+        if (L.fine) {
+          const int di[8] = {1, -1, 0, 0, 1, -1, -1, 1}, dj[8] = {0, 0, 1, -1, 1, -1, 1, -1};
+          put(12, 0);
+          for (int k = 0; k < 8; ++k) put((dj[k] + 2) * 5 + di[k] + 2, 6 * (k + 1));
+          scal(14, flt(n, 54));
+          scal(10, flt(n, 55));
+          scal(22, flt(n, 56));
+          scal(2, flt(n, 57));
+        } else {
+          for (int o = 0; o < 25; ++o) put(o, 6 * o);
+        }
+      }
+    }
+    if (fixed)
+      for (int n = 0; n < L.N; ++n) fixed[n] = fx[n] ? 1 : 0;
+  });
+}
+
+static float4* vectorPtr(btd_solver* s, int which, int level, size_t* count) {
+  if (which <= BTD_VEC_R) {
+    if (level < 0 || level >= (int)s->levels.size()) throw std::invalid_argument("level out of range");
+    Level& L = s->levels[level];
+    *count = L.N;
+    return which == BTD_VEC_X ? L.X : which == BTD_VEC_B ? L.B : L.R;
+  }
+  *count = s->N;
+  if (which == BTD_VEC_DELTA) return s->delta;
+  if (which == BTD_VEC_DX) return s->dx;
+  if (which == BTD_VEC_PRED) return s->pred;
+  throw std::invalid_argument("unknown vector");
+}
+
+int btd_read_vector(btd_solver* s, int32_t which, int32_t level, float* out4) {
+  GUARD({
+    checkSolver(s);
+    size_t n;
+    float4* p = vectorPtr(s, which, level, &n);
+    CK(cudaMemcpyAsync(out4, p, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+  });
+}
+
+int btd_write_vector(btd_solver* s, int32_t which, int32_t level, const float* in4) {
+  GUARD({
+    checkSolver(s);
+    size_t n;
+    float4* p = vectorPtr(s, which, level, &n);
+    CK(cudaMemcpyAsync(p, in4, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
+    s->sync();
+  });
+}
+
+}  // extern "C"

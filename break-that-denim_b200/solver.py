@@ -1,0 +1,231 @@
+"""GpuSolver: the host-side mirror of the reference's `GpuSolver` (src/simulation/gpu/solver.ts:194-838).
+
+Method names follow the reference (setState -> set_state, encodeSubstep -> substep, ...); every
+call goes through the C ABI of libbtd.so (include/btd.h). There is no CPU path: constructing a
+solver without a CUDA device raises.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import check
+
+FINE_ROW = 72  # the reference's fine row floats (solver.ts:99), for readers of its layouts
+COARSE_ROW = 200
+
+COUNTER_NAMES = {0: "ruptures", 1: "pulled_out", 2: "max_speed", 3: "alpha", 12: "rejected", 16: "pcg_last",
+                 17: "pcg_total", 18: "newton", 19: "rel_residual", 20: "errors"}
+
+
+def default_params(**kw):
+    """GPU_DEFAULTS (solver.ts:61-72) with keyword overrides (field names of btd_params)."""
+    p = _abi.Params()
+    check("btd_default_params", C.byref(p))
+    for k, v in kw.items():
+        if k == "gravity":
+            p.gravity[0], p.gravity[1], p.gravity[2] = v
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def _f(a, n, dt=np.float32):
+    a = np.ascontiguousarray(a, dt)
+    assert a.size == n, (a.size, n)
+    return a
+
+
+class GpuSolver:
+    """One patch (or several layers) on one GPU; owns its device memory and CUDA stream."""
+
+    def __init__(self, scene, params=None, **kw):
+        self.scene = scene
+        self.params = params if params is not None else default_params(**kw)
+        self.N = scene.N
+        self.C = scene.C
+        h = C.c_void_p()
+        check("btd_create", C.byref(scene.c()), C.byref(self.params), C.byref(h))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _abi.lib().btd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    # ---- per substep
+    def substep(self, min_iterations=0, max_iterations=0):
+        """encodeSubstep (solver.ts:737-760), launched on the solver's stream."""
+        check("btd_substep", self._h, min_iterations, max_iterations)
+
+    def substeps(self, count):
+        check("btd_substeps", self._h, count)
+
+    def synchronize(self):
+        check("btd_synchronize", self._h)
+
+    # ---- state I/O
+    def set_state(self, position, velocity=None):
+        """setState (solver.ts:833-837): positions (N, 3) or (N, 4); velocities or zero."""
+        pos = np.zeros((self.N, 4), np.float32)
+        pos[:, :3] = np.asarray(position, np.float64).reshape(self.N, -1)[:, :3]
+        vel = None
+        if velocity is not None:
+            vel = np.zeros((self.N, 4), np.float32)
+            vel[:, :3] = np.asarray(velocity, np.float64).reshape(self.N, -1)[:, :3]
+        check("btd_set_state", self._h, pos.ctypes.data_as(C.c_void_p), None if vel is None else vel.ctypes.data_as(C.c_void_p))
+
+    def state(self):
+        pos = np.zeros((self.N, 4), np.float32)
+        vel = np.zeros((self.N, 4), np.float32)
+        check("btd_get_state", self._h, pos.ctypes.data_as(C.c_void_p), vel.ctypes.data_as(C.c_void_p))
+        return pos, vel
+
+    @property
+    def x(self):
+        return self.state()[0][:, :3]
+
+    def set_segments(self, rest_length=None, intact=None, cut_mask=None, seg_flags=None, fail_site=None, tails=None):
+        """setSegments (solver.ts:821-824)."""
+        n2 = 2 * self.N
+        arrs = [None if rest_length is None else _f(rest_length, n2), None if intact is None else _f(intact, n2),
+                None if cut_mask is None else _f(cut_mask, n2, np.uint32),
+                None if seg_flags is None else _f(seg_flags, n2, np.uint32),
+                None if fail_site is None else _f(fail_site, n2), None if tails is None else _f(tails, 4 * self.N)]
+        check("btd_set_segments", self._h, *[None if a is None else a.ctypes.data_as(C.c_void_p) for a in arrs])
+
+    def segments(self):
+        n2 = 2 * self.N
+        rest, intact, fail = (np.zeros(n2, np.float32) for _ in range(3))
+        cut, flags = np.zeros(n2, np.uint32), np.zeros(n2, np.uint32)
+        tails = np.zeros(4 * self.N, np.float32)
+        check("btd_get_segments", self._h, *[a.ctypes.data_as(C.c_void_p) for a in (rest, intact, cut, flags, fail, tails)])
+        return dict(rest_length=rest, intact=intact, cut_mask=cut, seg_flags=flags, fail_site=fail, tails=tails)
+
+    def set_field(self, damage):
+        """setField (solver.ts:827-830): 2 damage codes per crossing."""
+        d = _f(damage, 2 * self.C, np.uint8)
+        check("btd_set_field", self._h, d.ctypes.data_as(C.c_void_p))
+
+    def field(self):
+        d = np.zeros(2 * self.C, np.uint8)
+        check("btd_get_field", self._h, d.ctypes.data_as(C.c_void_p))
+        return d
+
+    def reset_state(self):
+        check("btd_reset_state", self._h)
+
+    # ---- knobs
+    def set_floor(self, z):
+        """setFloor (solver.ts:796-801); None removes the floor."""
+        check("btd_set_floor", self._h, 0 if z is None else 1, 0.0 if z is None else float(z))
+
+    def set_timestep(self, h):
+        check("btd_set_timestep", self._h, float(h))
+
+    def set_history_enabled(self, on):
+        check("btd_set_history", self._h, int(bool(on)))
+
+    def set_newton_tolerance(self, tol):
+        check("btd_set_newton_tolerance", self._h, float(tol))
+
+    def set_pcg(self, max_iterations, rel_tol=0.0):
+        check("btd_set_pcg", self._h, int(max_iterations), float(rel_tol))
+
+    def counters(self):
+        out = np.zeros(32, np.uint32)
+        check("btd_read_counters", self._h, out.ctypes.data_as(C.c_void_p), 32)
+        return out
+
+    def counter_dict(self):
+        c = self.counters()
+        f = c.view(np.float32)
+        d = {name: int(c[k]) for k, name in COUNTER_NAMES.items()}
+        d["max_speed"] = float(f[2])
+        d["alpha"] = float(f[3])
+        d["rel_residual"] = float(f[19])
+        d["max_update"] = [float(f[4 + k]) for k in range(8)]
+        return d
+
+    def clear_counters(self):
+        check("btd_clear_counters", self._h)
+
+    # ---- stage encoders (solver.ts:574-728)
+    def encode_predict(self):
+        check("btd_stage_predict", self._h)
+
+    def encode_assemble(self, coarse=True):
+        check("btd_stage_assemble", self._h, int(coarse))
+
+    def encode_vcycle(self):
+        check("btd_stage_vcycle", self._h)
+
+    def encode_pcg(self):
+        check("btd_stage_pcg", self._h)
+
+    def encode_line_search(self):
+        e, m = np.zeros(4), np.zeros(4)
+        check("btd_stage_linesearch", self._h, e.ctypes.data_as(C.c_void_p), m.ctypes.data_as(C.c_void_p))
+        return e, m
+
+    def encode_apply(self, iteration=0):
+        check("btd_stage_apply", self._h, iteration)
+
+    def encode_newton_iteration(self, iteration=0):
+        check("btd_stage_newton", self._h, iteration)
+
+    def encode_finalize(self):
+        check("btd_stage_finalize", self._h)
+
+    def encode_damage(self):
+        check("btd_stage_damage", self._h)
+
+    STAGES = {"matvec": 0, "smooth": 1, "assemble": 2, "vcycle": 3, "hierarchy": 4, "substep": 5}
+
+    def launch_count(self, substeps, newton_iterations, pcg_iterations):
+        """Kernel launches of `substeps` substeps with the given Newton and PCG iteration totals."""
+        out = C.c_int64()
+        check("btd_launch_count", self._h, substeps, newton_iterations, pcg_iterations, C.byref(out))
+        return out.value
+
+    def profile_stage(self, stage, reps=10, flush=True):
+        """Mean device ms of one launch of a stage (CUDA events on the solver's stream)."""
+        ms = C.c_float()
+        check("btd_profile_stage", self._h, self.STAGES[stage], reps, int(flush), C.byref(ms))
+        return ms.value
+
+    # ---- levels and buffers
+    def level_count(self):
+        n = C.c_int32()
+        check("btd_level_count", self._h, C.byref(n))
+        return n.value
+
+    def level_nodes(self, k):
+        n = C.c_int32()
+        check("btd_level_nodes", self._h, k, C.byref(n))
+        return n.value
+
+    def read_operator(self, k):
+        """Level k's operator in the CPU reference's 25-offset layout: (N, 25, 3, 3), fixed (N,)."""
+        n = self.level_nodes(k)
+        A = np.zeros(n * 225)
+        fixed = np.zeros(n, np.uint8)
+        check("btd_read_operator", self._h, k, A.ctypes.data_as(C.c_void_p), fixed.ctypes.data_as(C.c_void_p))
+        return A.reshape(n, 25, 3, 3), fixed
+
+    VEC = {"X": 0, "B": 1, "R": 2, "delta": 3, "dx": 4, "pred": 5}
+
+    def read_vector(self, which, level=0):
+        n = self.level_nodes(level) if self.VEC[which] <= 2 else self.N
+        out = np.zeros((n, 4), np.float32)
+        check("btd_read_vector", self._h, self.VEC[which], level, out.ctypes.data_as(C.c_void_p))
+        return out[:, :3].astype(np.float64)
+
+    def write_vector(self, which, values, level=0):
+        n = self.level_nodes(level) if self.VEC[which] <= 2 else self.N
+        buf = np.zeros((n, 4), np.float32)
+        buf[:, :3] = np.asarray(values).reshape(n, 3)
+        check("btd_write_vector", self._h, self.VEC[which], level, buf.ctypes.data_as(C.c_void_p))

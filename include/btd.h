@@ -227,6 +227,23 @@ int btd_read_operator(btd_solver* s, int32_t level, double* out, uint8_t* fixed)
 int btd_read_vector(btd_solver* s, int32_t which, int32_t level, float* out4);
 int btd_write_vector(btd_solver* s, int32_t which, int32_t level, const float* in4);
 
+/* Per-stage timing (the reference's tools/gpu/scripts/profile.ts: timestamp queries per pass):
+ * launches stage `which` `reps` times on the solver's stream on the current system and returns the
+ * mean device time of one launch in ms, from CUDA events recorded on that stream. With flush != 0 a
+ * 256 MiB buffer is rewritten before every launch (outside the events) so each launch starts with a
+ * cold L2. which: 0 fine matvec (SpMV + dot), 1 fine smoother sweep (6 colour launches), 2 fine
+ * assembly, 3 V-cycle, 4 Galerkin hierarchy (prolongation weights + RAP of every level), 5 substep. */
+#define BTD_STAGE_MATVEC 0
+#define BTD_STAGE_SMOOTH 1
+#define BTD_STAGE_ASSEMBLE 2
+#define BTD_STAGE_VCYCLE 3
+#define BTD_STAGE_HIERARCHY 4
+#define BTD_STAGE_SUBSTEP 5 /* a whole substep: one launch of the captured substep graph */
+int btd_profile_stage(btd_solver* s, int32_t which, int32_t reps, int32_t flush, float* ms_per_launch);
+/* Kernel launches of substeps that ran `newton_iterations` Newton iterations and `pcg_iterations`
+ * PCG iterations in total (the graph's nodes that are kernels, loop bodies counted per pass). */
+int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton_iterations, int32_t pcg_iterations, int64_t* out);
+
 /* Last error message of the calling thread (always NUL-terminated when n > 0). */
 int btd_last_error(char* buf, size_t n);
 
