@@ -145,6 +145,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--eager", action="store_true", help="launch kernel by kernel (for per-kernel profilers)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     w = WORKLOADS[args.workload]
@@ -170,6 +171,8 @@ def main():
     sc = build_scene(btd, w)
     params = btd.configs.solver_params(w["h"], w["newton"], w["rel"])
     gpu = btd.GpuSolver(sc, params)
+    if args.eager:
+        gpu.set_graph_mode(False)
 
     def barrier():
         if dist is not None:

@@ -173,6 +173,7 @@ SIGNATURES = {
     "btd_set_history": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_set_newton_tolerance": ([C.c_void_p, C.c_float], C.c_int),
     "btd_set_pcg": ([C.c_void_p, C.c_int32, C.c_double], C.c_int),
+    "btd_set_graph_mode": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_read_counters": ([C.c_void_p, C.c_void_p, C.c_int32], C.c_int),
     "btd_clear_counters": ([C.c_void_p], C.c_int),
     "btd_stage_predict": ([C.c_void_p], C.c_int),

@@ -154,7 +154,9 @@ __global__ void __launch_bounds__(RAP_THREADS) k_rap(DLevel F, DLevel C) {
             int Ii = ki ? bri.hi : bri.lo;
             float wJ = pwSlot(wb, ki + 2 * kj);
             if (wJ == 0.f) continue;
-            int o = (J - cj + 2) * 5 + (Ii - ci + 2);
+            const int oj = J - cj + 2, oi = Ii - ci + 2;
+            if ((unsigned)oj > 4u || (unsigned)oi > 4u) continue;  // radius-2 closure (galerkin throws there)
+            int o = oj * 5 + oi;
             float s = wa * wJ;
             float* p = a25 + 6 * o;
             p[0] += Ab.xx * s, p[1] += Ab.xy * s, p[2] += Ab.xz * s, p[3] += Ab.yy * s, p[4] += Ab.yz * s, p[5] += Ab.zz * s;

@@ -48,6 +48,103 @@ __device__ __forceinline__ M3 m3Add(const M3& x, const M3& y) {
   return o;
 }
 
+// Line row of node n (k-th on its line, family fam) from a fine row: diagonal plus the Frobenius
+// majorisation of the +-2 along-line couplings, the +1 along-line block, and the rhs with every other
+// coupling lagged at the current iterate (lineRow, smooth.wgsl:49-84; smoothLines,
+// newtonMultigrid.ts:676-720). All loads are issued before any use.
+__device__ __forceinline__ void fineLineRow(const DLevel& L, int n, int k, int len, int fam, Sym* Bk, Sym* Ck, float3* rr) {
+  float4 pl[FINE_PLANES];
+#pragma unroll
+  for (int p = 0; p < FINE_PLANES; ++p) pl[p] = __ldg(&L.op[(size_t)p * L.N + n]);
+  const uint2 cc = L.coord[n];
+  const int i = cc.x & 0xFFFF, j = cc.x >> 16;
+  const DLevelLayer ly = L.layers[cc.y];
+  float3 xm[12];
+  bool ok[12];
+#pragma unroll
+  for (int q = 0; q < 12; ++q) {
+    const int2 o = fineOffset(q);
+    const int ii = i + o.x, jj = j + o.y;
+    ok[q] = ii >= 0 && jj >= 0 && ii < ly.nx && jj < ly.ny;
+    const int m = ok[q] ? ly.offset + jj * ly.nx + ii : n;
+    xm[q] = f3(L.X[m]);
+  }
+  const float3 xn = f3(L.X[n]);
+  float3 r = f3(L.B[n]);
+  const float* row = reinterpret_cast<const float*>(pl);
+  auto blk = [&](int b) { return Sym{row[6 * b], row[6 * b + 1], row[6 * b + 2], row[6 * b + 3], row[6 * b + 4], row[6 * b + 5]}; };
+  // along-line couplings: u-lines use +u (0), -u (1), +-2u scalars (8, 9); v-lines +v (2), -v (3), +-2v (10, 11)
+  const int qNext = fam == 0 ? 0 : 2, qPrev = fam == 0 ? 1 : 3, qS = fam == 0 ? 8 : 10;
+  float maj = 0.f;
+#pragma unroll
+  for (int q = 0; q < 12; ++q) {
+    if (q == qPrev) continue;
+    if (q == qNext) {
+      if (k + 1 < len) *Ck = blk(q + 1);
+      continue;
+    }
+    if (!ok[q]) continue;
+    if (q < 8) {
+      r -= blk(q + 1) * xm[q];
+    } else {
+      const float sc = row[54 + (q - 8)];
+      if (q == qS || q == qS + 1) maj += 1.7320508075688772f * fabsf(sc);
+      r -= sc * xm[q];
+    }
+  }
+  *Bk = blk(0) + symId(maj);
+  *rr = r + maj * xn;
+}
+
+// The same from a coarse (25-block) row, one stencil row of 5 blocks (30 floats) at a time.
+__device__ __forceinline__ void coarseLineRow(const DLevel& L, int n, int k, int len, int fam, Sym* Bk, Sym* Ck, float3* rr) {
+  const uint2 cc = L.coord[n];
+  const int i = cc.x & 0xFFFF, j = cc.x >> 16;
+  const DLevelLayer ly = L.layers[cc.y];
+  const float3 xn = f3(L.X[n]);
+  float3 r = f3(L.B[n]);
+  float maj = 0.f;
+  Sym D = symZero();
+#pragma unroll
+  for (int dj = -2; dj <= 2; ++dj) {
+    // floats 30 (dj + 2) .. + 29 live in planes p0 .. p0 + 8
+    const int f0 = 30 * (dj + 2), p0 = f0 >> 2, sh = f0 & 3;
+    float4 pl[9];
+#pragma unroll
+    for (int p = 0; p < 9; ++p) pl[p] = p0 + p < COARSE_PLANES ? __ldg(&L.op[(size_t)(p0 + p) * L.N + n]) : make_float4(0, 0, 0, 0);
+    float3 xm[5];
+    bool ok[5];
+#pragma unroll
+    for (int di = -2; di <= 2; ++di) {
+      const int ii = i + di, jj = j + dj;
+      ok[di + 2] = ii >= 0 && jj >= 0 && ii < ly.nx && jj < ly.ny;
+      const int m = ok[di + 2] ? ly.offset + jj * ly.nx + ii : n;
+      xm[di + 2] = f3(L.X[m]);
+    }
+    const float* row = reinterpret_cast<const float*>(pl) + sh;
+#pragma unroll
+    for (int di = -2; di <= 2; ++di) {
+      const float* b = row + 6 * (di + 2);
+      const Sym B = {b[0], b[1], b[2], b[3], b[4], b[5]};
+      const int along = fam == 0 ? di : dj, across = fam == 0 ? dj : di;
+      if (across == 0 && along == 0) {
+        D = B;
+        continue;
+      }
+      if (across == 0 && along == -1) continue;
+      if (across == 0 && along == 1) {
+        if (k + 1 < len) *Ck = B;
+        continue;
+      }
+      if (!ok[di + 2]) continue;
+      if (across == 0) maj += symFrob(B);
+      r -= B * xm[di + 2];
+    }
+  }
+  *Bk = D + symId(maj);
+  *rr = r + maj * xn;
+}
+
 template <class Rows>
 __global__ void __launch_bounds__(SM_THREADS) k_smooth(DLevel L, const int4* __restrict__ lines, int first) {
   extern __shared__ float sm[];
@@ -67,35 +164,16 @@ __global__ void __launch_bounds__(SM_THREADS) k_smooth(DLevel L, const int4* __r
   float* qr = qU + 9 * 2 * SM_PMAX;
   float* qx = qr + 3 * 2 * SM_PMAX;
 
-  // ---- phase 1: line rows
+  // ---- phase 1: line rows (each thread issues its row's and its neighbours' loads together)
   for (int k = tid; k < len; k += SM_THREADS) {
     const int n = n0 + k * st;
     Sym Bk = symId(1.f), Ck = symZero();
     float3 r = make_float3(0, 0, 0);
     if (!L.fixed[n]) {
-      int i, j, l;
-      nodeCoord(L, n, &i, &j, &l);
-      const DLevelLayer Ly = L.layers[l];
-      Sym D = Rows::diag(L.op, L.N, n);
-      r = f3(L.B[n]);
-      float maj = 0.f;
-      for (int c = 0; c < Rows::NC; ++c) {
-        const int2 off = Rows::offset(c);
-        const int along = fam == 0 ? off.x : off.y;
-        const int across = fam == 0 ? off.y : off.x;
-        if (across == 0 && along == -1) continue;
-        if (across == 0 && along == 1) {
-          if (k + 1 < len) Ck = Rows::coupling(L.op, L.N, n, c);
-          continue;
-        }
-        const int m = levelNode(Ly, i + off.x, j + off.y);
-        if (m < 0) continue;
-        const Sym Bc = Rows::coupling(L.op, L.N, n, c);
-        if (across == 0) maj += symFrob(Bc);
-        r -= Bc * f3(L.X[m]);
-      }
-      Bk = D + symId(maj);
-      r += maj * f3(L.X[n]);
+      if constexpr (Rows::NC == 12)
+        fineLineRow(L, n, k, len, fam, &Bk, &Ck, &r);
+      else
+        coarseLineRow(L, n, k, len, fam, &Bk, &Ck, &r);
     }
     stSym(sB + 6 * k, Bk);
     stSym(sC + 6 * k, Ck);

@@ -123,6 +123,7 @@ struct btd_solver {
   // graphs: substep graphs keyed by Newton iteration count; the standalone PCG graph
   std::map<int, cudaGraphExec_t> substepExec;
   cudaGraphExec_t pcgExec = nullptr;
+  bool useGraphs = true;
   void* flushBuf = nullptr;  // profiling only: rewritten to evict L2 between timed launches
 
   template <class T>
@@ -284,6 +285,38 @@ struct btd_solver {
     encPcgBody(bodyStream, a);
     cudaGraph_t out;
     CK(cudaStreamEndCapture(bodyStream, &out));
+  }
+
+  // The same PCG launched kernel by kernel, the stop read back after every iteration.
+  void runPCGEager(cudaStream_t s) {
+    PcgArgs a = pcgArgs(0, 0);
+    k_pcg_init<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    encVCycle(s, 0);
+    k_pcg_dot_rz<<<redBlocks, RED_THREADS, 0, s>>>(a, 1);
+    k_pcg_update_p<<<blocksFor(N, 256), 256, 0, s>>>(a, 1);
+    k_pcg_matvec<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    k_pcg_update_xr<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    for (;;) {
+      int conv = 0;
+      CK(cudaMemcpyAsync(&conv, &dScal->converged, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      if (conv) break;
+      encPcgBody(s, a);
+    }
+  }
+
+  void runSubstepEager(int newtonIterations) {
+    cudaStream_t s = stream;
+    CK(cudaMemsetAsync(dCounters + CNT_UPDATE, 0, sizeof(uint32_t) * MAX_NEWTON, s));
+    encPredict(s);
+    for (int it = 0; it < newtonIterations; ++it) {
+      encAssemble(s, it == 0 || !params.lag_coarse);
+      runPCGEager(s);
+      encLineSearch(s);
+      encApply(s, it);
+    }
+    encFinalize(s);
+    CK(cudaGetLastError());
   }
 
   void encLineSearch(cudaStream_t s) {
@@ -661,15 +694,22 @@ int btd_substep(btd_solver* s, int32_t min_iterations, int32_t max_iterations) {
     checkSolver(s);
     int iters = std::min(MAX_NEWTON, std::max(s->params.newton_iterations, (int)min_iterations));
     (void)max_iterations;
-    CK(cudaGraphLaunch(s->substepGraph(iters), s->stream));
+    if (s->useGraphs)
+      CK(cudaGraphLaunch(s->substepGraph(iters), s->stream));
+    else
+      s->runSubstepEager(iters);
   });
 }
 
 int btd_substeps(btd_solver* s, int32_t count) {
   GUARD({
     checkSolver(s);
-    cudaGraphExec_t ex = s->substepGraph(s->params.newton_iterations);
-    for (int k = 0; k < count; ++k) CK(cudaGraphLaunch(ex, s->stream));
+    if (!s->useGraphs) {
+      for (int k = 0; k < count; ++k) s->runSubstepEager(s->params.newton_iterations);
+    } else {
+      cudaGraphExec_t ex = s->substepGraph(s->params.newton_iterations);
+      for (int k = 0; k < count; ++k) CK(cudaGraphLaunch(ex, s->stream));
+    }
   });
 }
 
@@ -804,6 +844,13 @@ int btd_set_newton_tolerance(btd_solver* s, float tol) {
     s->params.newton_tolerance = tol;
     s->pushParams();
     s->sync();
+  });
+}
+
+int btd_set_graph_mode(btd_solver* s, int32_t use_graphs) {
+  GUARD({
+    checkSolver(s);
+    s->useGraphs = use_graphs != 0;
   });
 }
 
@@ -959,7 +1006,10 @@ int btd_profile_stage(btd_solver* s, int32_t which, int32_t reps, int32_t flush,
           s->encHierarchy(s->stream);
           break;
         default:
-          CK(cudaGraphLaunch(s->substepGraph(s->params.newton_iterations), s->stream));
+          if (s->useGraphs)
+            CK(cudaGraphLaunch(s->substepGraph(s->params.newton_iterations), s->stream));
+          else
+            s->runSubstepEager(s->params.newton_iterations);
       }
       CK(cudaEventRecord(e1, s->stream));
       CK(cudaEventSynchronize(e1));

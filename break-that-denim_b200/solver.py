@@ -132,6 +132,10 @@ class GpuSolver:
     def set_newton_tolerance(self, tol):
         check("btd_set_newton_tolerance", self._h, float(tol))
 
+    def set_graph_mode(self, use_graphs):
+        """True: one captured graph per substep; False: kernel by kernel (for per-kernel profilers)."""
+        check("btd_set_graph_mode", self._h, int(bool(use_graphs)))
+
     def set_pcg(self, max_iterations, rel_tol=0.0):
         check("btd_set_pcg", self._h, int(max_iterations), float(rel_tol))
 

@@ -192,6 +192,10 @@ int btd_set_timestep(btd_solver* s, float h);
 int btd_set_history(btd_solver* s, int32_t enabled);
 /* setNewtonTolerance (solver.ts:782-785). */
 int btd_set_newton_tolerance(btd_solver* s, float tolerance);
+/* Execution mode: 1 (default) launches each substep as one captured CUDA graph whose PCG loop is a
+ * device-side while-node; 0 launches the same kernels one by one with the PCG stop read back by
+ * the host after every iteration (for per-kernel profilers, which cannot see into such graphs). */
+int btd_set_graph_mode(btd_solver* s, int32_t use_graphs);
 /* Extension: PCG cap and relative-residual stop (0 = fixed count as the reference). */
 int btd_set_pcg(btd_solver* s, int32_t max_iterations, double rel_tol);
 
