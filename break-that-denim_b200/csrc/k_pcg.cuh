@@ -209,6 +209,52 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_update_xr(PcgArgs a) {
   }
 }
 
+// y = A x and x . y for a fine-level operator (the PCG matvec of pcg.wgsl:268-287 without its scalar
+// bookkeeping). `coord` may be null for a single-layer lattice, whose coordinates follow from nx.
+struct MatvecArgs {
+  int N, nx, ny;
+  const uint2* __restrict__ coord;
+  const DLevelLayer* __restrict__ layers;
+  const float4* __restrict__ op;
+  const uint32_t* __restrict__ fixed;
+  const float4* __restrict__ x;
+  float4* y;
+  double* xy;
+  Reduce red;
+};
+
+__global__ void __launch_bounds__(RED_THREADS) k_matvec_dot(MatvecArgs a) {
+  double v[1] = {0.0};
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < a.N; n += gridDim.x * blockDim.x) {
+    float3 y = make_float3(0, 0, 0);
+    if (!a.fixed[n]) {
+      int i, j;
+      DLevelLayer L;
+      if (a.coord) {
+        const uint2 c = a.coord[n];
+        i = c.x & 0xFFFF, j = c.x >> 16;
+        L = a.layers[c.y];
+      } else {
+        i = n % a.nx, j = n / a.nx;
+        L = {0, a.nx, a.ny, 0};
+      }
+      y = FineRows::diag(a.op, a.N, n) * f3(a.x[n]);
+#pragma unroll
+      for (int k = 0; k < FineRows::NC; ++k) {
+        int2 off = FineRows::offset(k);
+        int m = levelNode(L, i + off.x, j + off.y);
+        if (m < 0) continue;
+        y += FineRows::coupling(a.op, a.N, n, k) * f3(a.x[m]);
+      }
+    }
+    a.y[n] = make_float4(y.x, y.y, y.z, 0.f);
+    float3 x = f3(a.x[n]);
+    v[0] += (double)y.x * x.x + (double)y.y * x.y + (double)y.z * x.z;
+  }
+  double out[1];
+  if (gridReduce<1>(a.red, v, out) && threadIdx.x == 0) *a.xy = out[0];
+}
+
 // ------------------------------------------------------------------------------------ line search
 
 constexpr float LINE_NOISE = 4e-6f;

@@ -15,6 +15,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -447,6 +448,8 @@ void checkSolver(btd_solver* s) {
 }  // namespace
 
 extern "C" {
+
+static float4* vectorPtr(btd_solver* s, int which, int level, size_t* count);
 
 int btd_default_params(btd_params* out) {
   if (!out) return BTD_E_INVALID;
@@ -1104,6 +1107,61 @@ int btd_read_operator(btd_solver* s, int32_t level, double* out, uint8_t* fixed)
     }
     if (fixed)
       for (int n = 0; n < L.N; ++n) fixed[n] = fx[n] ? 1 : 0;
+  });
+}
+
+int btd_device_buffer(btd_solver* s, int32_t which, int32_t level, void** ptr, size_t* bytes) {
+  GUARD({
+    checkSolver(s);
+    if (!ptr) throw std::invalid_argument("null output");
+    size_t b = 0;
+    void* p = nullptr;
+    if (which == BTD_BUF_X) {
+      p = s->x, b = sizeof(float4) * s->N;
+    } else if (which == BTD_BUF_V) {
+      p = s->v, b = sizeof(float4) * s->N;
+    } else if (which == BTD_BUF_OP || which == BTD_BUF_FIXED) {
+      if (level < 0 || level >= (int)s->levels.size()) throw std::invalid_argument("level out of range");
+      Level& L = s->levels[level];
+      if (which == BTD_BUF_OP)
+        p = L.op, b = sizeof(float4) * (size_t)(L.fine ? FINE_PLANES : COARSE_PLANES) * L.N;
+      else
+        p = L.fixed, b = sizeof(uint32_t) * L.N;
+    } else {
+      size_t n = 0;
+      p = vectorPtr(s, which, level, &n);
+      b = sizeof(float4) * n;
+    }
+    *ptr = p;
+    if (bytes) *bytes = b;
+  });
+}
+
+int btd_stage_matvec(btd_solver* s, const float* x4, float* y4, double* xy) {
+  GUARD({
+    checkSolver(s);
+    if (!x4) throw std::invalid_argument("null input");
+    const Level& F = s->levels[0];
+    CK(cudaMemcpyAsync(s->p, x4, sizeof(float4) * s->N, cudaMemcpyHostToDevice, s->stream));
+    MatvecArgs a;
+    a.N = s->N;
+    a.nx = F.layers[0].nx;
+    a.ny = F.layers[0].ny;
+    a.coord = F.dCoord;
+    a.layers = F.dLayers;
+    a.op = F.op;
+    a.fixed = F.fixed;
+    a.x = s->p;
+    a.y = s->Ap;
+    a.xy = &s->dScal->pAp;
+    a.red = s->reduce();
+    k_matvec_dot<<<s->redBlocks, RED_THREADS, 0, s->stream>>>(a);
+    CK(cudaGetLastError());
+    if (y4) CK(cudaMemcpyAsync(y4, s->Ap, sizeof(float4) * s->N, cudaMemcpyDeviceToHost, s->stream));
+    double v = 0;
+    CK(cudaMemcpyAsync(&v, &s->dScal->pAp, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+    if (xy) *xy = v;
   });
 }
 

@@ -221,6 +221,23 @@ class GpuSolver:
         return A.reshape(n, 25, 3, 3), fixed
 
     VEC = {"X": 0, "B": 1, "R": 2, "delta": 3, "dx": 4, "pred": 5}
+    BUF = {"op": 16, "fixed": 17, "x": 18, "v": 19}
+
+    def device_buffer(self, which, level=0):
+        """(device pointer, bytes) of a solver buffer, for zero-copy consumers."""
+        ptr, n = C.c_void_p(), C.c_size_t()
+        code = self.BUF[which] if which in self.BUF else self.VEC[which]
+        check("btd_device_buffer", self._h, code, level, C.byref(ptr), C.byref(n))
+        return ptr.value, n.value
+
+    def matvec(self, x):
+        """y = A x and x . y with the last assembled fine operator (x: (N, 3))."""
+        xb = np.zeros((self.N, 4), np.float32)
+        xb[:, :3] = np.asarray(x).reshape(self.N, 3)
+        yb = np.zeros((self.N, 4), np.float32)
+        xy = C.c_double()
+        check("btd_stage_matvec", self._h, xb.ctypes.data_as(C.c_void_p), yb.ctypes.data_as(C.c_void_p), C.byref(xy))
+        return yb[:, :3].astype(np.float64), xy.value
 
     def read_vector(self, which, level=0):
         n = self.level_nodes(level) if self.VEC[which] <= 2 else self.N

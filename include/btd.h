@@ -229,6 +229,20 @@ int btd_read_operator(btd_solver* s, int32_t level, double* out, uint8_t* fixed)
 #define BTD_VEC_DX 4
 #define BTD_VEC_PRED 5
 int btd_read_vector(btd_solver* s, int32_t which, int32_t level, float* out4);
+/* Zero-copy access for consumers that bind the solver's buffers (the renderer and tools read
+ * GpuSolver.x, .levels[k].op etc. directly, solver.ts:198-263): device pointer and size in bytes of
+ * buffer `which` (BTD_VEC_* above, or BTD_BUF_*) of `level`. The pointer stays valid until
+ * btd_destroy. Fine operator rows are 15 float4 planes, plane p of node n at op[p * N + n]: nine
+ * symmetric blocks (xx xy xz yy yz zz) diag, +u, -u, +v, -v, +u+v, -u-v, -u+v, +u-v, then the scalar
+ * couplings +2u, -2u, +2v, -2v; coarse rows are 38 planes of 25 blocks in offset order. */
+#define BTD_BUF_OP 16
+#define BTD_BUF_FIXED 17
+#define BTD_BUF_X 18
+#define BTD_BUF_V 19
+int btd_device_buffer(btd_solver* s, int32_t which, int32_t level, void** ptr, size_t* bytes);
+/* Stage: y = A x and x . y with the fine operator of the last assembly (the PCG matvec, pcg.wgsl:268-287),
+ * x and y 4 floats per node on the host. Uses the solver's own reduction scratch. */
+int btd_stage_matvec(btd_solver* s, const float* x4, float* y4, double* xy);
 int btd_write_vector(btd_solver* s, int32_t which, int32_t level, const float* in4);
 
 /* Per-stage timing (the reference's tools/gpu/scripts/profile.ts: timestamp queries per pass):
