@@ -194,6 +194,8 @@ SIGNATURES = {
     "btd_launch_count": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, _p(C.c_int64)], C.c_int),
     "btd_device_buffer": ([C.c_void_p, C.c_int32, C.c_int32, _p(C.c_void_p), _p(C.c_size_t)], C.c_int),
     "btd_stage_matvec": ([C.c_void_p, C.c_void_p, C.c_void_p, _p(C.c_double)], C.c_int),
+    "btd_matvec_noalloc": ([C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                            C.c_void_p], C.c_int),
     "btd_last_error": ([C.c_char_p, C.c_size_t], C.c_int),
 }
 

@@ -1200,3 +1200,72 @@ int btd_write_vector(btd_solver* s, int32_t which, int32_t level, const float* i
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Allocation-free matvec. Some callers cannot allocate device memory at the point where they call
+// into the solve: a host that owns a fixed device pool (a game engine's or a plugin host's
+// allocator), a real-time or frame-budgeted thread where cudaMalloc's implicit synchronisation is
+// not allowed, or code running while another component captures the stream into a CUDA graph.
+// btd_matvec_noalloc serves them: its reduction scratch is the file-scope array below, sized for
+// NOALLOC_MAX_NODES nodes and resident on every GPU that loads this library until the process
+// exits. Every call shares that array and leaves its last contents there; calls that overlap on the
+// GPU (different streams, threads or devices sharing a context) race on it and must be serialised
+// by the caller.
+
+namespace {
+
+constexpr int NOALLOC_MAX_BLOCKS = 2048;                              // one partial per 256-node block
+constexpr int NOALLOC_MAX_NODES = NOALLOC_MAX_BLOCKS * RED_THREADS;  // 524,288 nodes
+constexpr size_t NOALLOC_TICKET_BYTES = 256;
+constexpr size_t NOALLOC_BYTES = NOALLOC_TICKET_BYTES + sizeof(double) * 8 * NOALLOC_MAX_BLOCKS;  // 131,328 bytes
+
+static __device__ __align__(256) unsigned char g_noallocScratch[NOALLOC_BYTES];
+
+std::mutex g_noallocMutex;
+void* g_noallocAddr[256] = {};
+
+// Device address of the scratch array on the current device, looked up once per device.
+void* noallocScratch() {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) throw std::runtime_error("device index out of range");
+  std::lock_guard<std::mutex> lock(g_noallocMutex);
+  if (!g_noallocAddr[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noallocScratch));
+    g_noallocAddr[dev] = p;
+  }
+  return g_noallocAddr[dev];
+}
+
+}  // namespace
+
+extern "C" int btd_matvec_noalloc(int32_t nx, int32_t ny, const void* op, const void* fixed, const void* x, void* y,
+                                  double* xy, void* stream) {
+  GUARD({
+    if (nx < 2 || ny < 2) throw std::invalid_argument("btd_matvec_noalloc: the lattice needs nx, ny >= 2");
+    const long long N = (long long)nx * ny;
+    if (N > NOALLOC_MAX_NODES)
+      throw std::invalid_argument("btd_matvec_noalloc: " + std::to_string(N) + " nodes exceed the allocation-free maximum of " +
+                                  std::to_string(NOALLOC_MAX_NODES));
+    if (!op || !fixed || !x || !y || !xy) throw std::invalid_argument("btd_matvec_noalloc: null device pointer");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned char* scratch = static_cast<unsigned char*>(noallocScratch());
+    // the reduction ticket must start at zero; the partials are written before they are read
+    CK(cudaMemsetAsync(scratch, 0, sizeof(unsigned), st));
+    MatvecArgs a;
+    a.N = (int)N;
+    a.nx = nx;
+    a.ny = ny;
+    a.coord = nullptr;
+    a.layers = nullptr;
+    a.op = static_cast<const float4*>(op);
+    a.fixed = static_cast<const uint32_t*>(fixed);
+    a.x = static_cast<const float4*>(x);
+    a.y = static_cast<float4*>(y);
+    a.xy = xy;
+    a.red = {reinterpret_cast<double*>(scratch + NOALLOC_TICKET_BYTES), reinterpret_cast<unsigned*>(scratch)};
+    k_matvec_dot<<<blocksFor((int)N, RED_THREADS), RED_THREADS, 0, st>>>(a);
+    CK(cudaGetLastError());
+  });
+}

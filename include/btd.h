@@ -262,6 +262,20 @@ int btd_profile_stage(btd_solver* s, int32_t which, int32_t reps, int32_t flush,
  * PCG iterations in total (the graph's nodes that are kernels, loop bodies counted per pass). */
 int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton_iterations, int32_t pcg_iterations, int64_t* out);
 
+/* y = A x and x . y for a single-layer nx x ny fine operator on caller-owned DEVICE buffers (op in
+ * the fine-row layout of btd_device_buffer, fixed flags as uint32, x and y 4 floats per node, xy one
+ * double), enqueued on `stream` (a cudaStream_t; NULL: the legacy default stream); the results are
+ * ready when that stream reaches this point. No counterpart in the reference: this entry point
+ * allocates nothing, for callers that cannot call cudaMalloc (a host with its own fixed device
+ * pool, a frame-budgeted thread where cudaMalloc's implicit synchronisation is not allowed, code
+ * running while a stream is being captured). Its reduction scratch is a static device array of
+ * 131,328 bytes that every GPU loading the library holds until exit; lattices of more than
+ * 524,288 nodes are rejected with BTD_E_INVALID. The first call on each device looks the array's
+ * address up (cudaGetSymbolAddress) and should come before any stream capture. All calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the caller. */
+int btd_matvec_noalloc(int32_t nx, int32_t ny, const void* op, const void* fixed, const void* x, void* y, double* xy,
+                       void* stream);
+
 /* Last error message of the calling thread (always NUL-terminated when n > 0). */
 int btd_last_error(char* buf, size_t n);
 
