@@ -180,7 +180,7 @@ __device__ __forceinline__ M3 pivotInverse(const M3& m) {
   float a20 = m.a[6], a21 = m.a[7], a22 = m.a[8] + e;
   float c00 = a11 * a22 - a12 * a21, c01 = a12 * a20 - a10 * a22, c02 = a10 * a21 - a11 * a20;
   float det = a00 * c00 + a01 * c01 + a02 * c02;
-  float id = 1.f / det;
+  float id = __frcp_rn(det);
   M3 o = {{c00 * id, (a02 * a21 - a01 * a22) * id, (a01 * a12 - a02 * a11) * id, c01 * id, (a00 * a22 - a02 * a20) * id,
            (a02 * a10 - a00 * a12) * id, c02 * id, (a01 * a20 - a00 * a21) * id, (a00 * a11 - a01 * a10) * id}};
   bool ok = true;

@@ -180,7 +180,9 @@ __global__ void __launch_bounds__(RAP_THREADS) k_rap(DLevel F, DLevel C) {
   C.fixed[I] = fixedRow ? 1u : 0u;
 }
 
-// r = b - A x on level F (residual, multigrid.wgsl:182-199); fixed rows give 0.
+// r = b - A x on level F (residual, multigrid.wgsl:182-199); fixed rows give 0. Loads are issued
+// unconditionally (neighbour index clamped, outside couplings zero) so they overlap: the fine row
+// in one round trip, the coarse row one stencil row of 5 blocks at a time.
 template <class Rows>
 __global__ void k_residual(DLevel F) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -192,18 +194,62 @@ __global__ void k_residual(DLevel F) {
   int i, j, l;
   nodeCoord(F, n, &i, &j, &l);
   const DLevelLayer L = F.layers[l];
-  float3 r = f3(F.B[n]) - Rows::diag(F.op, F.N, n) * f3(F.X[n]);
-#pragma unroll 4
-  for (int k = 0; k < Rows::NC; ++k) {
-    int2 off = Rows::offset(k);
-    int m = levelNode(L, i + off.x, j + off.y);
-    if (m < 0) continue;
-    r -= Rows::coupling(F.op, F.N, n, k) * f3(F.X[m]);
+  float3 r = f3(F.B[n]);
+  if constexpr (Rows::NC == 12) {
+    float4 pl[FINE_PLANES];
+#pragma unroll
+    for (int p = 0; p < FINE_PLANES; ++p) pl[p] = __ldg(&F.op[(size_t)p * F.N + n]);
+    float3 xm[12];
+    bool ok[12];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+      const int2 o = fineOffset(q);
+      const int ii = i + o.x, jj = j + o.y;
+      ok[q] = ii >= 0 && jj >= 0 && ii < L.nx && jj < L.ny;
+      xm[q] = f3(F.X[ok[q] ? L.offset + jj * L.nx + ii : n]);
+    }
+    const float3 xn = f3(F.X[n]);
+    const float* row = reinterpret_cast<const float*>(pl);
+    r -= Sym{row[0], row[1], row[2], row[3], row[4], row[5]} * xn;
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+      if (!ok[q]) continue;
+      if (q < 8) {
+        const float* b = row + 6 * q + 6;
+        r -= Sym{b[0], b[1], b[2], b[3], b[4], b[5]} * xm[q];
+      } else {
+        r -= row[54 + q - 8] * xm[q];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int dj = -2; dj <= 2; ++dj) {
+      const int f0 = 30 * (dj + 2), p0 = f0 >> 2, sh = f0 & 3;
+      float4 pl[9];
+#pragma unroll
+      for (int p = 0; p < 9; ++p) pl[p] = p0 + p < COARSE_PLANES ? __ldg(&F.op[(size_t)(p0 + p) * F.N + n]) : make_float4(0, 0, 0, 0);
+      float3 xm[5];
+      bool ok[5];
+#pragma unroll
+      for (int di = -2; di <= 2; ++di) {
+        const int ii = i + di, jj = j + dj;
+        ok[di + 2] = ii >= 0 && jj >= 0 && ii < L.nx && jj < L.ny;
+        xm[di + 2] = f3(F.X[ok[di + 2] ? L.offset + jj * L.nx + ii : n]);
+      }
+      const float* row = reinterpret_cast<const float*>(pl) + sh;
+#pragma unroll
+      for (int di = -2; di <= 2; ++di) {
+        if (!ok[di + 2]) continue;
+        const float* b = row + 6 * (di + 2);
+        r -= Sym{b[0], b[1], b[2], b[3], b[4], b[5]} * xm[di + 2];
+      }
+    }
   }
   F.R[n] = make_float4(r.x, r.y, r.z, 0.f);
 }
 
-// b_c = P^T r_f and x_c = 0 (restrictResidual, multigrid.wgsl:204-232).
+// b_c = P^T r_f and x_c = 0 (restrictResidual, multigrid.wgsl:204-232): the up to 3 x 3 fine nodes of
+// coarse node I, all loads issued together.
 __global__ void k_restrict(DLevel F, DLevel C) {
   int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= C.N) return;
@@ -215,18 +261,26 @@ __global__ void k_restrict(DLevel F, DLevel C) {
   int ci, cj, l;
   nodeCoord(C, I, &ci, &cj, &l);
   const DLevelLayer Lf = F.layers[l];
-  int fi0 = coarseToFine(ci, Lf.nx), fj0 = coarseToFine(cj, Lf.ny);
+  const int fi0 = coarseToFine(ci, Lf.nx), fj0 = coarseToFine(cj, Lf.ny);
+  float4 w4[9], r4[9];
+  uint32_t fx[9];
+  bool use[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    const int ai = fi0 - 1 + q % 3, aj = fj0 - 1 + q / 3;
+    use[q] = ai >= 0 && ai < Lf.nx && aj >= 0 && aj < Lf.ny && weightOf(ai, ci, Lf.nx) != 0.f && weightOf(aj, cj, Lf.ny) != 0.f;
+    const int a = use[q] ? levelNode(Lf, ai, aj) : levelNode(Lf, fi0, fj0);
+    w4[q] = F.pw[a];
+    r4[q] = F.R[a];
+    fx[q] = F.fixed[a];
+  }
   float3 s = make_float3(0, 0, 0);
-  for (int aj = fj0 - 1; aj <= fj0 + 1; ++aj) {
-    if (aj < 0 || aj >= Lf.ny || weightOf(aj, cj, Lf.ny) == 0.f) continue;
-    for (int ai = fi0 - 1; ai <= fi0 + 1; ++ai) {
-      if (ai < 0 || ai >= Lf.nx || weightOf(ai, ci, Lf.nx) == 0.f) continue;
-      int a = levelNode(Lf, ai, aj);
-      if (F.fixed[a]) continue;
-      Bracket bai = bracketOf(ai, Lf.nx), baj = bracketOf(aj, Lf.ny);
-      float w = pwSlot(F.pw[a], (bai.lo == ci ? 0 : 1) + 2 * (baj.lo == cj ? 0 : 1));
-      s += w * f3(F.R[a]);
-    }
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    if (!use[q] || fx[q]) continue;
+    const int ai = fi0 - 1 + q % 3, aj = fj0 - 1 + q / 3;
+    const Bracket bai = bracketOf(ai, Lf.nx), baj = bracketOf(aj, Lf.ny);
+    s += pwSlot(w4[q], (bai.lo == ci ? 0 : 1) + 2 * (baj.lo == cj ? 0 : 1)) * f3(r4[q]);
   }
   C.B[I] = make_float4(s.x, s.y, s.z, 0.f);
 }
@@ -239,19 +293,18 @@ __global__ void k_prolong(DLevel F, DLevel C) {
   nodeCoord(F, a, &i, &j, &l);
   const DLevelLayer Lf = F.layers[l];
   const DLevelLayer Lc = C.layers[l];
-  Bracket bi = bracketOf(i, Lf.nx), bj = bracketOf(j, Lf.ny);
-  float4 w = F.pw[a];
+  const Bracket bi = bracketOf(i, Lf.nx), bj = bracketOf(j, Lf.ny);
+  const float4 w = F.pw[a];
+  const float4 x = F.X[a];
+  float3 xc[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) xc[q] = f3(C.X[levelNode(Lc, (q & 1) ? bi.hi : bi.lo, (q & 2) ? bj.hi : bj.lo)]);
   float3 s = make_float3(0, 0, 0);
-  for (int kj = 0; kj < 2; ++kj) {
-    int J = kj ? bj.hi : bj.lo;
-    for (int ki = 0; ki < 2; ++ki) {
-      int Ii = ki ? bi.hi : bi.lo;
-      float wk = pwSlot(w, ki + 2 * kj);
-      if (wk == 0.f) continue;
-      s += wk * f3(C.X[levelNode(Lc, Ii, J)]);
-    }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float wk = pwSlot(w, q);
+    if (wk != 0.f) s += wk * xc[q];
   }
-  float4 x = F.X[a];
   F.X[a] = make_float4(x.x + s.x, x.y + s.y, x.z + s.z, 0.f);
 }
 

@@ -73,12 +73,15 @@ struct Level {
   }
 };
 
-// Line tables (lineTable, lattice.ts:330-350): v-lines coloured i mod 3, then u-lines j mod 3.
+// Line tables (lineTable, lattice.ts:330-350): v-lines coloured i mod 3, then u-lines j mod 3;
+// entry (start node, stride, length, family | layer << 1).
 static void buildLines(Level& L) {
   std::vector<int4> byColour[6];
-  for (auto& ly : L.layers) {
-    for (int i = 0; i < ly.nx; ++i) byColour[i % 3].push_back(make_int4(ly.offset + i, ly.nx, ly.ny, 1));
-    for (int j = 0; j < ly.ny; ++j) byColour[3 + j % 3].push_back(make_int4(ly.offset + j * ly.nx, 1, ly.nx, 0));
+  for (size_t l = 0; l < L.layers.size(); ++l) {
+    const auto& ly = L.layers[l];
+    const int tag = (int)(l << 1);
+    for (int i = 0; i < ly.nx; ++i) byColour[i % 3].push_back(make_int4(ly.offset + i, ly.nx, ly.ny, 1 | tag));
+    for (int j = 0; j < ly.ny; ++j) byColour[3 + j % 3].push_back(make_int4(ly.offset + j * ly.nx, 1, ly.nx, 0 | tag));
     L.maxLine = std::max(L.maxLine, std::max(ly.nx, ly.ny));
   }
   L.lines.clear();
@@ -215,7 +218,7 @@ struct btd_solver {
 
   void encSmooth(cudaStream_t s, int k, bool reverse) {
     Level& L = levels[k];
-    size_t smem = sizeof(float) * smoothSmemFloats(L.maxLine);
+    size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine) : smoothSmemBytes<CoarseRows>(L.maxLine);
     for (int q = 0; q < 6; ++q) {
       int c = reverse ? 5 - q : q;
       int count = L.colourStart[c + 1] - L.colourStart[c];
@@ -618,6 +621,7 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
       }
       cur = nxt;
     }
+    size_t smemFine = 0, smemCoarse = 0;
     for (size_t k = 0; k < s->levels.size(); ++k) {
       Level& L = s->levels[k];
       L.dLayers = s->alloc<DLevelLayer>(L.layers.size());
@@ -639,14 +643,18 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
       L.B = s->alloc<float4>(L.N);
       L.R = s->alloc<float4>(L.N);
       L.pw = s->alloc<float4>(L.N);
-      size_t smem = sizeof(float) * smoothSmemFloats(L.maxLine);
-      if (smem > 48 * 1024) {
-        if (L.fine)
-          CK(cudaFuncSetAttribute(k_smooth<FineRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        else
-          CK(cudaFuncSetAttribute(k_smooth<CoarseRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      }
+      size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine) : smoothSmemBytes<CoarseRows>(L.maxLine);
+      if (smem > 227 * 1024)
+        throw std::invalid_argument("yarn lines of " + std::to_string(L.maxLine) + " nodes exceed the smoother's shared memory");
+      if (L.fine)
+        smemFine = std::max(smemFine, smem);
+      else
+        smemCoarse = std::max(smemCoarse, smem);
     }
+
+    // the smoother's dynamic shared memory: the largest line of each row layout
+    if (smemFine) CK(cudaFuncSetAttribute(k_smooth<FineRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemFine));
+    if (smemCoarse) CK(cudaFuncSetAttribute(k_smooth<CoarseRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemCoarse));
 
     // ---- parameters
     SimParams& P = s->hostP;
