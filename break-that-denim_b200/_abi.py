@@ -180,6 +180,7 @@ SIGNATURES = {
     "btd_stage_assemble": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_stage_vcycle": ([C.c_void_p], C.c_int),
     "btd_stage_pcg": ([C.c_void_p], C.c_int),
+    "btd_stage_smooth": ([C.c_void_p, C.c_int32, C.c_int32], C.c_int),
     "btd_stage_linesearch": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "btd_stage_apply": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_stage_newton": ([C.c_void_p, C.c_int32], C.c_int),
@@ -196,6 +197,13 @@ SIGNATURES = {
     "btd_stage_matvec": ([C.c_void_p, C.c_void_p, C.c_void_p, _p(C.c_double)], C.c_int),
     "btd_matvec_noalloc": ([C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                             C.c_void_p], C.c_int),
+    "btd_set_grip": ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                      C.c_float, C.c_float, C.c_float, C.c_float], C.c_int),
+    "btd_set_grip_target": ([C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
+    "btd_set_grip_pinch": ([C.c_void_p, C.c_int32, C.c_float], C.c_int),
+    "btd_set_grip_hold": ([C.c_void_p, C.c_int32, C.c_float], C.c_int),
+    "btd_release_grip": ([C.c_void_p, C.c_int32], C.c_int),
+    "btd_read_grip": ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, _p(C.c_int32)], C.c_int),
     "btd_last_error": ([C.c_char_p, C.c_size_t], C.c_int),
 }
 

@@ -22,6 +22,7 @@
 
 #include "btd.h"
 #include "common.cuh"
+#include "k_grip.cuh"
 #include "k_history.cuh"
 #include "k_mg.cuh"
 #include "k_pcg.cuh"
@@ -54,6 +55,11 @@ struct Level {
   DLevelLayer* dLayers = nullptr;
   uint2* dCoord = nullptr;
   int4* dLines = nullptr;
+  // line factors (k_line_factor): each line's region starts at facBase[line]
+  std::vector<int> facBase;
+  int* dFacBase = nullptr;
+  float4* fac = nullptr;
+  size_t facF4 = 0;
   float4* op = nullptr;
   uint32_t* fixed = nullptr;
   float4 *X = nullptr, *B = nullptr, *R = nullptr, *pw = nullptr;
@@ -90,6 +96,13 @@ static void buildLines(Level& L) {
     L.lines.insert(L.lines.end(), byColour[c].begin(), byColour[c].end());
   }
   L.colourStart[6] = (int)L.lines.size();
+  L.facBase.clear();
+  size_t off = 0;
+  for (const int4& ln : L.lines) {
+    L.facBase.push_back((int)off);
+    off += lineFactorF4(ln.z);
+  }
+  L.facF4 = off;
 }
 
 }  // namespace btd
@@ -124,7 +137,21 @@ struct btd_solver {
   uint8_t *damage = nullptr, *area = nullptr, *sep = nullptr, *marks = nullptr;
   std::vector<Level> levels;
   std::vector<DLayer> hostLayers;
-  // graphs: substep graphs keyed by Newton iteration count; the standalone PCG graph
+  // grips (interaction.ts attachPatch/setTarget/release): device slots + entries, host mirror of
+  // the slots, the base stiffness of each (setHold scales it) and the slot holding each node
+  GripSlot* dGripSlots = nullptr;
+  GripEntry* dGripEntries = nullptr;
+  float4* dGripGoal = nullptr;
+  GripSlot hostGrip[GRIPS] = {};
+  float gripStiffness[GRIPS] = {};
+  std::vector<int8_t> gripOwner;
+  bool gripsOn() const {
+    for (int g = 0; g < GRIPS; ++g)
+      if (hostGrip[g].goal.w > 0.f) return true;
+    return false;
+  }
+  // graphs: substep graphs keyed by Newton iteration count and whether grips are held; the
+  // standalone PCG graph
   std::map<int, cudaGraphExec_t> substepExec;
   cudaGraphExec_t pcgExec = nullptr;
   bool useGraphs = true;
@@ -158,6 +185,17 @@ struct btd_solver {
     return a;
   }
   Reduce reduce() const { return {dPartials, dTicket}; }
+  GripArgs gripArgs() const {
+    GripArgs a;
+    a.slots = dGripSlots;
+    a.entries = dGripEntries;
+    a.goal = dGripGoal;
+    a.x = x;
+    a.dx = dx;
+    a.ext = ext;
+    a.adds = params.self_contact ? 1 : 0;
+    return a;
+  }
   PcgArgs pcgArgs(cudaGraphConditionalHandle h, int useCond) const {
     PcgArgs a;
     a.F = levels[0].dev();
@@ -193,9 +231,17 @@ struct btd_solver {
 
   // ---------------------------------------------------------------- stage encoders (stream s)
 
-  void encPredict(cudaStream_t s) {
+  // encodePredict + preSubstep (solver.ts:742): predictor, then each held grip's lead from the
+  // committed positions, then the start of the projected iterate.
+  void encPredict(cudaStream_t s, bool grips) {
     k_predict<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs());
+    if (grips) k_grip_lead<<<GRIPS, 256, 0, s>>>(gripArgs());
     k_project_start<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs());
+  }
+
+  // preAssemble (solver.ts:690): grip terms at the current iterate into ext.
+  void encGripTerms(cudaStream_t s, bool grips) {
+    if (grips) k_grip_terms<<<GRIPS * GRIP_ENTRIES / 128, 128, 0, s>>>(gripArgs());
   }
 
   void encHierarchy(cudaStream_t s) {
@@ -208,12 +254,24 @@ struct btd_solver {
         k_prolong_weights<CoarseRows, false><<<blocksFor(F.N, 128), 128, 0, s>>>(F, segs);
         k_rap<CoarseRows><<<blocksFor(Cl.N, RAP_THREADS), RAP_THREADS, 0, s>>>(F, Cl);
       }
+      encFactor(s, (int)k + 1);
     }
   }
 
   void encAssemble(cudaStream_t s, bool coarse) {
     k_assemble<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs(), levels[0].op, levels[0].B);
+    encFactor(s, 0);
     if (coarse) encHierarchy(s);
+  }
+
+  // Line factors of level k, every line in one launch (after its operator changed).
+  void encFactor(cudaStream_t s, int k) {
+    Level& L = levels[k];
+    const int count = (int)L.lines.size();
+    if (L.fine)
+      k_line_factor<FineRows><<<count, SM_THREADS, factorSmemBytes<FineRows>(L.maxLine), s>>>(L.dev(), L.dLines, L.dFacBase, L.fac);
+    else
+      k_line_factor<CoarseRows><<<count, SM_THREADS, factorSmemBytes<CoarseRows>(L.maxLine), s>>>(L.dev(), L.dLines, L.dFacBase, L.fac);
   }
 
   void encSmooth(cudaStream_t s, int k, bool reverse) {
@@ -224,9 +282,9 @@ struct btd_solver {
       int count = L.colourStart[c + 1] - L.colourStart[c];
       if (count == 0) continue;
       if (L.fine)
-        k_smooth<FineRows><<<count, SM_THREADS, smem, s>>>(L.dev(), L.dLines, L.colourStart[c]);
+        k_smooth<FineRows><<<count, SM_THREADS, smem, s>>>(L.dev(), L.dLines, L.dFacBase, L.fac, L.colourStart[c]);
       else
-        k_smooth<CoarseRows><<<count, SM_THREADS, smem, s>>>(L.dev(), L.dLines, L.colourStart[c]);
+        k_smooth<CoarseRows><<<count, SM_THREADS, smem, s>>>(L.dev(), L.dLines, L.dFacBase, L.fac, L.colourStart[c]);
     }
   }
 
@@ -311,9 +369,11 @@ struct btd_solver {
 
   void runSubstepEager(int newtonIterations) {
     cudaStream_t s = stream;
+    const bool grips = gripsOn();
     CK(cudaMemsetAsync(dCounters + CNT_UPDATE, 0, sizeof(uint32_t) * MAX_NEWTON, s));
-    encPredict(s);
+    encPredict(s, grips);
     for (int it = 0; it < newtonIterations; ++it) {
+      encGripTerms(s, grips);
       encAssemble(s, it == 0 || !params.lag_coarse);
       runPCGEager(s);
       encLineSearch(s);
@@ -340,7 +400,8 @@ struct btd_solver {
   }
 
   // encodeNewtonIteration (solver.ts:687-696).
-  void encNewton(cudaStream_t s, int it) {
+  void encNewton(cudaStream_t s, int it, bool grips) {
+    encGripTerms(s, grips);
     encAssemble(s, it == 0 || !params.lag_coarse);
     encPCG(s);
     encLineSearch(s);
@@ -368,10 +429,10 @@ struct btd_solver {
   }
   void encDamageGated(cudaStream_t s);
 
-  void encSubstep(cudaStream_t s, int newtonIterations) {
+  void encSubstep(cudaStream_t s, int newtonIterations, bool grips) {
     CK(cudaMemsetAsync(dCounters + CNT_UPDATE, 0, sizeof(uint32_t) * MAX_NEWTON, s));
-    encPredict(s);
-    for (int it = 0; it < newtonIterations; ++it) encNewton(s, it);
+    encPredict(s, grips);
+    for (int it = 0; it < newtonIterations; ++it) encNewton(s, it, grips);
     encFinalize(s);
   }
 
@@ -394,10 +455,12 @@ struct btd_solver {
   }
 
   cudaGraphExec_t substepGraph(int iters) {
-    auto it = substepExec.find(iters);
+    const bool grips = gripsOn();
+    const int key = 2 * iters + (grips ? 1 : 0);
+    auto it = substepExec.find(key);
     if (it != substepExec.end()) return it->second;
-    cudaGraphExec_t ex = capture([&](cudaStream_t s) { encSubstep(s, iters); });
-    substepExec[iters] = ex;
+    cudaGraphExec_t ex = capture([&](cudaStream_t s) { encSubstep(s, iters, grips); });
+    substepExec[key] = ex;
     return ex;
   }
 
@@ -563,6 +626,10 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
     s->dx = s->alloc<float4>(N);
     s->pred = s->alloc<float4>(N);
     s->ext = s->alloc<float4>(3 * (size_t)N);
+    s->dGripSlots = s->alloc<GripSlot>(GRIPS);
+    s->dGripEntries = s->alloc<GripEntry>((size_t)GRIPS * GRIP_ENTRIES);
+    s->dGripGoal = s->alloc<float4>(3 * GRIPS);
+    s->gripOwner.assign(N, -1);
     s->delta = s->alloc<float4>(N);
     s->p = s->alloc<float4>(N);
     s->Ap = s->alloc<float4>(N);
@@ -621,7 +688,7 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
       }
       cur = nxt;
     }
-    size_t smemFine = 0, smemCoarse = 0;
+    size_t smemFine = 0, smemCoarse = 0, fsmemFine = 0, fsmemCoarse = 0;
     for (size_t k = 0; k < s->levels.size(); ++k) {
       Level& L = s->levels[k];
       L.dLayers = s->alloc<DLevelLayer>(L.layers.size());
@@ -636,6 +703,9 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
       CK(cudaMemcpyAsync(L.dCoord, cc.data(), sizeof(uint2) * L.N, cudaMemcpyHostToDevice, st));
       L.dLines = s->alloc<int4>(L.lines.size());
       CK(cudaMemcpyAsync(L.dLines, L.lines.data(), sizeof(int4) * L.lines.size(), cudaMemcpyHostToDevice, st));
+      L.dFacBase = s->alloc<int>(L.facBase.size());
+      CK(cudaMemcpyAsync(L.dFacBase, L.facBase.data(), sizeof(int) * L.facBase.size(), cudaMemcpyHostToDevice, st));
+      L.fac = s->alloc<float4>(L.facF4);
       L.op = s->alloc<float4>((size_t)(L.fine ? FINE_PLANES : COARSE_PLANES) * L.N);
       L.fixed = s->alloc<uint32_t>(L.N);
       if (k == 0) CK(cudaMemcpyAsync(L.fixed, pinned.data(), sizeof(uint32_t) * N, cudaMemcpyHostToDevice, st));
@@ -643,18 +713,22 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
       L.B = s->alloc<float4>(L.N);
       L.R = s->alloc<float4>(L.N);
       L.pw = s->alloc<float4>(L.N);
-      size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine) : smoothSmemBytes<CoarseRows>(L.maxLine);
-      if (smem > 227 * 1024)
+      const size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine) : smoothSmemBytes<CoarseRows>(L.maxLine);
+      const size_t fsmem = L.fine ? factorSmemBytes<FineRows>(L.maxLine) : factorSmemBytes<CoarseRows>(L.maxLine);
+      if (L.maxLine > SM_MAX_LINE || smem > 227 * 1024 || fsmem > 227 * 1024)
         throw std::invalid_argument("yarn lines of " + std::to_string(L.maxLine) + " nodes exceed the smoother's shared memory");
       if (L.fine)
-        smemFine = std::max(smemFine, smem);
+        smemFine = std::max(smemFine, smem), fsmemFine = std::max(fsmemFine, fsmem);
       else
-        smemCoarse = std::max(smemCoarse, smem);
+        smemCoarse = std::max(smemCoarse, smem), fsmemCoarse = std::max(fsmemCoarse, fsmem);
     }
 
     // the smoother's dynamic shared memory: the largest line of each row layout
     if (smemFine) CK(cudaFuncSetAttribute(k_smooth<FineRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemFine));
     if (smemCoarse) CK(cudaFuncSetAttribute(k_smooth<CoarseRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemCoarse));
+    if (fsmemFine) CK(cudaFuncSetAttribute(k_line_factor<FineRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmemFine));
+    if (fsmemCoarse)
+      CK(cudaFuncSetAttribute(k_line_factor<CoarseRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmemCoarse));
 
     // ---- parameters
     SimParams& P = s->hostP;
@@ -898,7 +972,7 @@ int btd_clear_counters(btd_solver* s) {
 int btd_stage_predict(btd_solver* s) {
   GUARD({
     checkSolver(s);
-    s->encPredict(s->stream);
+    s->encPredict(s->stream, s->gripsOn());
     CK(cudaGetLastError());
     s->sync();
   });
@@ -918,6 +992,16 @@ int btd_stage_vcycle(btd_solver* s) {
     checkSolver(s);
     CK(cudaMemsetAsync(s->levels[0].X, 0, sizeof(float4) * s->N, s->stream));
     s->encVCycle(s->stream, 0);
+    CK(cudaGetLastError());
+    s->sync();
+  });
+}
+
+int btd_stage_smooth(btd_solver* s, int32_t level, int32_t reverse) {
+  GUARD({
+    checkSolver(s);
+    if (level < 0 || level >= (int)s->levels.size()) throw std::invalid_argument("level out of range");
+    s->encSmooth(s->stream, level, reverse != 0);
     CK(cudaGetLastError());
     s->sync();
   });
@@ -958,7 +1042,7 @@ int btd_stage_apply(btd_solver* s, int32_t it) {
 int btd_stage_newton(btd_solver* s, int32_t it) {
   GUARD({
     checkSolver(s);
-    cudaGraphExec_t ex = s->capture([&](cudaStream_t q) { s->encNewton(q, it); });
+    cudaGraphExec_t ex = s->capture([&](cudaStream_t q) { s->encNewton(q, it, s->gripsOn()); });
     cudaError_t e = cudaGraphLaunch(ex, s->stream);
     cudaError_t e2 = cudaStreamSynchronize(s->stream);
     cudaGraphExecDestroy(ex);
@@ -982,6 +1066,137 @@ int btd_stage_damage(btd_solver* s) {
     s->encDamage(s->stream);
     CK(cudaGetLastError());
     s->sync();
+  });
+}
+
+// ---------------------------------------------------------------- grips (interaction.ts:223-318)
+
+static_assert(GRIPS == BTD_GRIPS && GRIP_ENTRIES == BTD_GRIP_ENTRIES, "grip limits differ from btd.h");
+static_assert(sizeof(GripEntry) == 32 && sizeof(GripSlot) == 64, "grip layout");
+
+static void checkSlot(btd_solver* s, int32_t slot) {
+  checkSolver(s);
+  if (slot < 0 || slot >= GRIPS) throw std::invalid_argument("grip slot " + std::to_string(slot) + " outside [0, " + std::to_string(GRIPS) + ")");
+}
+
+static void pushGrip(btd_solver* s, int32_t slot) {
+  CK(cudaMemcpyAsync(s->dGripSlots + slot, &s->hostGrip[slot], sizeof(GripSlot), cudaMemcpyHostToDevice, s->stream));
+}
+
+// release (interaction.ts:302-313): the slot's count drops to zero; without contact the grips own
+// ext, which is cleared (the remaining grips rewrite their entries every iteration).
+static void releaseGrip(btd_solver* s, int32_t slot) {
+  if (s->hostGrip[slot].goal.w <= 0.f) return;
+  for (int n = 0; n < s->N; ++n)
+    if (s->gripOwner[n] == slot) s->gripOwner[n] = -1;
+  s->hostGrip[slot].goal.w = 0.f;
+  pushGrip(s, slot);
+  if (!s->params.self_contact) CK(cudaMemsetAsync(s->ext, 0, sizeof(float4) * 3 * (size_t)s->N, s->stream));
+}
+
+int btd_set_grip(btd_solver* s, int32_t slot, const int32_t* nodes, const float* weights, const float* sides, int32_t count,
+                 int32_t picked, const float* anchor, float stiffness, float max_lead, float pad_pitch, float slip) {
+  GUARD({
+    checkSlot(s, slot);
+    if (!nodes || !weights || !anchor) throw std::invalid_argument("null grip nodes, weights or anchor");
+    if (count < 1 || count > GRIP_ENTRIES)
+      throw std::invalid_argument("grip entry count " + std::to_string(count) + " outside [1, " + std::to_string(GRIP_ENTRIES) + "]");
+    if (picked < 0 || picked >= s->N) throw std::invalid_argument("picked node outside the lattice");
+    if (!(std::isfinite(stiffness) && stiffness >= 0.f)) throw std::invalid_argument("grip stiffness must be finite and >= 0");
+    if (!(max_lead > 0.f)) throw std::invalid_argument("grip max_lead must be > 0");
+    if (!(std::isfinite(pad_pitch) && pad_pitch >= 0.f) || !(std::isfinite(slip) && slip >= 0.f))
+      throw std::invalid_argument("grip pad_pitch and slip must be finite and >= 0");
+    for (int q = 0; q < 3; ++q)
+      if (!std::isfinite(anchor[q])) throw std::invalid_argument("grip anchor must be finite");
+    releaseGrip(s, slot);
+    // a node belongs to one patch at most, so every ext entry has one writer (interact.wgsl:4-6)
+    std::vector<GripEntry> entries(count);
+    std::vector<int> sorted(nodes, nodes + count);
+    std::sort(sorted.begin(), sorted.end());
+    if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end()) throw std::invalid_argument("a node appears twice in one grip patch");
+    for (int k = 0; k < count; ++k) {
+      const int n = nodes[k];
+      const float sd = sides ? sides[k] : 0.f;
+      if (n < 0 || n >= s->N) throw std::invalid_argument("grip node " + std::to_string(n) + " outside the lattice");
+      if (s->gripOwner[n] >= 0) throw std::invalid_argument("node " + std::to_string(n) + " is held by grip " + std::to_string(s->gripOwner[n]));
+      if (!(std::isfinite(weights[k]) && weights[k] >= 0.f)) throw std::invalid_argument("grip weights must be finite and >= 0");
+      if (sd != 0.f && sd != 1.f && sd != -1.f) throw std::invalid_argument("grip sides must be -1, 0 or +1");
+      entries[k] = GripEntry{(uint32_t)n, weights[k], sd, 0.f, make_float4(0, 0, 0, 0)};
+    }
+    for (int k = 0; k < count; ++k) s->gripOwner[nodes[k]] = (int8_t)slot;
+    GripSlot& S = s->hostGrip[slot];
+    uint32_t pk = (uint32_t)picked;
+    float pkBits;
+    std::memcpy(&pkBits, &pk, sizeof pkBits);
+    S.goal = make_float4(anchor[0], anchor[1], anchor[2], (float)count);
+    S.params = make_float4(stiffness, max_lead, pkBits, 1.f);
+    S.anchor = make_float4(anchor[0], anchor[1], anchor[2], pad_pitch);
+    S.hold = make_float4(slip, 0.f, 0.f, 0.f);
+    s->gripStiffness[slot] = stiffness;
+    CK(cudaMemcpyAsync(s->dGripEntries + (size_t)slot * GRIP_ENTRIES, entries.data(), sizeof(GripEntry) * count,
+                       cudaMemcpyHostToDevice, s->stream));
+    pushGrip(s, slot);
+    k_grip_init<<<blocksFor(count, 64), 64, 0, s->stream>>>(s->gripArgs(), slot);
+    CK(cudaGetLastError());
+    s->sync();
+  });
+}
+
+int btd_set_grip_target(btd_solver* s, int32_t slot, const float* target) {
+  GUARD({
+    checkSlot(s, slot);
+    if (!target) throw std::invalid_argument("null grip target");
+    GripSlot& S = s->hostGrip[slot];
+    if (S.goal.w <= 0.f) return BTD_OK;
+    S.goal = make_float4(target[0], target[1], target[2], S.goal.w);
+    pushGrip(s, slot);
+  });
+}
+
+int btd_set_grip_pinch(btd_solver* s, int32_t slot, float scale) {
+  GUARD({
+    checkSlot(s, slot);
+    if (s->hostGrip[slot].goal.w <= 0.f) return BTD_OK;
+    s->hostGrip[slot].params.w = scale;
+    pushGrip(s, slot);
+  });
+}
+
+int btd_set_grip_hold(btd_solver* s, int32_t slot, float fraction) {
+  GUARD({
+    checkSlot(s, slot);
+    if (s->hostGrip[slot].goal.w <= 0.f) return BTD_OK;
+    s->hostGrip[slot].params.x = s->gripStiffness[slot] * fraction;
+    pushGrip(s, slot);
+  });
+}
+
+int btd_release_grip(btd_solver* s, int32_t slot) {
+  GUARD({
+    checkSlot(s, slot);
+    releaseGrip(s, slot);
+    s->sync();
+  });
+}
+
+int btd_read_grip(btd_solver* s, int32_t slot, int32_t* nodes, float* weights, int32_t capacity, float* handle12,
+                  int32_t* count) {
+  GUARD({
+    checkSlot(s, slot);
+    const int n = (int)s->hostGrip[slot].goal.w;
+    if (count) *count = n;
+    std::vector<GripEntry> e(std::max(n, 1));
+    float4 goal[3];
+    if (n > 0)
+      CK(cudaMemcpyAsync(e.data(), s->dGripEntries + (size_t)slot * GRIP_ENTRIES, sizeof(GripEntry) * n, cudaMemcpyDeviceToHost,
+                         s->stream));
+    CK(cudaMemcpyAsync(goal, s->dGripGoal + 3 * slot, sizeof goal, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+    for (int k = 0; k < std::min(n, (int)capacity); ++k) {
+      if (nodes) nodes[k] = (int32_t)e[k].node;
+      if (weights) weights[k] = e[k].w;
+    }
+    if (handle12) std::memcpy(handle12, goal, sizeof goal);
   });
 }
 
@@ -1049,10 +1264,13 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
     for (int k = 0; k + 1 < L; ++k) V += 2 * colours(k) + 3;
     // per Newton iteration: assembly, PCG prologue (init + V-cycle + 4), line search, apply; the
     // hierarchy (weights + RAP per coarse level) on the first iteration; V-cycle + 4 per extra PCG pass
-    const int64_t perNewton = 1 + (1 + V + 4) + 1 + 1;
-    const int64_t hierarchy = 2 * (L - 1);
+    // held grips add their lead once per substep and their terms once per Newton iteration; the
+    // assembly and every Galerkin product are followed by their level's line factorisation
+    const int64_t grips = s->gripsOn() ? 1 : 0;
+    const int64_t perNewton = 2 + (1 + V + 4) + 1 + 1 + grips;
+    const int64_t hierarchy = 3 * (L - 1);
     const int64_t hierPerSubstep = s->params.lag_coarse ? hierarchy : hierarchy * (newton / std::max(1, substeps));
-    const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4;
+    const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips;
     *out = (int64_t)substeps * (perSubstep + hierPerSubstep) + (int64_t)newton * perNewton + (int64_t)(pcg - newton) * (V + 4);
   });
 }

@@ -69,9 +69,10 @@ class GpuSolver:
 
     # ---- state I/O
     def set_state(self, position, velocity=None):
-        """setState (solver.ts:833-837): positions (N, 3) or (N, 4); velocities or zero."""
+        """setState (solver.ts:833-837): positions (N, 3) or (N, 4) (w >= 0.5 retires a node); velocities or zero."""
         pos = np.zeros((self.N, 4), np.float32)
-        pos[:, :3] = np.asarray(position, np.float64).reshape(self.N, -1)[:, :3]
+        src = np.asarray(position, np.float64).reshape(self.N, -1)
+        pos[:, :src.shape[1]] = src[:, :4]
         vel = None
         if velocity is not None:
             vel = np.zeros((self.N, 4), np.float32)
@@ -181,11 +182,56 @@ class GpuSolver:
     def encode_newton_iteration(self, iteration=0):
         check("btd_stage_newton", self._h, iteration)
 
+    def encode_smooth(self, level=0, reverse=False):
+        """encodeSmooth (solver.ts:601-622): one line sweep of `level`, X <- S(X, B) in place."""
+        check("btd_stage_smooth", self._h, level, int(reverse))
+
     def encode_finalize(self):
         check("btd_stage_finalize", self._h)
 
     def encode_damage(self):
         check("btd_stage_damage", self._h)
+
+    # ---- grips (Interaction, src/simulation/gpu/interaction.ts:223-318)
+    GRIPS = 4
+    GRIP_ENTRIES = 512
+
+    def attach_patch(self, slot, picked, nodes, weights, anchor, stiffness, max_lead, sides=None, pad_pitch=0.0, slip=0.0):
+        """attachPatch (interaction.ts:223-261): grip `slot` holds `nodes` with `weights` (GripPatch
+        fields); offsets and the handle's origin are taken from node `picked` on the device."""
+        nodes = np.ascontiguousarray(nodes, np.int32)
+        w = _f(weights, nodes.size)
+        sd = None if sides is None else _f(sides, nodes.size)
+        a = _f(anchor, 3)
+        check("btd_set_grip", self._h, slot, nodes.ctypes.data_as(C.c_void_p), w.ctypes.data_as(C.c_void_p),
+              None if sd is None else sd.ctypes.data_as(C.c_void_p), nodes.size, int(picked),
+              a.ctypes.data_as(C.c_void_p), stiffness, max_lead, pad_pitch, slip)
+
+    def set_target(self, target, slot=0):
+        """setTarget (interaction.ts:276-281): requested handle in the frame of the attach anchor."""
+        t = _f(target, 3)
+        check("btd_set_grip_target", self._h, slot, t.ctypes.data_as(C.c_void_p))
+
+    def set_pinch(self, scale, slot=0):
+        check("btd_set_grip_pinch", self._h, slot, scale)
+
+    def set_hold(self, fraction, slot=0):
+        check("btd_set_grip_hold", self._h, slot, fraction)
+
+    def release(self, slot=0):
+        check("btd_release_grip", self._h, slot)
+
+    def read_grip(self, slot=0):
+        """(nodes, current weights, handle (3,), origin (3,), closing axis (3,)) of grip `slot`."""
+        count = C.c_int32()
+        nodes = np.zeros(self.GRIP_ENTRIES, np.int32)
+        w = np.zeros(self.GRIP_ENTRIES, np.float32)
+        goal = np.zeros(12, np.float32)
+        check("btd_read_grip", self._h, slot, nodes.ctypes.data_as(C.c_void_p), w.ctypes.data_as(C.c_void_p),
+              self.GRIP_ENTRIES, goal.ctypes.data_as(C.c_void_p), C.byref(count))
+        n = count.value
+        g = goal.reshape(3, 4)[:, :3].astype(np.float64)
+        return nodes[:n].copy(), w[:n].copy(), g[0], g[1], g[2]
 
     STAGES = {"matvec": 0, "smooth": 1, "assemble": 2, "vcycle": 3, "hierarchy": 4, "substep": 5}
 

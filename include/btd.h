@@ -207,6 +207,9 @@ int btd_clear_counters(btd_solver* s);
 int btd_stage_predict(btd_solver* s);                  /* encodePredict */
 int btd_stage_assemble(btd_solver* s, int32_t coarse); /* encodeAssemble(pass, coarse) */
 int btd_stage_vcycle(btd_solver* s);                   /* encodeVCycle(pass, 0): X0 = V(B0), X0 zeroed first */
+/* encodeSmooth (solver.ts:601-622): one yarn-line sweep of level `level` in place, X <- S(X, B);
+ * reverse runs the colours backwards (the post-smoother). */
+int btd_stage_smooth(btd_solver* s, int32_t level, int32_t reverse);
 int btd_stage_pcg(btd_solver* s);                      /* encodePCG: delta = PCG(B0) */
 /* encodeLineSearch: energy changes e[4] and magnitude sums m[4] along delta, alpha chosen on device. */
 int btd_stage_linesearch(btd_solver* s, double* e4, double* m4);
@@ -244,6 +247,37 @@ int btd_device_buffer(btd_solver* s, int32_t which, int32_t level, void** ptr, s
  * x and y 4 floats per node on the host. Uses the solver's own reduction scratch. */
 int btd_stage_matvec(btd_solver* s, const float* x4, float* y4, double* xy);
 int btd_write_vector(btd_solver* s, int32_t which, int32_t level, const float* in4);
+
+/* ---- Grips (Interaction, src/simulation/gpu/interaction.ts:223-318; interact.wgsl:96-197).
+ * Up to BTD_GRIPS grips, each a patch of at most BTD_GRIP_ENTRIES material nodes pulled by springs of
+ * stiffness `stiffness` x weight toward a handle. No node is in two patches. Held grips add one
+ * launch per substep (the lead) and one per Newton iteration (the terms); no held grip, no launch.
+ *
+ * btd_set_grip replaces attachPatch(slot, picked, patch, anchor, maxLead) (interaction.ts:223-261):
+ * `nodes`/`weights`/`sides` are GripPatch.nodes/weights/sides (sides may be null: a radial patch),
+ * `pad_pitch` and `slip` are GripPatch.padPitch and .slip (0: the hold does not slip), `anchor` is
+ * where the caller takes the picked material to be. Entry offsets and the handle's origin are taken
+ * on the device from node `picked`'s current position, so a target equal to the anchor moves nothing.
+ * Errors (BTD_E_INVALID): slot, count or node out of range, a node twice or held by another grip,
+ * negative or non-finite weight/stiffness, max_lead <= 0, a side other than -1/0/+1. */
+#define BTD_GRIPS 4
+#define BTD_GRIP_ENTRIES 512
+int btd_set_grip(btd_solver* s, int32_t slot, const int32_t* nodes, const float* weights, const float* sides, int32_t count,
+                 int32_t picked, const float* anchor3, float stiffness, float max_lead, float pad_pitch, float slip);
+/* setTarget (interaction.ts:276-281): requested handle in the frame of the attach anchor. */
+int btd_set_grip_target(btd_solver* s, int32_t slot, const float* target3);
+/* setPinch (interaction.ts:263-267): spread of the patch relative to grab time (1: as grabbed). */
+int btd_set_grip_pinch(btd_solver* s, int32_t slot, float scale);
+/* setHold (interaction.ts:269-274): stiffness = attach stiffness x fraction. */
+int btd_set_grip_hold(btd_solver* s, int32_t slot, float fraction);
+/* release (interaction.ts:302-313); without self-contact it also clears ext. Target, pinch and hold
+ * calls on a slot that holds nothing do nothing and return BTD_OK, like the reference's. */
+int btd_release_grip(btd_solver* s, int32_t slot);
+/* Readback for tests (the reference's tests read the grip buffer, tests/gpu/interaction.ts:318-324):
+ * the entry count, up to `capacity` entries' nodes and current weights (0 once slipped out), and
+ * 12 floats: the effective handle, the origin and the closing axis of the last lead, xyz + pad. */
+int btd_read_grip(btd_solver* s, int32_t slot, int32_t* nodes, float* weights, int32_t capacity, float* handle12,
+                  int32_t* count);
 
 /* Per-stage timing (the reference's tools/gpu/scripts/profile.ts: timestamp queries per pass):
  * launches stage `which` `reps` times on the solver's stream on the current system and returns the

@@ -200,6 +200,9 @@ class Oracle:
     def finalize(self):
         _call("ora_finalize", C.c_void_p(self._h))
 
+    def update_damage(self):
+        _call("ora_update_damage", C.c_void_p(self._h))
+
     def substep(self):
         _call("ora_substep", C.c_void_p(self._h))
 

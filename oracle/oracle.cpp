@@ -1970,6 +1970,10 @@ int ora_finalize(ora_solver* o) {
   o->s.finalize();
   return 0;
 }
+int ora_update_damage(ora_solver* o) {
+  o->s.updateDamage();
+  return 0;
+}
 int ora_substep(ora_solver* o) {
   try {
     o->s.predict();

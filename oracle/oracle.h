@@ -71,6 +71,8 @@ int ora_predict(ora_solver* s);
 int ora_newton_step(ora_solver* s, double* max_update, int32_t* pcg_iterations, double* rel_residual,
                     double* alpha);
 int ora_finalize(ora_solver* s);
+/* updateDamage (solver.ts(ref):659-666): field update, pull-out and span coupling at the current x. */
+int ora_update_damage(ora_solver* s);
 int ora_substep(ora_solver* s);
 
 /* Energies (solver.ts(ref):387-595). */

@@ -38,3 +38,21 @@ def copy_state(oracle, gpu):
     gpu.set_segments(**seg)
     gpu.set_field(oracle.field())
     return xf, vf
+
+
+def kink_rows(oracle):
+    """kinkRows (correctness.ts:53-68): rows touched by a span within rounding of the axial kink."""
+    x, _, dx, _ = oracle.state()
+    seg = oracle.segments()
+    sc = oracle.scene
+    nx = sc.nx
+    rows = set()
+    for s in range(2 * sc.N):
+        if (seg["seg_flags"][s] & 3) != 1:
+            continue
+        a = s >> 1
+        b = a + (1 if s & 1 == 0 else nx)
+        l = np.linalg.norm((x[b] + dx[b]) - (x[a] + dx[a]))
+        if abs(l / seg["rest_length"][s] - 1) < 1e-6:
+            rows.update((a, b))
+    return rows
