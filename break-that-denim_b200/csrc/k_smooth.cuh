@@ -9,24 +9,31 @@
 //                  plus the Frobenius majorisation of the +-2 along-line couplings, and the +1 block),
 //                  then the partition method - the line cut into P chunks, each chunk's interior
 //                  eliminated in terms of the chunk's end unknowns - and odd-even cyclic reduction of
-//                  the 2P end equations. It stores every pivot inverse and multiplier a solve needs.
+//                  the 2P end equations. It stores every pivot inverse and multiplier a solve needs,
+//                  and a line-contiguous copy of each row's right-hand-side couplings.
 //   k_smooth       every sweep, one CTA per line of one colour: the lagged right-hand side (b minus the
 //                  off-line and +-2 couplings at the current iterate, plus the majorisation term), then
 //                  the same elimination applied to the right-hand side only - a short chain of 3x3
 //                  matrix-vector products - and the write-back.
 //
-// Both kernels stage with cp.async: a thread's row planes and stencil unknowns land in shared-memory
-// columns (element p of thread t at p * SM_THREADS + t, so a warp's accesses fall in distinct banks),
-// all copies in flight at once. Lines of one colour are three apart and never read each other's
+// A sweep stages with cp.async, all copies of a tile in flight at once: the line's factors, its rows'
+// coupling copies (contiguous along the line whatever the family, so every 32-byte sector fetched is
+// used) and five columns of unknowns - the line itself and two lines either side - from which every
+// stencil neighbour is read. Lines of one colour are three apart and never read each other's
 // unknowns (Jacobi within a colour). Every pivot is regularised by pivotInverse. The lower block of
 // row k is the +1 block of row k - 1 (symmetric), as solvePenta takes it.
 //
-// Factor layout per line (float4 units, from the line's base): node planes p = 0..14 of node k at
-// p * len + k - planes 0-2 the pivot inverse Minv (padded 3x3; .y of plane 2 holds the majorisation
-// coefficient), 3-5 Minv A (A the lower block), 6-8 G = Minv C, 9-11 V, 12-14 W (interior k:
-// x_k = v_k + V_k x_s + W_k x_e); at a chunk's ends planes 0-2 hold the coupling into the chunk. Then
-// per cyclic-reduction elimination (level by level) the multipliers al, ga (6 float4), then per
-// reduced row Dinv, Dinv L, Dinv U (9 float4).
+// Factor region of a line (float4 units, from the line's base):
+//   node planes p = 0..14, node k at p * NP + (its padded position, see chunkSlot): 0-2 the pivot
+//     inverse Minv (padded 3x3; .y and .z of plane 2 hold the majorisation coefficient and whether
+//     the row is fixed), 3-5 Minv A (A the lower block), 6-8 G = Minv C, 9-11 V, 12-14 W (interior k:
+//     x_k = v_k + V_k x_s + W_k x_e); at a chunk's ends planes 0-2 hold the coupling into the chunk;
+//   per cyclic-reduction elimination (level by level) the multipliers al, ga (6 float4), then per
+//     reduced row Dinv, Dinv L, Dinv U (9 float4);
+//   coupling planes p = 0..RC-1 of node k at p * len + k: the row's couplings other than the +-1
+//     along-line blocks, in coupling order (6 floats a block, 1 a scalar), zero where the neighbour is
+//     outside the layer or the row is fixed, then the rhs scale (0 on a fixed row, else 1) and the
+//     majorisation coefficient.
 #pragma once
 
 #include "common.cuh"
@@ -45,32 +52,52 @@ template <class Rows>
 struct SlotOf;
 template <>
 struct SlotOf<FineRows> {
-  static constexpr int PLANES = FINE_PLANES, NC = 12;
+  // 6 off-line blocks and 4 scalars (40 floats), rhs scale, majorisation
+  static constexpr int PLANES = FINE_PLANES, NC = 12, COEF_FLOATS = 40, RC = 11;
 };
 template <>
 struct SlotOf<CoarseRows> {
-  static constexpr int PLANES = COARSE_PLANES, NC = 24;
+  // 22 blocks (132 floats), rhs scale, majorisation
+  static constexpr int PLANES = COARSE_PLANES, NC = 24, COEF_FLOATS = 132, RC = 34;
 };
 
 __host__ __device__ constexpr int linePartitions(int len) {
   return len / 2 < 1 ? 1 : (len / 2 < SM_PMAX ? len / 2 : SM_PMAX);
 }
-// float4 count of one line's factor region
+// Per-node arrays of the solve keep each chunk in a slot of an odd number S >= its size of float4,
+// node k of chunk t at t S + (k - start of t): the chunk threads, one per chunk, then step through
+// distinct shared-memory banks. A line's node arrays hold P S entries.
+__host__ __device__ constexpr int chunkSlot(int len) { return (len / linePartitions(len) + 1) | 1; }
+__host__ __device__ constexpr int lineNodesPadded(int len) { return linePartitions(len) * chunkSlot(len); }
+// float4 count of the factors of a line (node planes and reduced system)
+__host__ __device__ constexpr int lineSolveF4(int len) {
+  return FAC_NODE * lineNodesPadded(len) + (FAC_DOWN + FAC_BACK) * 2 * linePartitions(len);
+}
+template <class Rows>
 __host__ __device__ constexpr int lineFactorF4(int len) {
-  return FAC_NODE * len + (FAC_DOWN + FAC_BACK) * 2 * linePartitions(len);
+  return lineSolveF4(len) + SlotOf<Rows>::RC * len;
 }
 
-// Shared memory (bytes) of the two kernels for lines up to len nodes.
+// Shared memory (bytes) of a sweep over lines up to len nodes staged in tiles of T nodes: factors,
+// coupling planes of a tile, five columns of unknowns (tile plus two either side), b of a tile, r, v,
+// reduced r and x.
 template <class Rows>
-__host__ __device__ constexpr size_t smoothSmemBytes(int len) {
-  // staging columns (row planes, stencil unknowns, own unknown, rhs), factors, r, v, reduced r and x
-  return 16 * ((size_t)SM_THREADS * (SlotOf<Rows>::PLANES + SlotOf<Rows>::NC + 2) + (size_t)lineFactorF4(len) + 2 * (size_t)len +
-               4 * (size_t)SM_PMAX);
+__host__ __device__ constexpr size_t smoothSmemBytes(int len, int T) {
+  return 16 * ((size_t)lineSolveF4(len) + (size_t)SlotOf<Rows>::RC * T + 5 * ((size_t)T + 4) + (size_t)T +
+               2 * (size_t)lineNodesPadded(len) + 4 * (size_t)SM_PMAX);
+}
+// Tile of a level whose lines reach len nodes: the whole line when it fits, else 256 or 128 nodes.
+template <class Rows>
+__host__ inline int smoothTile(int len) {
+  constexpr size_t cap = 227 * 1024;
+  if (smoothSmemBytes<Rows>(len, len) <= cap) return len;
+  if (len > 256 && smoothSmemBytes<Rows>(len, 256) <= cap) return 256;
+  return 128;
 }
 template <class Rows>
 __host__ __device__ constexpr size_t factorSmemBytes(int len) {
-  // staging columns (row planes), line rows B and C, factors, reduced L, D, U
-  return 16 * ((size_t)SM_THREADS * SlotOf<Rows>::PLANES + 4 * (size_t)len + (size_t)lineFactorF4(len) + 9 * 2 * (size_t)SM_PMAX);
+  // staging columns (row planes), line rows B and C, node planes and reduced system, reduced L, D, U
+  return 16 * ((size_t)SM_THREADS * SlotOf<Rows>::PLANES + 4 * (size_t)len + (size_t)lineSolveF4(len) + 9 * 2 * (size_t)SM_PMAX);
 }
 
 __device__ __forceinline__ void cpAsync16(void* smem, const void* gmem, bool valid) {
@@ -83,15 +110,55 @@ __device__ __forceinline__ void cpAsyncWaitAll() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// Bulk copies (the TMA engine, no tensor map, no multicast) into this CTA's shared memory, completed
+// on an mbarrier: a few large requests instead of one per 16 bytes, which keeps an SM's L2 traffic
+// near its bandwidth.
+__device__ __forceinline__ unsigned smemAddr(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbarInit(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbarExpectTx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulkCopy(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(smemAddr(dst)),
+               "l"(src), "r"(bytes), "r"(smemAddr(bar))
+               : "memory");
+}
+// Generic-proxy accesses to shared memory before this point are ordered before later bulk copies.
+__device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ bool mbarTryWait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smemAddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for phase `parity` of an mbarrier (each try suspends the thread for a while). If it
+// runs out, the error flag is raised and the wait is given a second bound, so the CTA does not exit
+// with its copies in flight; either way the kernel goes on (with garbage, flagged) instead of hanging.
+constexpr int MBAR_TRIES = 1 << 20;
+constexpr uint32_t ERR_COPY_TIMEOUT = 1u;
+__device__ __forceinline__ void mbarWaitBounded(uint64_t* bar, unsigned parity, uint32_t* err) {
+  for (int i = 0; i < MBAR_TRIES; ++i)
+    if (mbarTryWait(bar, parity)) return;
+  if (err) atomicOr(err, ERR_COPY_TIMEOUT);
+  for (int i = 0; i < MBAR_TRIES; ++i)
+    if (mbarTryWait(bar, parity)) return;
+}
+
 // 3x3 blocks padded to 12 floats (three float4, strided by `s` float4).
 __device__ __forceinline__ M3 ldM(const float4* p, int s = 1) {
   const float4 a = p[0], b = p[s], c = p[2 * s];
   return {{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x}};
 }
-__device__ __forceinline__ void stM(float4* p, const M3& m, int s = 1, float extra = 0.f) {
+__device__ __forceinline__ void stM(float4* p, const M3& m, int s = 1, float extra = 0.f, float extra2 = 0.f) {
   p[0] = make_float4(m.a[0], m.a[1], m.a[2], m.a[3]);
   p[s] = make_float4(m.a[4], m.a[5], m.a[6], m.a[7]);
-  p[2 * s] = make_float4(m.a[8], extra, 0.f, 0.f);
+  p[2 * s] = make_float4(m.a[8], extra, extra2, 0.f);
 }
 __device__ __forceinline__ Sym ldS(const float4* p) {
   const float4 a = p[0], b = p[1];
@@ -110,116 +177,105 @@ __device__ __forceinline__ M3 m3Add(const M3& x, const M3& y) {
   return o;
 }
 
-// Float f of a row staged in a shared-memory column (plane f / 4, stride SM_THREADS).
-__device__ __forceinline__ float colF(const float4* col, int f) {
-  return reinterpret_cast<const float*>(col + (f >> 2) * SM_THREADS)[f & 3];
+// Float f of planes strided by `stride` float4 (plane f / 4).
+__device__ __forceinline__ float colF(const float4* col, int f, int stride = SM_THREADS) {
+  return reinterpret_cast<const float*>(col + (f >> 2) * stride)[f & 3];
 }
-__device__ __forceinline__ Sym colSym(const float4* col, int f) {
-  return {colF(col, f), colF(col, f + 1), colF(col, f + 2), colF(col, f + 3), colF(col, f + 4), colF(col, f + 5)};
+__device__ __forceinline__ Sym colSym(const float4* col, int f, int stride = SM_THREADS) {
+  return {colF(col, f, stride), colF(col, f + 1, stride), colF(col, f + 2, stride),
+          colF(col, f + 3, stride), colF(col, f + 4, stride), colF(col, f + 5, stride)};
+}
+__device__ __forceinline__ void putF(float4* col, int f, int stride, float v) {
+  reinterpret_cast<float*>(col + (f >> 2) * stride)[f & 3] = v;
 }
 
-// Coupling q of a row: its float offset in the row, its lattice offset, and its role in a line of
-// family fam: 1 the +1 along-line block (into the line matrix), -1 the -1 block (the previous row's
-// +1 block, by symmetry), 2 a +-2 along-line coupling (majorised), 0 an off-line coupling.
+// Coupling q of a row: its float offset in the row, and its role in a line of family fam: 1 the +1
+// along-line block (into the line matrix), -1 the -1 block (the previous row's +1 block, by
+// symmetry), 2 a +-2 along-line coupling (majorised), 0 an off-line coupling.
 template <class Rows>
 struct Coupling;
 template <>
 struct Coupling<FineRows> {
-  __device__ static int diagF() { return 0; }
-  __device__ static bool scalar(int q) { return q >= 8; }
-  __device__ static int floatAt(int q) { return q < 8 ? 6 * q + 6 : 54 + (q - 8); }
-  __device__ static int role(int q, int fam) {
-    if (q == (fam == 0 ? 0 : 2)) return 1;
-    if (q == (fam == 0 ? 1 : 3)) return -1;
-    if (q == (fam == 0 ? 8 : 10) || q == (fam == 0 ? 9 : 11)) return 2;
-    return 0;
+  __device__ static constexpr int diagF() { return 0; }
+  __device__ static constexpr bool scalar(int q) { return q >= 8; }
+  __device__ static constexpr int width(int q) { return q >= 8 ? 1 : 6; }
+  __device__ static constexpr int floatAt(int q) { return q < 8 ? 6 * q + 6 : 54 + (q - 8); }
+  __device__ static constexpr int role(int q, int fam) {
+    return q == (fam == 0 ? 0 : 2)                                 ? 1
+           : q == (fam == 0 ? 1 : 3)                               ? -1
+           : (q == (fam == 0 ? 8 : 10) || q == (fam == 0 ? 9 : 11)) ? 2
+                                                                    : 0;
   }
 };
 template <>
 struct Coupling<CoarseRows> {
-  __device__ static int diagF() { return 72; }
-  __device__ static bool scalar(int) { return false; }
-  __device__ static int floatAt(int q) { return 6 * (q >= 12 ? q + 1 : q); }
-  __device__ static int role(int q, int fam) {
-    const int o = q >= 12 ? q + 1 : q;
-    const int di = o % 5 - 2, dj = o / 5 - 2;
-    const int along = fam == 0 ? di : dj, across = fam == 0 ? dj : di;
-    if (across != 0) return 0;
-    return along == 1 ? 1 : along == -1 ? -1 : 2;
+  __device__ static constexpr int diagF() { return 72; }
+  __device__ static constexpr bool scalar(int) { return false; }
+  __device__ static constexpr int width(int) { return 6; }
+  __device__ static constexpr int floatAt(int q) { return 6 * (q >= 12 ? q + 1 : q); }
+  __device__ static constexpr int role(int q, int fam) {
+    return (fam == 0 ? (q >= 12 ? q + 1 : q) / 5 - 2 : (q >= 12 ? q + 1 : q) % 5 - 2) != 0 ? 0
+           : (fam == 0 ? (q >= 12 ? q + 1 : q) % 5 - 2 : (q >= 12 ? q + 1 : q) / 5 - 2) == 1  ? 1
+           : (fam == 0 ? (q >= 12 ? q + 1 : q) % 5 - 2 : (q >= 12 ? q + 1 : q) / 5 - 2) == -1 ? -1
+                                                                                              : 2;
   }
 };
 
-// Line row of node (i, j) from its staged row planes: B = D + maj I, C the +1 block (zero at the
-// line's end), maj = sqrt(3) |s| per scalar or ||B||_F per block +-2 along-line coupling with an
-// in-bounds neighbour (lineRow, smooth.wgsl:49-84; smoothLines, newtonMultigrid.ts:676-720).
-template <class Rows>
-__device__ __forceinline__ void lineMatrixFromCol(const float4* col, int i, int j, const DLevelLayer& ly, int k, int len, int fam,
-                                                  Sym* Bk, Sym* Ck, float* majOut) {
-  using Cp = Coupling<Rows>;
-  float maj = 0.f;
-  *Ck = symZero();
-#pragma unroll
-  for (int q = 0; q < SlotOf<Rows>::NC; ++q) {
-    const int role = Cp::role(q, fam);
-    if (role == 1) {
-      if (k + 1 < len) *Ck = Cp::scalar(q) ? symId(colF(col, Cp::floatAt(q))) : colSym(col, Cp::floatAt(q));
-      continue;
-    }
-    if (role != 2) continue;
-    const int2 o = Rows::offset(q);
-    const int ii = i + o.x, jj = j + o.y;
-    if (ii < 0 || jj < 0 || ii >= ly.nx || jj >= ly.ny) continue;
-    maj += Cp::scalar(q) ? 1.7320508075688772f * fabsf(colF(col, Cp::floatAt(q))) : symFrob(colSym(col, Cp::floatAt(q)));
-  }
-  *Bk = colSym(col, Cp::diagF()) + symId(maj);
-  *majOut = maj;
-}
-
-// Lagged right-hand side of the same row: b - sum over off-line and +-2 couplings of A x, plus
-// maj x_n. Staged columns: row planes, then the stencil unknowns in coupling order, own, rhs.
-template <class Rows>
-__device__ __forceinline__ float3 lineRhsFromCol(const float4* col, int i, int j, const DLevelLayer& ly, int fam, float maj) {
-  using Cp = Coupling<Rows>;
-  constexpr int PL = SlotOf<Rows>::PLANES, NC = SlotOf<Rows>::NC;
-  const float3 xn = f3(col[(PL + NC) * SM_THREADS]);
-  float3 r = f3(col[(PL + NC + 1) * SM_THREADS]);
-#pragma unroll
-  for (int q = 0; q < NC; ++q) {
-    const int role = Cp::role(q, fam);
-    if (role == 1 || role == -1) continue;
-    const int2 o = Rows::offset(q);
-    const int ii = i + o.x, jj = j + o.y;
-    if (ii < 0 || jj < 0 || ii >= ly.nx || jj >= ly.ny) continue;
-    const float3 xm = f3(col[(PL + q) * SM_THREADS]);
-    if (Cp::scalar(q))
-      r -= colF(col, Cp::floatAt(q)) * xm;
-    else
-      r -= colSym(col, Cp::floatAt(q)) * xm;
-  }
-  return r + maj * xn;
-}
-
-// Chunk t of a line of len nodes cut into P chunks: [ks, ke].
+// Chunk t of a line of len nodes cut into P chunks: [ks, ke]; idx is a node's padded position.
 struct Chunks {
-  int P, base, extra;
-  __device__ Chunks(int len) : P(linePartitions(len)), base(len / linePartitions(len)), extra(len % linePartitions(len)) {}
+  int P, base, extra, S;
+  __device__ Chunks(int len)
+      : P(linePartitions(len)), base(len / linePartitions(len)), extra(len % linePartitions(len)), S(chunkSlot(len)) {}
   __device__ int start(int t) const { return t * base + min(t, extra); }
   __device__ int size(int t) const { return base + (t < extra ? 1 : 0); }
   __device__ int of(int k) const {
     const int cut = extra * (base + 1);
     return k < cut ? k / (base + 1) : extra + (k - cut) / base;
   }
+  __device__ int idx(int k) const {
+    const int t = of(k);
+    return t * S + (k - start(t));
+  }
 };
 
-// Elimination slots of cyclic reduction over Q rows: at stride s the rows q with (q + 1) % 2s == 0;
-// slot = (rows of the smaller strides) + (q + 1) / 2s - 1.
-__device__ __forceinline__ int crSlot(int Q, int stride, int q) {
-  int off = 0;
-  for (int s = 1; s < stride; s *= 2) off += Q / (2 * s);
-  return off + (q + 1) / (2 * stride) - 1;
-}
-
 // ------------------------------------------------------------------------------------------ factor
+
+// Line row of node (i, j) from its staged row planes: B = D + maj I, C the +1 block (zero at the
+// line's end), maj = sqrt(3) |s| per scalar or ||B||_F per block +-2 along-line coupling with an
+// in-bounds neighbour (lineRow, smooth.wgsl:49-84; smoothLines, newtonMultigrid.ts:676-720); and the
+// row's coupling copy written to `cp` (planes strided by cstride).
+template <class Rows>
+__device__ __forceinline__ void lineRowFromCol(const float4* col, int i, int j, const DLevelLayer& ly, int k, int len, int fam,
+                                               bool fixedNode, Sym* Bk, Sym* Ck, float* majOut, float4* cp, int cstride) {
+  using Cp = Coupling<Rows>;
+  constexpr int CF = SlotOf<Rows>::COEF_FLOATS;
+  float maj = 0.f;
+  *Ck = symZero();
+  int pos = 0;
+#pragma unroll
+  for (int q = 0; q < SlotOf<Rows>::NC; ++q) {
+    const int role = Cp::role(q, fam);
+    const int2 o = Rows::offset(q);
+    const int ii = i + o.x, jj = j + o.y;
+    const bool in = !fixedNode && ii >= 0 && jj >= 0 && ii < ly.nx && jj < ly.ny;
+    if (role == 1) {
+      if (!fixedNode && k + 1 < len) *Ck = Cp::scalar(q) ? symId(colF(col, Cp::floatAt(q))) : colSym(col, Cp::floatAt(q));
+      continue;
+    }
+    if (role == -1) continue;
+#pragma unroll
+    for (int w = 0; w < Cp::width(q); ++w) putF(cp, pos + w, cstride, in ? colF(col, Cp::floatAt(q) + w) : 0.f);
+    pos += Cp::width(q);
+    if (role == 2 && in)
+      maj += Cp::scalar(q) ? 1.7320508075688772f * fabsf(colF(col, Cp::floatAt(q))) : symFrob(colSym(col, Cp::floatAt(q)));
+  }
+  putF(cp, CF, cstride, fixedNode ? 0.f : 1.f);
+  putF(cp, CF + 1, cstride, maj);
+#pragma unroll
+  for (int w = CF + 2; w < 4 * SlotOf<Rows>::RC; ++w) putF(cp, w, cstride, 0.f);
+  *Bk = fixedNode ? symId(1.f) : colSym(col, Cp::diagF()) + symId(maj);
+  *majOut = maj;
+}
 
 template <class Rows>
 __global__ void __launch_bounds__(SM_THREADS) k_line_factor(DLevel L, const int4* __restrict__ lines, const int* __restrict__ base,
@@ -231,20 +287,21 @@ __global__ void __launch_bounds__(SM_THREADS) k_line_factor(DLevel L, const int4
   const DLevelLayer ly = L.layers[line.w >> 1];
   const int tid = threadIdx.x;
   const Chunks ch(len);
-  const int P = ch.P, Q = 2 * P;
+  const int P = ch.P, Q = 2 * P, NP = lineNodesPadded(len), S = ch.S;
   float4* cols = sm4;
   float4* sB = cols + SM_THREADS * PL;  // 2 per node
   float4* sC = sB + 2 * len;            // 2 per node
-  float4* sF = sC + 2 * len;            // the line's factor region
-  float4* qL = sF + lineFactorF4(len);  // 3 per reduced row
+  float4* sF = sC + 2 * len;            // node planes and reduced system
+  float4* qL = sF + lineSolveF4(len);   // 3 per reduced row
   float4* qD = qL + 3 * 2 * SM_PMAX;
   float4* qU = qD + 3 * 2 * SM_PMAX;
-  float4* fDown = sF + FAC_NODE * len;
+  float4* fDown = sF + FAC_NODE * NP;
   float4* fBack = fDown + FAC_DOWN * Q;
+  float4* out = fac + base[blockIdx.x];
   const int local0 = n0 - ly.offset;
   const int i0 = local0 % ly.nx, j0 = local0 / ly.nx;
 
-  // ---- line rows
+  // ---- line rows and the coupling copy
   for (int k = tid; k < len; k += SM_THREADS) {
     const int n = n0 + k * st;
     const int i = fam == 0 ? i0 + k : i0, j = fam == 0 ? j0 : j0 + k;
@@ -252,18 +309,23 @@ __global__ void __launch_bounds__(SM_THREADS) k_line_factor(DLevel L, const int4
 #pragma unroll
     for (int p = 0; p < PL; ++p) cpAsync16(col + p * SM_THREADS, L.op + (size_t)p * L.N + n, true);
     cpAsyncWaitAll();
-    Sym Bk = symId(1.f), Ck = symZero();
-    float maj = 0.f;
-    if (!L.fixed[n]) lineMatrixFromCol<Rows>(col, i, j, ly, k, len, fam, &Bk, &Ck, &maj);
+    Sym Bk, Ck;
+    float maj;
+    if (fam == 0)
+      lineRowFromCol<Rows>(col, i, j, ly, k, len, 0, L.fixed[n] != 0u, &Bk, &Ck, &maj, out + lineSolveF4(len) + k, len);
+    else
+      lineRowFromCol<Rows>(col, i, j, ly, k, len, 1, L.fixed[n] != 0u, &Bk, &Ck, &maj, out + lineSolveF4(len) + k, len);
     stS(sB + 2 * k, Bk);
     stS(sC + 2 * k, Ck);
-    sF[2 * len + k] = make_float4(0.f, maj, 0.f, 0.f);
+    sF[2 * NP + ch.idx(k)] = make_float4(0.f, maj, L.fixed[n] != 0u ? 1.f : 0.f, 0.f);
   }
   __syncthreads();
 
-  // ---- chunk interiors: Minv, Minv A, G; then V, W by the backward pass; reduced rows
+  // ---- chunk interiors: Minv, Minv A, G; then V, W by the backward pass; reduced rows. Node k of
+  // chunk t sits at t S + (k - ks) in the node planes.
   if (tid < P) {
     const int ks = ch.start(tid), mlen = ch.size(tid), ke = ks + mlen - 1;
+    float4* nd = sF + tid * S - ks;  // node k's entry of plane p: nd[p * NP + k]
     M3 Gp = m3Zero(), Hsp = m3Id(), Hep = m3Zero();
     for (int k = ks + 1; k < ke; ++k) {
       const M3 Ak = m3FromSym(ldS(sC + 2 * (k - 1)));
@@ -278,23 +340,23 @@ __global__ void __launch_bounds__(SM_THREADS) k_line_factor(DLevel L, const int4
         Cext = Ck;
       const M3 Hs = m3Neg(m3Mul(QA, Hsp));
       const M3 He = m3Sub(m3Neg(m3Mul(QA, Hep)), m3Mul(Minv, Cext));
-      const float maj = sF[2 * len + k].y;
-      stM(sF + k, Minv, len, maj);
-      stM(sF + 3 * len + k, QA, len);
-      stM(sF + 6 * len + k, G, len);
-      stM(sF + 9 * len + k, Hs, len);
-      stM(sF + 12 * len + k, He, len);
+      const float4 mf = nd[2 * NP + k];
+      stM(nd + k, Minv, NP, mf.y, mf.z);
+      stM(nd + 3 * NP + k, QA, NP);
+      stM(nd + 6 * NP + k, G, NP);
+      stM(nd + 9 * NP + k, Hs, NP);
+      stM(nd + 12 * NP + k, He, NP);
       Gp = G, Hsp = Hs, Hep = He;
     }
     M3 VS = m3Zero(), WS = m3Id(), VE = m3Id(), WE = m3Zero();
     if (mlen >= 3) {
       M3 Vn = m3Zero(), Wn = m3Zero();
       for (int k = ke - 1; k > ks; --k) {
-        const M3 G = ldM(sF + 6 * len + k, len);
-        const M3 V = m3Sub(ldM(sF + 9 * len + k, len), m3Mul(G, Vn));
-        const M3 W = m3Sub(ldM(sF + 12 * len + k, len), m3Mul(G, Wn));
-        stM(sF + 9 * len + k, V, len);
-        stM(sF + 12 * len + k, W, len);
+        const M3 G = ldM(nd + 6 * NP + k, NP);
+        const M3 V = m3Sub(ldM(nd + 9 * NP + k, NP), m3Mul(G, Vn));
+        const M3 W = m3Sub(ldM(nd + 12 * NP + k, NP), m3Mul(G, Wn));
+        stM(nd + 9 * NP + k, V, NP);
+        stM(nd + 12 * NP + k, W, NP);
         if (k == ke - 1) VE = V, WE = W;
         Vn = V, Wn = W;
       }
@@ -305,9 +367,9 @@ __global__ void __launch_bounds__(SM_THREADS) k_line_factor(DLevel L, const int4
     const M3 Ae = m3FromSym(ldS(sC + 2 * (ke - 1))), Be = m3FromSym(ldS(sB + 2 * ke));
     const M3 Ce = m3FromSym(ldS(sC + 2 * ke));
     // couplings the reduced right-hand sides need: Cs at the chunk's start, Ae at its end
-    const float majS = sF[2 * len + ks].y, majE = sF[2 * len + ke].y;
-    stM(sF + ks, Cs, len, majS);
-    if (ke != ks) stM(sF + ke, Ae, len, majE);
+    const float4 mS = nd[2 * NP + ks], mE = nd[2 * NP + ke];
+    stM(nd + ks, Cs, NP, mS.y, mS.z);
+    stM(nd + ke, Ae, NP, mE.y, mE.z);
     stM(qL + 3 * (2 * tid), As);
     stM(qD + 3 * (2 * tid), m3Add(Bs, m3Mul(Cs, VS)));
     stM(qU + 3 * (2 * tid), m3Mul(Cs, WS));
@@ -317,24 +379,25 @@ __global__ void __launch_bounds__(SM_THREADS) k_line_factor(DLevel L, const int4
   }
   __syncthreads();
 
-  // ---- odd-even cyclic reduction of the 2P reduced rows. At stride s the rows with
-  // (q + 1) % 2s == 0 eliminate their neighbours q -+ s, which no longer change.
-  int stride = 1;
-  while (2 * stride <= Q) {
-    const int q = tid;
-    if (q < Q && (q + 1) % (2 * stride) == 0) {
-      const int lo = q - stride;
+  // ---- odd-even cyclic reduction of the 2P reduced rows. At stride s = 2^lv the rows with
+  // (q + 1) % 2s == 0 eliminate their neighbours q -+ s, which no longer change; their multipliers
+  // go to slot (rows of the smaller strides) + (q + 1) / 2s - 1.
+  int lv = 0, off = 0;
+  while ((2 << lv) <= Q) {
+    const int s = 1 << lv, q = tid;
+    if (q < Q && ((q + 1) & (2 * s - 1)) == 0) {
+      const int lo = q - s;
       const M3 al = m3Mul(ldM(qL + 3 * q), pivotInverse(ldM(qD + 3 * lo)));
       M3 D = m3Sub(ldM(qD + 3 * q), m3Mul(al, ldM(qU + 3 * lo)));
       const M3 Lq = m3Neg(m3Mul(al, ldM(qL + 3 * lo)));
       M3 Uq = m3Zero(), ga = m3Zero();
-      if (q + stride < Q) {
-        const int hi = q + stride;
+      if (q + s < Q) {
+        const int hi = q + s;
         ga = m3Mul(ldM(qU + 3 * q), pivotInverse(ldM(qD + 3 * hi)));
         D = m3Sub(D, m3Mul(ga, ldM(qL + 3 * hi)));
         Uq = m3Neg(m3Mul(ga, ldM(qU + 3 * hi)));
       }
-      const int slot = crSlot(Q, stride, q);
+      const int slot = off + ((q + 1) >> (lv + 1)) - 1;
       stM(fDown + FAC_DOWN * slot, al);
       stM(fDown + FAC_DOWN * slot + 3, ga);
       stM(qD + 3 * q, D);
@@ -342,132 +405,192 @@ __global__ void __launch_bounds__(SM_THREADS) k_line_factor(DLevel L, const int4
       stM(qU + 3 * q, Uq);
     }
     __syncthreads();
-    stride *= 2;
+    off += Q >> (lv + 1);
+    ++lv;
   }
-  while (stride > 0) {
-    const int q = tid;
-    if (q < Q && (q + 1) % stride == 0 && (q + 1) % (2 * stride) != 0) {
+  for (; lv >= 0; --lv) {
+    const int s = 1 << lv, q = tid;
+    if (q < Q && ((q + 1) & (s - 1)) == 0 && ((q + 1) & s) != 0) {
       const M3 Dinv = pivotInverse(ldM(qD + 3 * q));
-      const M3 DL = q >= stride ? m3Mul(Dinv, ldM(qL + 3 * q)) : m3Zero();
-      const M3 DU = q + stride < Q ? m3Mul(Dinv, ldM(qU + 3 * q)) : m3Zero();
+      const M3 DL = q >= s ? m3Mul(Dinv, ldM(qL + 3 * q)) : m3Zero();
+      const M3 DU = q + s < Q ? m3Mul(Dinv, ldM(qU + 3 * q)) : m3Zero();
       stM(fBack + FAC_BACK * q, Dinv);
       stM(fBack + FAC_BACK * q + 3, DL);
       stM(fBack + FAC_BACK * q + 6, DU);
     }
     __syncthreads();
-    stride /= 2;
   }
 
-  // ---- the region out, coalesced
-  float4* out = fac + base[blockIdx.x];
-  const int total = lineFactorF4(len);
+  // ---- node planes and reduced system out, coalesced
+  const int total = lineSolveF4(len);
   for (int e = tid; e < total; e += SM_THREADS) out[e] = sF[e];
 }
 
 // ------------------------------------------------------------------------------------------ sweep
 
-template <class Rows>
-__global__ void __launch_bounds__(SM_THREADS) k_smooth(DLevel L, const int4* __restrict__ lines, const int* __restrict__ base,
-                                                       const float4* __restrict__ fac, int first) {
-  constexpr int PL = SlotOf<Rows>::PLANES, NC = SlotOf<Rows>::NC, SLOT = PL + NC + 2;
+// The lines of one colour launch: either each line from the line table (scenes of several layers),
+// or, in a single layer, line b at start0 + b startStep with its factors at base0 + b baseStep.
+struct LineGeom {
+  int first;  // table index of block 0
+  int table;
+  int start0, startStep, stride, len, base0, baseStep;
+  DLevelLayer ly;
+};
+
+template <class Rows, int FAM>
+__global__ void __launch_bounds__(SM_THREADS) k_smooth(DLevel L, LineGeom g, const int4* __restrict__ lines, const int* __restrict__ base,
+                                                       const float4* __restrict__ fac, int T, uint32_t* err) {
+  __shared__ uint64_t bar;
+  using Cp = Coupling<Rows>;
+  constexpr int RC = SlotOf<Rows>::RC, CF = SlotOf<Rows>::COEF_FLOATS;
   extern __shared__ float4 sm4[];
-  const int li = first + blockIdx.x;
-  const int4 line = lines[li];
-  const int n0 = line.x, st = line.y, len = line.z, fam = line.w & 1;
-  const DLevelLayer ly = L.layers[line.w >> 1];
+  int n0, st, len, fb;
+  DLevelLayer ly;
+  if (g.table) {
+    const int4 line = lines[g.first + blockIdx.x];
+    n0 = line.x, st = line.y, len = line.z;
+    ly = L.layers[line.w >> 1];
+    fb = base[g.first + blockIdx.x];
+  } else {
+    n0 = g.start0 + blockIdx.x * g.startStep, st = g.stride, len = g.len;
+    ly = g.ly;
+    fb = g.base0 + blockIdx.x * g.baseStep;
+  }
   const int tid = threadIdx.x;
   const Chunks ch(len);
-  const int P = ch.P, Q = 2 * P;
-  const int total = lineFactorF4(len);
-  float4* cols = sm4;
-  float4* sF = cols + SM_THREADS * SLOT;
-  float4* sR = sF + total;  // r, then the reduced solution's recovery reads it
-  float4* sV = sR + len;    // h, then v
-  float4* qr = sV + len;
+  const int P = ch.P, Q = 2 * P, NP = lineNodesPadded(len), S = ch.S;
+  const int solveF4 = lineSolveF4(len);
+  const int TX = T + 4;
+  float4* sF = sm4;
+  float4* sCp = sF + solveF4;  // coupling planes of the tile, plane stride T
+  float4* sX = sCp + RC * T;   // 5 columns of TX unknowns
+  float4* sBt = sX + 5 * TX;   // b of the tile
+  float4* sR = sBt + T;        // r (padded node positions)
+  float4* sV = sR + NP;        // h, then v
+  float4* qr = sV + NP;
   float4* qx = qr + 2 * SM_PMAX;
-  const float4* fDown = sF + FAC_NODE * len;
+  const float4* fDown = sF + FAC_NODE * NP;
   const float4* fBack = fDown + FAC_DOWN * Q;
+  const float4* src = fac + fb;
+  // the line's position across its family, and the node step to the neighbouring line
   const int local0 = n0 - ly.offset;
-  const int i0 = local0 % ly.nx, j0 = local0 / ly.nx;
+  const int across0 = FAM == 0 ? local0 / ly.nx : local0 % ly.nx;
+  const int nAcross = FAM == 0 ? ly.ny : ly.nx, acrossStep = FAM == 0 ? ly.nx : 1;
 
-  // ---- stage the factors and, tile by tile, each node's row planes and stencil unknowns; build r
-  const float4* src = fac + base[li];
-  for (int e = tid; e < total; e += SM_THREADS) cpAsync16(sF + e, src + e, true);
-  for (int k = tid; k < len; k += SM_THREADS) {
-    const int n = n0 + k * st;
-    const int i = fam == 0 ? i0 + k : i0, j = fam == 0 ? j0 : j0 + k;
-    float4* col = cols + tid;
-#pragma unroll
-    for (int p = 0; p < PL; ++p) cpAsync16(col + p * SM_THREADS, L.op + (size_t)p * L.N + n, true);
-#pragma unroll
-    for (int q = 0; q < NC; ++q) {
-      const int2 o = Rows::offset(q);
-      const int ii = i + o.x, jj = j + o.y;
-      const bool ok = ii >= 0 && jj >= 0 && ii < ly.nx && jj < ly.ny;
-      cpAsync16(col + (PL + q) * SM_THREADS, L.X + (ok ? ly.offset + jj * ly.nx + ii : n), ok);
+  // ---- stage: the factors and, tile by tile, the coupling planes by bulk copies (thread 0), the
+  // unknowns and b by cp.async (strided along a v-line); then build r
+  if (tid == 0) mbarInit(&bar, 1);
+  __syncthreads();
+  unsigned phase = 0;
+  for (int k0 = 0; k0 < len; k0 += T) {
+    const int tn = min(T, len - k0);
+    if (tid == 0) {
+      fenceProxyAsync();
+      const unsigned coefBytes = 16u * RC * tn;
+      mbarExpectTx(&bar, coefBytes + (k0 == 0 ? 16u * solveF4 : 0u));
+      if (k0 == 0) bulkCopy(sF, src, 16u * solveF4, &bar);
+      if (tn == len && len == T)
+        bulkCopy(sCp, src + solveF4, coefBytes, &bar);
+      else
+        for (int p = 0; p < RC; ++p) bulkCopy(sCp + p * T, src + solveF4 + p * len + k0, 16u * tn, &bar);
     }
-    cpAsync16(col + (PL + NC) * SM_THREADS, L.X + n, true);
-    cpAsync16(col + (PL + NC + 1) * SM_THREADS, L.B + n, true);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      const int c = across0 + a - 2;
+      for (int kk = tid; kk < tn + 4; kk += SM_THREADS) {
+        const int k = k0 + kk - 2;
+        const bool ok = k >= 0 && k < len && c >= 0 && c < nAcross;
+        cpAsync16(sX + a * TX + kk, L.X + (ok ? n0 + k * st + (a - 2) * acrossStep : n0), ok);
+      }
+    }
+    for (int kk = tid; kk < tn; kk += SM_THREADS) cpAsync16(sBt + kk, L.B + n0 + (k0 + kk) * st, true);
     cpAsyncWaitAll();
-    float3 r = make_float3(0, 0, 0);
-    if (!L.fixed[n]) r = lineRhsFromCol<Rows>(col, i, j, ly, fam, sF[2 * len + k].y);
-    stV(sR + k, r);
-  }
-  cpAsyncWaitAll();
-  __syncthreads();
-
-  // ---- chunk interiors: h_k = Minv_k r_k - (Minv A)_k h_{k-1}, v_k = h_k - G_k v_{k+1}; reduced r
-  if (tid < P) {
-    const int ks = ch.start(tid), mlen = ch.size(tid), ke = ks + mlen - 1;
-    float3 h = make_float3(0, 0, 0);
-    for (int k = ks + 1; k < ke; ++k) {
-      h = m3Vec(ldM(sF + k, len), ldV(sR + k)) - m3Vec(ldM(sF + 3 * len + k, len), h);
-      stV(sV + k, h);
-    }
-    float3 v = make_float3(0, 0, 0), vS = v, vE = v;
-    for (int k = ke - 1; k > ks; --k) {
-      v = ldV(sV + k) - m3Vec(ldM(sF + 6 * len + k, len), v);
-      stV(sV + k, v);
-      if (k == ke - 1) vE = v;
-    }
-    if (mlen >= 3) vS = v;
-    stV(qr + 2 * tid, ldV(sR + ks) - m3Vec(ldM(sF + ks, len), vS));
-    stV(qr + 2 * tid + 1, ldV(sR + ke) - m3Vec(ldM(sF + ke, len), vE));
-  }
-  __syncthreads();
-
-  // ---- cyclic reduction of the reduced right-hand sides, then the reduced solution
-  int stride = 1;
-  while (2 * stride <= Q) {
-    const int q = tid;
-    if (q < Q && (q + 1) % (2 * stride) == 0) {
-      const float4* f = fDown + FAC_DOWN * crSlot(Q, stride, q);
-      float3 r = ldV(qr + q) - m3Vec(ldM(f), ldV(qr + q - stride));
-      if (q + stride < Q) r = r - m3Vec(ldM(f + 3), ldV(qr + q + stride));
-      stV(qr + q, r);
+    mbarWaitBounded(&bar, phase, err);
+    phase ^= 1u;
+    __syncthreads();
+    for (int kk = tid; kk < tn; kk += SM_THREADS) {
+      const float4* cp = sCp + kk;
+      const float4* xc = sX + kk + 2;
+      float3 r = colF(cp, CF, T) * f3(sBt[kk]);
+      int pos = 0;
+#pragma unroll
+      for (int q = 0; q < SlotOf<Rows>::NC; ++q) {
+        const int role = Cp::role(q, FAM);
+        if (role == 1 || role == -1) continue;
+        const int2 o = Rows::offset(q);
+        const int along = FAM == 0 ? o.x : o.y, across = FAM == 0 ? o.y : o.x;
+        const float3 xm = f3(xc[(across + 2) * TX + along]);
+        if (Cp::scalar(q))
+          r -= colF(cp, pos, T) * xm;
+        else
+          r -= colSym(cp, pos, T) * xm;
+        pos += Cp::width(q);
+      }
+      stV(sR + ch.idx(k0 + kk), r + colF(cp, CF + 1, T) * f3(xc[2 * TX]));
     }
     __syncthreads();
-    stride *= 2;
-  }
-  while (stride > 0) {
-    const int q = tid;
-    if (q < Q && (q + 1) % stride == 0 && (q + 1) % (2 * stride) != 0) {
-      const float4* f = fBack + FAC_BACK * q;
-      float3 x = m3Vec(ldM(f), ldV(qr + q));
-      if (q >= stride) x = x - m3Vec(ldM(f + 3), ldV(qx + q - stride));
-      if (q + stride < Q) x = x - m3Vec(ldM(f + 6), ldV(qx + q + stride));
-      stV(qx + q, x);
-    }
-    __syncthreads();
-    stride /= 2;
   }
 
-  // ---- recovery and write-back, every node in parallel
+  // ---- warp 0: chunk interiors (lane t, chunk t): h_k = Minv_k r_k - (Minv A)_k h_{k-1},
+  // v_k = h_k - G_k v_{k+1}; the reduced right-hand sides; then cyclic reduction, the rows of each
+  // level on consecutive lanes (at most Q / 2 <= 32 of them), synchronised within the warp
+  if (tid < 32) {
+    const int lane = tid;
+    if (lane < P) {
+      const int ks = ch.start(lane), mlen = ch.size(lane), ke = ks + mlen - 1;
+      const int o = lane * S - ks;  // padded position of node k: o + k
+      float3 h = make_float3(0, 0, 0);
+      for (int k = ks + 1; k < ke; ++k) {
+        h = m3Vec(ldM(sF + o + k, NP), ldV(sR + o + k)) - m3Vec(ldM(sF + 3 * NP + o + k, NP), h);
+        stV(sV + o + k, h);
+      }
+      float3 v = make_float3(0, 0, 0), vS = v, vE = v;
+      for (int k = ke - 1; k > ks; --k) {
+        v = ldV(sV + o + k) - m3Vec(ldM(sF + 6 * NP + o + k, NP), v);
+        stV(sV + o + k, v);
+        if (k == ke - 1) vE = v;
+      }
+      if (mlen >= 3) vS = v;
+      stV(qr + 2 * lane, ldV(sR + o + ks) - m3Vec(ldM(sF + o + ks, NP), vS));
+      stV(qr + 2 * lane + 1, ldV(sR + o + ke) - m3Vec(ldM(sF + o + ke, NP), vE));
+    }
+    __syncwarp();
+    // down: at stride s = 2^lv, row q = 2s (m + 1) - 1 on lane m takes its multipliers from slot
+    // (rows of the smaller strides) + m
+    int lv = 0, off = 0;
+    for (; (2 << lv) <= Q; ++lv) {
+      const int s = 1 << lv, cnt = Q >> (lv + 1);
+      if (lane < cnt) {
+        const int q = ((lane + 1) << (lv + 1)) - 1;
+        const float4* f = fDown + FAC_DOWN * (off + lane);
+        float3 r = ldV(qr + q) - m3Vec(ldM(f), ldV(qr + q - s));
+        if (q + s < Q) r = r - m3Vec(ldM(f + 3), ldV(qr + q + s));
+        stV(qr + q, r);
+      }
+      __syncwarp();
+      off += cnt;
+    }
+    // up: at stride s the rows q = s (2m + 1) - 1 on lane m
+    for (; lv >= 0; --lv) {
+      const int s = 1 << lv, q = s * (2 * lane + 1) - 1;
+      if (q < Q) {
+        const float4* f = fBack + FAC_BACK * q;
+        float3 x = m3Vec(ldM(f), ldV(qr + q));
+        if (q >= s) x = x - m3Vec(ldM(f + 3), ldV(qx + q - s));
+        if (q + s < Q) x = x - m3Vec(ldM(f + 6), ldV(qx + q + s));
+        stV(qx + q, x);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+
+  // ---- recovery and write-back, every node in parallel (fixed rows keep their unknowns)
   for (int k = tid; k < len; k += SM_THREADS) {
-    const int n = n0 + k * st;
-    if (L.fixed[n]) continue;
     const int t = ch.of(k);
     const int ks = ch.start(t), ke = ks + ch.size(t) - 1;
+    const int ix = t * S + (k - ks);
+    if (sF[2 * NP + ix].z != 0.f) continue;
     const float3 xs = ldV(qx + 2 * t), xe = ldV(qx + 2 * t + 1);
     float3 x;
     if (k == ks)
@@ -475,8 +598,8 @@ __global__ void __launch_bounds__(SM_THREADS) k_smooth(DLevel L, const int4* __r
     else if (k == ke)
       x = xe;
     else
-      x = ldV(sV + k) + m3Vec(ldM(sF + 9 * len + k, len), xs) + m3Vec(ldM(sF + 12 * len + k, len), xe);
-    L.X[n] = make_float4(x.x, x.y, x.z, 0.f);
+      x = ldV(sV + ix) + m3Vec(ldM(sF + 9 * NP + ix, NP), xs) + m3Vec(ldM(sF + 12 * NP + ix, NP), xe);
+    L.X[n0 + k * st] = make_float4(x.x, x.y, x.z, 0.f);
   }
 }
 

@@ -57,6 +57,8 @@ struct Level {
   int4* dLines = nullptr;
   // line factors (k_line_factor): each line's region starts at facBase[line]
   std::vector<int> facBase;
+  int tile = 0;          // sweep staging tile (nodes)
+  LineGeom geom[6] = {};  // launch geometry per colour
   int* dFacBase = nullptr;
   float4* fac = nullptr;
   size_t facF4 = 0;
@@ -80,7 +82,8 @@ struct Level {
 };
 
 // Line tables (lineTable, lattice.ts:330-350): v-lines coloured i mod 3, then u-lines j mod 3;
-// entry (start node, stride, length, family | layer << 1).
+// entry (start node, stride, length, family | layer << 1). Then each line's factor region, and per
+// colour the launch geometry (computed from the block index on a single layer).
 static void buildLines(Level& L) {
   std::vector<int4> byColour[6];
   for (size_t l = 0; l < L.layers.size(); ++l) {
@@ -96,13 +99,38 @@ static void buildLines(Level& L) {
     L.lines.insert(L.lines.end(), byColour[c].begin(), byColour[c].end());
   }
   L.colourStart[6] = (int)L.lines.size();
+  auto regionF4 = [&](int len) { return L.fine ? lineFactorF4<FineRows>(len) : lineFactorF4<CoarseRows>(len); };
   L.facBase.clear();
   size_t off = 0;
   for (const int4& ln : L.lines) {
     L.facBase.push_back((int)off);
-    off += lineFactorF4(ln.z);
+    off += regionF4(ln.z);
   }
   L.facF4 = off;
+  L.tile = L.fine ? smoothTile<FineRows>(L.maxLine) : smoothTile<CoarseRows>(L.maxLine);
+  for (int c = 0; c < 6; ++c) {
+    LineGeom& g = L.geom[c];
+    g = LineGeom{};
+    g.first = L.colourStart[c];
+    g.table = 1;
+    if (L.layers.size() != 1 || L.colourStart[c + 1] == L.colourStart[c]) continue;
+    const DLevelLayer& ly = L.layers[0];
+    const int fam = c < 3 ? 1 : 0, c3 = c % 3;
+    g.ly = ly;
+    g.start0 = ly.offset + (fam == 1 ? c3 : c3 * ly.nx);
+    g.startStep = fam == 1 ? 3 : 3 * ly.nx;
+    g.stride = fam == 1 ? ly.nx : 1;
+    g.len = fam == 1 ? ly.ny : ly.nx;
+    g.base0 = L.facBase[g.first];
+    g.baseStep = regionF4(g.len);
+    bool same = true;
+    for (int b = 0; b < L.colourStart[c + 1] - g.first; ++b) {
+      const int4 ln = L.lines[g.first + b];
+      same = same && ln.x == g.start0 + b * g.startStep && ln.y == g.stride && ln.z == g.len &&
+             L.facBase[g.first + b] == g.base0 + b * g.baseStep;
+    }
+    g.table = same ? 0 : 1;
+  }
 }
 
 }  // namespace btd
@@ -274,17 +302,27 @@ struct btd_solver {
       k_line_factor<CoarseRows><<<count, SM_THREADS, factorSmemBytes<CoarseRows>(L.maxLine), s>>>(L.dev(), L.dLines, L.dFacBase, L.fac);
   }
 
+  // One sweep of level k: the six colours, v-lines first (reversed for the post-smoother).
   void encSmooth(cudaStream_t s, int k, bool reverse) {
     Level& L = levels[k];
-    size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine) : smoothSmemBytes<CoarseRows>(L.maxLine);
+    const size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine, L.tile) : smoothSmemBytes<CoarseRows>(L.maxLine, L.tile);
+    const DLevel d = L.dev();
     for (int q = 0; q < 6; ++q) {
-      int c = reverse ? 5 - q : q;
-      int count = L.colourStart[c + 1] - L.colourStart[c];
+      const int c = reverse ? 5 - q : q;
+      const int count = L.colourStart[c + 1] - L.colourStart[c];
       if (count == 0) continue;
-      if (L.fine)
-        k_smooth<FineRows><<<count, SM_THREADS, smem, s>>>(L.dev(), L.dLines, L.dFacBase, L.fac, L.colourStart[c]);
-      else
-        k_smooth<CoarseRows><<<count, SM_THREADS, smem, s>>>(L.dev(), L.dLines, L.dFacBase, L.fac, L.colourStart[c]);
+      const LineGeom& g = L.geom[c];
+      if (L.fine) {
+        if (c < 3)
+          k_smooth<FineRows, 1><<<count, SM_THREADS, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+        else
+          k_smooth<FineRows, 0><<<count, SM_THREADS, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+      } else {
+        if (c < 3)
+          k_smooth<CoarseRows, 1><<<count, SM_THREADS, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+        else
+          k_smooth<CoarseRows, 0><<<count, SM_THREADS, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+      }
     }
   }
 
@@ -485,7 +523,16 @@ void btd_solver::encDamageGated(cudaStream_t s) { encDamage(s); }
 
 namespace {
 
+// A bounded device-side wait ran out (the kernel raised a flag in the counters and went on).
+struct DeviceTimeout : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
 int fail(const std::exception& e) {
+  if (dynamic_cast<const DeviceTimeout*>(&e)) {
+    btd::setError(e.what());
+    return BTD_E_TIMEOUT;
+  }
   if (dynamic_cast<const CudaError*>(&e)) {
     btd::setError(e.what());
     return BTD_E_CUDA;
@@ -713,7 +760,7 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
       L.B = s->alloc<float4>(L.N);
       L.R = s->alloc<float4>(L.N);
       L.pw = s->alloc<float4>(L.N);
-      const size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine) : smoothSmemBytes<CoarseRows>(L.maxLine);
+      const size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine, L.tile) : smoothSmemBytes<CoarseRows>(L.maxLine, L.tile);
       const size_t fsmem = L.fine ? factorSmemBytes<FineRows>(L.maxLine) : factorSmemBytes<CoarseRows>(L.maxLine);
       if (L.maxLine > SM_MAX_LINE || smem > 227 * 1024 || fsmem > 227 * 1024)
         throw std::invalid_argument("yarn lines of " + std::to_string(L.maxLine) + " nodes exceed the smoother's shared memory");
@@ -724,8 +771,14 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
     }
 
     // the smoother's dynamic shared memory: the largest line of each row layout
-    if (smemFine) CK(cudaFuncSetAttribute(k_smooth<FineRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemFine));
-    if (smemCoarse) CK(cudaFuncSetAttribute(k_smooth<CoarseRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemCoarse));
+    if (smemFine) {
+      CK(cudaFuncSetAttribute(k_smooth<FineRows, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemFine));
+      CK(cudaFuncSetAttribute(k_smooth<FineRows, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemFine));
+    }
+    if (smemCoarse) {
+      CK(cudaFuncSetAttribute(k_smooth<CoarseRows, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemCoarse));
+      CK(cudaFuncSetAttribute(k_smooth<CoarseRows, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemCoarse));
+    }
     if (fsmemFine) CK(cudaFuncSetAttribute(k_line_factor<FineRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmemFine));
     if (fsmemCoarse)
       CK(cudaFuncSetAttribute(k_line_factor<CoarseRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmemCoarse));
@@ -798,7 +851,19 @@ int btd_substeps(btd_solver* s, int32_t count) {
   });
 }
 
-int btd_synchronize(btd_solver* s) { GUARD({ checkSolver(s); s->sync(); }); }
+int btd_synchronize(btd_solver* s) {
+  GUARD({
+    checkSolver(s);
+    uint32_t flags = 0;
+    CK(cudaMemcpyAsync(&flags, s->dCounters + CNT_ERROR, sizeof flags, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+    if (flags) {
+      CK(cudaMemsetAsync(s->dCounters + CNT_ERROR, 0, sizeof flags, s->stream));
+      s->sync();
+      throw DeviceTimeout("a bounded device-side wait ran out (flags 0x" + std::to_string(flags) + "); results since the last synchronize are unreliable");
+    }
+  });
+}
 
 int btd_set_state(btd_solver* s, const float* pos4, const float* vel4) {
   GUARD({

@@ -167,6 +167,9 @@ int btd_substep(btd_solver* s, int32_t min_iterations, int32_t max_iterations);
 /* The engine's per-frame loop of substeps (worker.ts:664-674), stream-ordered, one launch each. */
 int btd_substeps(btd_solver* s, int32_t count);
 /* Wait for all submitted work (the reference's onSubmittedWorkDone). */
+/* Wait for the solver's stream (onSubmittedWorkDone). Returns BTD_E_TIMEOUT, once, when a bounded
+ * device-side wait (a staging copy's completion) ran out since the last call: the kernels never hang
+ * on one; they flag it in counter slot 20 and go on. */
 int btd_synchronize(btd_solver* s);
 
 /* setState (solver.ts:833-837): positions (4 floats per node) and velocities (NULL: zero). */
