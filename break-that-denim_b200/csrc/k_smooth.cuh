@@ -8,13 +8,15 @@
 //                  a coarse one), every line of the level in one launch: line rows (diagonal block
 //                  plus the Frobenius majorisation of the +-2 along-line couplings, and the +1 block),
 //                  then the partition method - the line cut into P chunks, each chunk's interior
-//                  eliminated in terms of the chunk's end unknowns - and odd-even cyclic reduction of
-//                  the 2P end equations. It stores every pivot inverse and multiplier a solve needs,
-//                  and a line-contiguous copy of each row's right-hand-side couplings.
+//                  eliminated in terms of the chunk's end unknowns - and the inverse of the system
+//                  of the 2P end equations (block LU, then one column per thread). It stores every
+//                  pivot inverse and multiplier a solve needs, and a line-contiguous copy of each
+//                  row's right-hand-side couplings.
 //   k_smooth       every sweep, one CTA per line of one colour: the lagged right-hand side (b minus the
 //                  off-line and +-2 couplings at the current iterate, plus the majorisation term), then
 //                  the same elimination applied to the right-hand side only - a short chain of 3x3
-//                  matrix-vector products - and the write-back.
+//                  matrix-vector products per chunk, one dense product for the end unknowns - and the
+//                  write-back.
 //
 // A sweep stages with cp.async, all copies of a tile in flight at once: the line's factors, its rows'
 // coupling copies (contiguous along the line whatever the family, so every 32-byte sector fetched is
@@ -28,8 +30,8 @@
 //     inverse Minv (padded 3x3; .y and .z of plane 2 hold the majorisation coefficient and whether
 //     the row is fixed), 3-5 Minv A (A the lower block), 6-8 G = Minv C, 9-11 V, 12-14 W (interior k:
 //     x_k = v_k + V_k x_s + W_k x_e); at a chunk's ends planes 0-2 hold the coupling into the chunk;
-//   per cyclic-reduction elimination (level by level) the multipliers al, ga (6 float4), then per
-//     reduced row Dinv, Dinv L, Dinv U (9 float4);
+//   the inverse of the 2P x 2P block-tridiagonal system of the chunks' end unknowns, dense (see
+//     denseStride);
 //   coupling planes p = 0..RC-1 of node k at p * len + k: the row's couplings other than the +-1
 //     along-line blocks, in coupling order (6 floats a block, 1 a scalar), zero where the neighbour is
 //     outside the layer or the row is fixed, then the rhs scale (0 on a fixed row, else 1) and the
@@ -42,11 +44,9 @@
 namespace btd {
 
 constexpr int SM_THREADS = 128;
-constexpr int SM_PMAX = 32;
+constexpr int SM_PMAX = 16;
 constexpr int SM_MAX_LINE = 512;
 constexpr int FAC_NODE = 15;
-constexpr int FAC_DOWN = 6;
-constexpr int FAC_BACK = 9;
 
 template <class Rows>
 struct SlotOf;
@@ -69,9 +69,13 @@ __host__ __device__ constexpr int linePartitions(int len) {
 // distinct shared-memory banks. A line's node arrays hold P S entries.
 __host__ __device__ constexpr int chunkSlot(int len) { return (len / linePartitions(len) + 1) | 1; }
 __host__ __device__ constexpr int lineNodesPadded(int len) { return linePartitions(len) * chunkSlot(len); }
-// float4 count of the factors of a line (node planes and reduced system)
+// The reduced system's inverse: 3Q x 3Q floats, column j at j (3Q + 1) (an odd stride: the threads
+// that build one column each, and those that read one row each, fall in distinct banks).
+__host__ __device__ constexpr int denseStride(int Q) { return 3 * Q + 1; }
+__host__ __device__ constexpr int denseF4(int Q) { return (3 * Q * denseStride(Q) + 3) / 4; }
+// float4 count of the factors of a line (node planes and the reduced system's inverse)
 __host__ __device__ constexpr int lineSolveF4(int len) {
-  return FAC_NODE * lineNodesPadded(len) + (FAC_DOWN + FAC_BACK) * 2 * linePartitions(len);
+  return FAC_NODE * lineNodesPadded(len) + denseF4(2 * linePartitions(len));
 }
 template <class Rows>
 __host__ __device__ constexpr int lineFactorF4(int len) {
@@ -224,8 +228,9 @@ struct Coupling<CoarseRows> {
 // Chunk t of a line of len nodes cut into P chunks: [ks, ke]; idx is a node's padded position.
 struct Chunks {
   int P, base, extra, S;
-  __device__ Chunks(int len)
+  __host__ __device__ Chunks(int len)
       : P(linePartitions(len)), base(len / linePartitions(len)), extra(len % linePartitions(len)), S(chunkSlot(len)) {}
+  __host__ __device__ Chunks(int P_, int base_, int extra_, int S_) : P(P_), base(base_), extra(extra_), S(S_) {}
   __device__ int start(int t) const { return t * base + min(t, extra); }
   __device__ int size(int t) const { return base + (t < extra ? 1 : 0); }
   __device__ int of(int k) const {
@@ -295,8 +300,7 @@ __global__ void __launch_bounds__(SM_THREADS) k_line_factor(DLevel L, const int4
   float4* qL = sF + lineSolveF4(len);   // 3 per reduced row
   float4* qD = qL + 3 * 2 * SM_PMAX;
   float4* qU = qD + 3 * 2 * SM_PMAX;
-  float4* fDown = sF + FAC_NODE * NP;
-  float4* fBack = fDown + FAC_DOWN * Q;
+  float* dense = reinterpret_cast<float*>(sF + FAC_NODE * NP);
   float4* out = fac + base[blockIdx.x];
   const int local0 = n0 - ly.offset;
   const int i0 = local0 % ly.nx, j0 = local0 / ly.nx;
@@ -379,47 +383,37 @@ __global__ void __launch_bounds__(SM_THREADS) k_line_factor(DLevel L, const int4
   }
   __syncthreads();
 
-  // ---- odd-even cyclic reduction of the 2P reduced rows. At stride s = 2^lv the rows with
-  // (q + 1) % 2s == 0 eliminate their neighbours q -+ s, which no longer change; their multipliers
-  // go to slot (rows of the smaller strides) + (q + 1) / 2s - 1.
-  int lv = 0, off = 0;
-  while ((2 << lv) <= Q) {
-    const int s = 1 << lv, q = tid;
-    if (q < Q && ((q + 1) & (2 * s - 1)) == 0) {
-      const int lo = q - s;
-      const M3 al = m3Mul(ldM(qL + 3 * q), pivotInverse(ldM(qD + 3 * lo)));
-      M3 D = m3Sub(ldM(qD + 3 * q), m3Mul(al, ldM(qU + 3 * lo)));
-      const M3 Lq = m3Neg(m3Mul(al, ldM(qL + 3 * lo)));
-      M3 Uq = m3Zero(), ga = m3Zero();
-      if (q + s < Q) {
-        const int hi = q + s;
-        ga = m3Mul(ldM(qU + 3 * q), pivotInverse(ldM(qD + 3 * hi)));
-        D = m3Sub(D, m3Mul(ga, ldM(qL + 3 * hi)));
-        Uq = m3Neg(m3Mul(ga, ldM(qU + 3 * hi)));
-      }
-      const int slot = off + ((q + 1) >> (lv + 1)) - 1;
-      stM(fDown + FAC_DOWN * slot, al);
-      stM(fDown + FAC_DOWN * slot + 3, ga);
-      stM(qD + 3 * q, D);
-      stM(qL + 3 * q, Lq);
-      stM(qU + 3 * q, Uq);
+  // ---- the reduced system's inverse. Block LU by one thread (rows q of L, D, U: pivot inverses
+  // Dinv_q of D_q - L_q G_{q-1}, G_q = Dinv_q U_q, in place of D and U), then column j of the inverse
+  // by thread j: forward y_q = Dinv_q (e_j - L_q y_{q-1}), back x_q = y_q - G_q x_{q+1}, in place.
+  if (tid == 0) {
+    M3 G = m3Zero();
+    for (int q = 0; q < Q; ++q) {
+      const M3 Lq = ldM(qL + 3 * q);
+      const M3 Dinv = pivotInverse(m3Sub(ldM(qD + 3 * q), m3Mul(Lq, G)));
+      G = m3Mul(Dinv, ldM(qU + 3 * q));
+      stM(qD + 3 * q, Dinv);
+      stM(qU + 3 * q, G);
     }
-    __syncthreads();
-    off += Q >> (lv + 1);
-    ++lv;
   }
-  for (; lv >= 0; --lv) {
-    const int s = 1 << lv, q = tid;
-    if (q < Q && ((q + 1) & (s - 1)) == 0 && ((q + 1) & s) != 0) {
-      const M3 Dinv = pivotInverse(ldM(qD + 3 * q));
-      const M3 DL = q >= s ? m3Mul(Dinv, ldM(qL + 3 * q)) : m3Zero();
-      const M3 DU = q + s < Q ? m3Mul(Dinv, ldM(qU + 3 * q)) : m3Zero();
-      stM(fBack + FAC_BACK * q, Dinv);
-      stM(fBack + FAC_BACK * q + 3, DL);
-      stM(fBack + FAC_BACK * q + 6, DU);
+  __syncthreads();
+  const int QS = denseStride(Q);
+  for (int j = tid; j < 3 * Q; j += SM_THREADS) {
+    float* col = dense + j * QS;
+    float3 y = make_float3(0, 0, 0);
+    for (int q = 0; q < Q; ++q) {
+      float3 b = make_float3(q == j / 3 && j % 3 == 0 ? 1.f : 0.f, q == j / 3 && j % 3 == 1 ? 1.f : 0.f,
+                             q == j / 3 && j % 3 == 2 ? 1.f : 0.f);
+      y = m3Vec(ldM(qD + 3 * q), b - m3Vec(ldM(qL + 3 * q), y));
+      col[3 * q] = y.x, col[3 * q + 1] = y.y, col[3 * q + 2] = y.z;
     }
-    __syncthreads();
+    float3 x = y;
+    for (int q = Q - 2; q >= 0; --q) {
+      x = make_float3(col[3 * q], col[3 * q + 1], col[3 * q + 2]) - m3Vec(ldM(qU + 3 * q), x);
+      col[3 * q] = x.x, col[3 * q + 1] = x.y, col[3 * q + 2] = x.z;
+    }
   }
+  __syncthreads();
 
   // ---- node planes and reduced system out, coalesced
   const int total = lineSolveF4(len);
@@ -434,32 +428,42 @@ struct LineGeom {
   int first;  // table index of block 0
   int table;
   int start0, startStep, stride, len, base0, baseStep;
+  int across0;  // position of line 0 across its family (line b at across0 + 3 b)
+  int P, chunkBase, chunkExtra, S;  // the lines' chunks (Chunks(len))
   DLevelLayer ly;
 };
 
+// One CTA per line, blockDim.x threads (a multiple of 32, up to SM_SWEEP_THREADS).
+constexpr int SM_SWEEP_THREADS = 256;
+__host__ inline int sweepThreads(int maxLine) { return std::min(SM_SWEEP_THREADS, std::max(64, (maxLine + 31) / 32 * 32)); }
+
 template <class Rows, int FAM>
-__global__ void __launch_bounds__(SM_THREADS) k_smooth(DLevel L, LineGeom g, const int4* __restrict__ lines, const int* __restrict__ base,
+__global__ void __launch_bounds__(SM_SWEEP_THREADS) k_smooth(DLevel L, LineGeom g, const int4* __restrict__ lines, const int* __restrict__ base,
                                                        const float4* __restrict__ fac, int T, uint32_t* err) {
   __shared__ uint64_t bar;
   using Cp = Coupling<Rows>;
   constexpr int RC = SlotOf<Rows>::RC, CF = SlotOf<Rows>::COEF_FLOATS;
   extern __shared__ float4 sm4[];
-  int n0, st, len, fb;
+  int n0, st, len, fb, across0;
   DLevelLayer ly;
+  Chunks ch(g.P, g.chunkBase, g.chunkExtra, g.S);
   if (g.table) {
     const int4 line = lines[g.first + blockIdx.x];
     n0 = line.x, st = line.y, len = line.z;
     ly = L.layers[line.w >> 1];
     fb = base[g.first + blockIdx.x];
+    ch = Chunks(len);
+    across0 = FAM == 0 ? (n0 - ly.offset) / ly.nx : (n0 - ly.offset) % ly.nx;
   } else {
     n0 = g.start0 + blockIdx.x * g.startStep, st = g.stride, len = g.len;
     ly = g.ly;
     fb = g.base0 + blockIdx.x * g.baseStep;
+    across0 = g.across0 + 3 * blockIdx.x;
   }
-  const int tid = threadIdx.x;
-  const Chunks ch(len);
-  const int P = ch.P, Q = 2 * P, NP = lineNodesPadded(len), S = ch.S;
-  const int solveF4 = lineSolveF4(len);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int P = ch.P, Q = 2 * P, S = ch.S, NP = P * S;
+  const int QS = denseStride(Q);
+  const int solveF4 = FAC_NODE * NP + denseF4(Q);
   const int TX = T + 4;
   float4* sF = sm4;
   float4* sCp = sF + solveF4;  // coupling planes of the tile, plane stride T
@@ -469,12 +473,9 @@ __global__ void __launch_bounds__(SM_THREADS) k_smooth(DLevel L, LineGeom g, con
   float4* sV = sR + NP;        // h, then v
   float4* qr = sV + NP;
   float4* qx = qr + 2 * SM_PMAX;
-  const float4* fDown = sF + FAC_NODE * NP;
-  const float4* fBack = fDown + FAC_DOWN * Q;
+  const float* dense = reinterpret_cast<const float*>(sF + FAC_NODE * NP);
   const float4* src = fac + fb;
-  // the line's position across its family, and the node step to the neighbouring line
-  const int local0 = n0 - ly.offset;
-  const int across0 = FAM == 0 ? local0 / ly.nx : local0 % ly.nx;
+  // lines across the family, and the node step to the neighbouring line
   const int nAcross = FAM == 0 ? ly.ny : ly.nx, acrossStep = FAM == 0 ? ly.nx : 1;
 
   // ---- stage: the factors and, tile by tile, the coupling planes by bulk copies (thread 0), the
@@ -497,18 +498,18 @@ __global__ void __launch_bounds__(SM_THREADS) k_smooth(DLevel L, LineGeom g, con
 #pragma unroll
     for (int a = 0; a < 5; ++a) {
       const int c = across0 + a - 2;
-      for (int kk = tid; kk < tn + 4; kk += SM_THREADS) {
+      for (int kk = tid; kk < tn + 4; kk += nt) {
         const int k = k0 + kk - 2;
         const bool ok = k >= 0 && k < len && c >= 0 && c < nAcross;
         cpAsync16(sX + a * TX + kk, L.X + (ok ? n0 + k * st + (a - 2) * acrossStep : n0), ok);
       }
     }
-    for (int kk = tid; kk < tn; kk += SM_THREADS) cpAsync16(sBt + kk, L.B + n0 + (k0 + kk) * st, true);
+    for (int kk = tid; kk < tn; kk += nt) cpAsync16(sBt + kk, L.B + n0 + (k0 + kk) * st, true);
     cpAsyncWaitAll();
     mbarWaitBounded(&bar, phase, err);
     phase ^= 1u;
     __syncthreads();
-    for (int kk = tid; kk < tn; kk += SM_THREADS) {
+    for (int kk = tid; kk < tn; kk += nt) {
       const float4* cp = sCp + kk;
       const float4* xc = sX + kk + 2;
       float3 r = colF(cp, CF, T) * f3(sBt[kk]);
@@ -526,67 +527,71 @@ __global__ void __launch_bounds__(SM_THREADS) k_smooth(DLevel L, LineGeom g, con
           r -= colSym(cp, pos, T) * xm;
         pos += Cp::width(q);
       }
-      stV(sR + ch.idx(k0 + kk), r + colF(cp, CF + 1, T) * f3(xc[2 * TX]));
+      r = r + colF(cp, CF + 1, T) * f3(xc[2 * TX]);
+      // interior nodes of a chunk keep Minv r, the chain's independent half
+      const int k = k0 + kk, t = ch.of(k), ks = ch.start(t), ix = t * S + (k - ks);
+      if (k != ks && k != ks + ch.size(t) - 1) r = m3Vec(ldM(sF + ix, NP), r);
+      stV(sR + ix, r);
     }
     __syncthreads();
   }
 
-  // ---- warp 0: chunk interiors (lane t, chunk t): h_k = Minv_k r_k - (Minv A)_k h_{k-1},
-  // v_k = h_k - G_k v_{k+1}; the reduced right-hand sides; then cyclic reduction, the rows of each
-  // level on consecutive lanes (at most Q / 2 <= 32 of them), synchronised within the warp
-  if (tid < 32) {
+  // ---- chunk interiors, lane t of warp 0 on chunk t: h_k = (Minv r)_k - (Minv A)_k h_{k-1},
+  // v_k = h_k - G_k v_{k+1} (each step's matrices loaded a step ahead, off the dependent chain);
+  // then the reduced right-hand sides
+  if (tid < P) {
     const int lane = tid;
-    if (lane < P) {
-      const int ks = ch.start(lane), mlen = ch.size(lane), ke = ks + mlen - 1;
-      const int o = lane * S - ks;  // padded position of node k: o + k
-      float3 h = make_float3(0, 0, 0);
+    const int ks = ch.start(lane), mlen = ch.size(lane), ke = ks + mlen - 1;
+    const int o = lane * S - ks;  // padded position of node k: o + k
+    float3 h = make_float3(0, 0, 0);
+    if (ks + 1 < ke) {
+      M3 Qa = ldM(sF + 3 * NP + o + ks + 1, NP);
+      float3 tk = ldV(sR + o + ks + 1);
       for (int k = ks + 1; k < ke; ++k) {
-        h = m3Vec(ldM(sF + o + k, NP), ldV(sR + o + k)) - m3Vec(ldM(sF + 3 * NP + o + k, NP), h);
+        M3 QaN = Qa;
+        float3 tN = tk;
+        if (k + 1 < ke) QaN = ldM(sF + 3 * NP + o + k + 1, NP), tN = ldV(sR + o + k + 1);
+        h = tk - m3Vec(Qa, h);
         stV(sV + o + k, h);
+        Qa = QaN, tk = tN;
       }
-      float3 v = make_float3(0, 0, 0), vS = v, vE = v;
+    }
+    float3 v = make_float3(0, 0, 0), vS = v, vE = v;
+    if (ks + 1 < ke) {
+      M3 Gk = ldM(sF + 6 * NP + o + ke - 1, NP);
+      float3 hk = ldV(sV + o + ke - 1);
       for (int k = ke - 1; k > ks; --k) {
-        v = ldV(sV + o + k) - m3Vec(ldM(sF + 6 * NP + o + k, NP), v);
+        M3 GN = Gk;
+        float3 hN = hk;
+        if (k - 1 > ks) GN = ldM(sF + 6 * NP + o + k - 1, NP), hN = ldV(sV + o + k - 1);
+        v = hk - m3Vec(Gk, v);
         stV(sV + o + k, v);
         if (k == ke - 1) vE = v;
+        Gk = GN, hk = hN;
       }
-      if (mlen >= 3) vS = v;
-      stV(qr + 2 * lane, ldV(sR + o + ks) - m3Vec(ldM(sF + o + ks, NP), vS));
-      stV(qr + 2 * lane + 1, ldV(sR + o + ke) - m3Vec(ldM(sF + o + ke, NP), vE));
     }
-    __syncwarp();
-    // down: at stride s = 2^lv, row q = 2s (m + 1) - 1 on lane m takes its multipliers from slot
-    // (rows of the smaller strides) + m
-    int lv = 0, off = 0;
-    for (; (2 << lv) <= Q; ++lv) {
-      const int s = 1 << lv, cnt = Q >> (lv + 1);
-      if (lane < cnt) {
-        const int q = ((lane + 1) << (lv + 1)) - 1;
-        const float4* f = fDown + FAC_DOWN * (off + lane);
-        float3 r = ldV(qr + q) - m3Vec(ldM(f), ldV(qr + q - s));
-        if (q + s < Q) r = r - m3Vec(ldM(f + 3), ldV(qr + q + s));
-        stV(qr + q, r);
-      }
-      __syncwarp();
-      off += cnt;
+    if (mlen >= 3) vS = v;
+    stV(qr + 2 * lane, ldV(sR + o + ks) - m3Vec(ldM(sF + o + ks, NP), vS));
+    stV(qr + 2 * lane + 1, ldV(sR + o + ke) - m3Vec(ldM(sF + o + ke, NP), vE));
+  }
+  __syncthreads();
+
+  // ---- the end unknowns: x = inverse . r, thread o on output o (3Q of them)
+  for (int o = tid; o < 3 * Q; o += nt) {
+    const float* row = dense + o;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for (int q = 0; q < Q; ++q) {
+      const float4 rq = qr[q];
+      a0 = fmaf(row[(3 * q) * QS], rq.x, a0);
+      a1 = fmaf(row[(3 * q + 1) * QS], rq.y, a1);
+      a2 = fmaf(row[(3 * q + 2) * QS], rq.z, a2);
     }
-    // up: at stride s the rows q = s (2m + 1) - 1 on lane m
-    for (; lv >= 0; --lv) {
-      const int s = 1 << lv, q = s * (2 * lane + 1) - 1;
-      if (q < Q) {
-        const float4* f = fBack + FAC_BACK * q;
-        float3 x = m3Vec(ldM(f), ldV(qr + q));
-        if (q >= s) x = x - m3Vec(ldM(f + 3), ldV(qx + q - s));
-        if (q + s < Q) x = x - m3Vec(ldM(f + 6), ldV(qx + q + s));
-        stV(qx + q, x);
-      }
-      __syncwarp();
-    }
+    reinterpret_cast<float*>(qx)[4 * (o / 3) + o % 3] = (a0 + a1) + a2;
   }
   __syncthreads();
 
   // ---- recovery and write-back, every node in parallel (fixed rows keep their unknowns)
-  for (int k = tid; k < len; k += SM_THREADS) {
+  for (int k = tid; k < len; k += nt) {
     const int t = ch.of(k);
     const int ks = ch.start(t), ke = ks + ch.size(t) - 1;
     const int ix = t * S + (k - ks);

@@ -58,6 +58,7 @@ struct Level {
   // line factors (k_line_factor): each line's region starts at facBase[line]
   std::vector<int> facBase;
   int tile = 0;          // sweep staging tile (nodes)
+  int threads = 0;       // sweep CTA size
   LineGeom geom[6] = {};  // launch geometry per colour
   int* dFacBase = nullptr;
   float4* fac = nullptr;
@@ -108,6 +109,7 @@ static void buildLines(Level& L) {
   }
   L.facF4 = off;
   L.tile = L.fine ? smoothTile<FineRows>(L.maxLine) : smoothTile<CoarseRows>(L.maxLine);
+  L.threads = sweepThreads(L.maxLine);
   for (int c = 0; c < 6; ++c) {
     LineGeom& g = L.geom[c];
     g = LineGeom{};
@@ -123,6 +125,9 @@ static void buildLines(Level& L) {
     g.len = fam == 1 ? ly.ny : ly.nx;
     g.base0 = L.facBase[g.first];
     g.baseStep = regionF4(g.len);
+    g.across0 = c3;
+    const Chunks ch(g.len);
+    g.P = ch.P, g.chunkBase = ch.base, g.chunkExtra = ch.extra, g.S = ch.S;
     bool same = true;
     for (int b = 0; b < L.colourStart[c + 1] - g.first; ++b) {
       const int4 ln = L.lines[g.first + b];
@@ -314,14 +319,14 @@ struct btd_solver {
       const LineGeom& g = L.geom[c];
       if (L.fine) {
         if (c < 3)
-          k_smooth<FineRows, 1><<<count, SM_THREADS, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+          k_smooth<FineRows, 1><<<count, L.threads, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
         else
-          k_smooth<FineRows, 0><<<count, SM_THREADS, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+          k_smooth<FineRows, 0><<<count, L.threads, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
       } else {
         if (c < 3)
-          k_smooth<CoarseRows, 1><<<count, SM_THREADS, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+          k_smooth<CoarseRows, 1><<<count, L.threads, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
         else
-          k_smooth<CoarseRows, 0><<<count, SM_THREADS, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+          k_smooth<CoarseRows, 0><<<count, L.threads, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
       }
     }
   }
