@@ -231,6 +231,7 @@ struct Chunks {
   __host__ __device__ Chunks(int len)
       : P(linePartitions(len)), base(len / linePartitions(len)), extra(len % linePartitions(len)), S(chunkSlot(len)) {}
   __host__ __device__ Chunks(int P_, int base_, int extra_, int S_) : P(P_), base(base_), extra(extra_), S(S_) {}
+  __host__ __device__ Chunks() : P(1), base(1), extra(0), S(1) {}
   __device__ int start(int t) const { return t * base + min(t, extra); }
   __device__ int size(int t) const { return base + (t < extra ? 1 : 0); }
   __device__ int of(int k) const {
@@ -437,29 +438,47 @@ struct LineGeom {
 constexpr int SM_SWEEP_THREADS = 256;
 __host__ inline int sweepThreads(int maxLine) { return std::min(SM_SWEEP_THREADS, std::max(64, (maxLine + 31) / 32 * 32)); }
 
-template <class Rows, int FAM>
-__global__ void __launch_bounds__(SM_SWEEP_THREADS) k_smooth(DLevel L, LineGeom g, const int4* __restrict__ lines, const int* __restrict__ base,
-                                                       const float4* __restrict__ fac, int T, uint32_t* err) {
-  __shared__ uint64_t bar;
-  using Cp = Coupling<Rows>;
-  constexpr int RC = SlotOf<Rows>::RC, CF = SlotOf<Rows>::COEF_FLOATS;
-  extern __shared__ float4 sm4[];
+// One line of a sweep, its geometry resolved.
+struct LineAt {
   int n0, st, len, fb, across0;
   DLevelLayer ly;
-  Chunks ch(g.P, g.chunkBase, g.chunkExtra, g.S);
-  if (g.table) {
-    const int4 line = lines[g.first + blockIdx.x];
-    n0 = line.x, st = line.y, len = line.z;
-    ly = L.layers[line.w >> 1];
-    fb = base[g.first + blockIdx.x];
-    ch = Chunks(len);
-    across0 = FAM == 0 ? (n0 - ly.offset) / ly.nx : (n0 - ly.offset) % ly.nx;
-  } else {
-    n0 = g.start0 + blockIdx.x * g.startStep, st = g.stride, len = g.len;
-    ly = g.ly;
-    fb = g.base0 + blockIdx.x * g.baseStep;
-    across0 = g.across0 + 3 * blockIdx.x;
-  }
+  Chunks ch;
+};
+__device__ __forceinline__ LineAt lineAt(const LineGeom& g, int b) {
+  return LineAt{g.start0 + b * g.startStep, g.stride,  g.len, g.base0 + b * g.baseStep, g.across0 + 3 * b,
+                g.ly,                       Chunks(g.P, g.chunkBase, g.chunkExtra, g.S)};
+}
+
+// Thread 0: the first tile's bulk copies of a line (its factors and coupling planes), completing
+// the mbarrier's current phase.
+template <class Rows>
+__device__ __forceinline__ void issueLineCopies(const LineAt& a, const float4* __restrict__ fac, int T, float4* sm4, uint64_t* bar) {
+  constexpr int RC = SlotOf<Rows>::RC;
+  const int Q = 2 * a.ch.P, NP = a.ch.P * a.ch.S;
+  const int solveF4 = FAC_NODE * NP + denseF4(Q);
+  const int tn = min(T, a.len);
+  const float4* src = fac + a.fb;
+  float4* sCp = sm4 + solveF4;
+  fenceProxyAsync();
+  const unsigned coefBytes = 16u * RC * tn;
+  mbarExpectTx(bar, coefBytes + 16u * solveF4);
+  bulkCopy(sm4, src, 16u * solveF4, bar);
+  if (tn == a.len && a.len == T)
+    bulkCopy(sCp, src + solveF4, coefBytes, bar);
+  else
+    for (int p = 0; p < RC; ++p) bulkCopy(sCp + p * T, src + solveF4 + p * a.len, 16u * tn, bar);
+}
+
+// Solve line `a` in place of its unknowns. The mbarrier `bar` is initialised; `phase` is the parity
+// its next phase completes with; with `prefetched` thread 0 already issued the first tile's copies.
+template <class Rows, int FAM>
+__device__ __forceinline__ void sweepLine(const DLevel& L, const LineAt& a, const float4* __restrict__ fac, int T, uint32_t* err,
+                                          float4* sm4, uint64_t* bar, unsigned& phase, bool prefetched) {
+  using Cp = Coupling<Rows>;
+  constexpr int RC = SlotOf<Rows>::RC, CF = SlotOf<Rows>::COEF_FLOATS;
+  const int n0 = a.n0, st = a.st, len = a.len, across0 = a.across0;
+  const DLevelLayer ly = a.ly;
+  const Chunks ch = a.ch;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int P = ch.P, Q = 2 * P, S = ch.S, NP = P * S;
   const int QS = denseStride(Q);
@@ -474,26 +493,19 @@ __global__ void __launch_bounds__(SM_SWEEP_THREADS) k_smooth(DLevel L, LineGeom 
   float4* qr = sV + NP;
   float4* qx = qr + 2 * SM_PMAX;
   const float* dense = reinterpret_cast<const float*>(sF + FAC_NODE * NP);
-  const float4* src = fac + fb;
+  const float4* src = fac + a.fb;
   // lines across the family, and the node step to the neighbouring line
   const int nAcross = FAM == 0 ? ly.ny : ly.nx, acrossStep = FAM == 0 ? ly.nx : 1;
 
   // ---- stage: the factors and, tile by tile, the coupling planes by bulk copies (thread 0), the
   // unknowns and b by cp.async (strided along a v-line); then build r
-  if (tid == 0) mbarInit(&bar, 1);
-  __syncthreads();
-  unsigned phase = 0;
   for (int k0 = 0; k0 < len; k0 += T) {
     const int tn = min(T, len - k0);
-    if (tid == 0) {
+    if (tid == 0 && k0 == 0 && !prefetched) issueLineCopies<Rows>(a, fac, T, sm4, bar);
+    if (tid == 0 && k0 > 0) {
       fenceProxyAsync();
-      const unsigned coefBytes = 16u * RC * tn;
-      mbarExpectTx(&bar, coefBytes + (k0 == 0 ? 16u * solveF4 : 0u));
-      if (k0 == 0) bulkCopy(sF, src, 16u * solveF4, &bar);
-      if (tn == len && len == T)
-        bulkCopy(sCp, src + solveF4, coefBytes, &bar);
-      else
-        for (int p = 0; p < RC; ++p) bulkCopy(sCp + p * T, src + solveF4 + p * len + k0, 16u * tn, &bar);
+      mbarExpectTx(bar, 16u * RC * tn);
+      for (int p = 0; p < RC; ++p) bulkCopy(sCp + p * T, src + solveF4 + p * len + k0, 16u * tn, bar);
     }
 #pragma unroll
     for (int a = 0; a < 5; ++a) {
@@ -506,7 +518,7 @@ __global__ void __launch_bounds__(SM_SWEEP_THREADS) k_smooth(DLevel L, LineGeom 
     }
     for (int kk = tid; kk < tn; kk += nt) cpAsync16(sBt + kk, L.B + n0 + (k0 + kk) * st, true);
     cpAsyncWaitAll();
-    mbarWaitBounded(&bar, phase, err);
+    mbarWaitBounded(bar, phase, err);
     phase ^= 1u;
     __syncthreads();
     for (int kk = tid; kk < tn; kk += nt) {
@@ -606,6 +618,29 @@ __global__ void __launch_bounds__(SM_SWEEP_THREADS) k_smooth(DLevel L, LineGeom 
       x = ldV(sV + ix) + m3Vec(ldM(sF + 9 * NP + ix, NP), xs) + m3Vec(ldM(sF + 12 * NP + ix, NP), xe);
     L.X[n0 + k * st] = make_float4(x.x, x.y, x.z, 0.f);
   }
+}
+
+
+template <class Rows, int FAM>
+__global__ void __launch_bounds__(SM_SWEEP_THREADS) k_smooth(DLevel L, LineGeom g, const int4* __restrict__ lines, const int* __restrict__ base,
+                                                       const float4* __restrict__ fac, int T, uint32_t* err) {
+  __shared__ uint64_t bar;
+  extern __shared__ float4 sm4[];
+  LineAt a;
+  if (g.table) {
+    const int4 line = lines[g.first + blockIdx.x];
+    a.n0 = line.x, a.st = line.y, a.len = line.z;
+    a.ly = L.layers[line.w >> 1];
+    a.fb = base[g.first + blockIdx.x];
+    a.ch = Chunks(a.len);
+    a.across0 = FAM == 0 ? (a.n0 - a.ly.offset) / a.ly.nx : (a.n0 - a.ly.offset) % a.ly.nx;
+  } else {
+    a = lineAt(g, blockIdx.x);
+  }
+  if (threadIdx.x == 0) mbarInit(&bar, 1);
+  __syncthreads();
+  unsigned phase = 0;
+  sweepLine<Rows, FAM>(L, a, fac, T, err, sm4, &bar, phase, false);
 }
 
 }  // namespace btd
