@@ -92,5 +92,5 @@ def config0(seed=1):
 def solver_params(h, newton_iterations, pcg_rel_tol, pcg_cap=500, **kw):
     from .solver import default_params
 
-    return default_params(h=h, newton_iterations=newton_iterations, newton_max=newton_iterations, pcg_iterations=pcg_cap,
-                          pcg_rel_tol=pcg_rel_tol, **kw)
+    kw.setdefault("newton_max", newton_iterations)
+    return default_params(h=h, newton_iterations=newton_iterations, pcg_iterations=pcg_cap, pcg_rel_tol=pcg_rel_tol, **kw)

@@ -357,4 +357,11 @@ __global__ void k_commit(StepArgs A) {
   A.x[n] = make_float4(xn.x + d.x, xn.y + d.y, xn.z + d.z, xn.w);
 }
 
+// gate (gate.wgsl:12-23): the next optional Newton iteration runs only while iteration `prev` moved
+// some node by more than the tolerance (the graph's conditional node reads the decision).
+__global__ void k_gate(const uint32_t* __restrict__ counters, int prev, const SimParams* __restrict__ P, cudaGraphConditionalHandle h) {
+  const float moved = __uint_as_float(counters[CNT_UPDATE + prev]);
+  cudaGraphSetConditional(h, moved > P->newtonTol ? 1u : 0u);
+}
+
 }  // namespace btd

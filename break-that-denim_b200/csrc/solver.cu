@@ -144,7 +144,7 @@ using namespace btd;
 
 struct btd_solver {
   int device = 0;
-  cudaStream_t stream = nullptr, bodyStream = nullptr;
+  cudaStream_t stream = nullptr, bodyStream = nullptr, gateStream = nullptr;
   btd_params params{};
   SimParams hostP{};
   int N = 0, C = 0, nLayers = 0;
@@ -410,12 +410,22 @@ struct btd_solver {
     }
   }
 
-  void runSubstepEager(int newtonIterations) {
+  // The substep launched kernel by kernel; a gated iteration runs when the host reads that the one
+  // before moved some node by more than the tolerance.
+  void runSubstepEager(int newtonIterations, int newtonMax) {
     cudaStream_t s = stream;
     const bool grips = gripsOn();
     CK(cudaMemsetAsync(dCounters + CNT_UPDATE, 0, sizeof(uint32_t) * MAX_NEWTON, s));
     encPredict(s, grips);
-    for (int it = 0; it < newtonIterations; ++it) {
+    for (int it = 0; it < newtonMax; ++it) {
+      if (it >= newtonIterations) {
+        uint32_t moved = 0;
+        CK(cudaMemcpyAsync(&moved, dCounters + CNT_UPDATE + it - 1, sizeof moved, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        float m;
+        std::memcpy(&m, &moved, sizeof m);
+        if (!(m > hostP.newtonTol)) break;
+      }
       encGripTerms(s, grips);
       encAssemble(s, it == 0 || !params.lag_coarse);
       runPCGEager(s);
@@ -472,10 +482,40 @@ struct btd_solver {
   }
   void encDamageGated(cudaStream_t s);
 
-  void encSubstep(cudaStream_t s, int newtonIterations, bool grips) {
+  // Gated Newton iteration `it` (encodeSubstep's optional iterations, solver.ts:744-757; gate.wgsl):
+  // a conditional node runs it only while iteration it - 1 still moved some node by more than the
+  // tolerance. A skipped iteration leaves its update slot at zero, so every later one stays off.
+  // Must be called while `s` is capturing.
+  void encGatedNewton(cudaStream_t s, int it, bool grips) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nDeps = 0;
+    CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nDeps));
+    if (st != cudaStreamCaptureStatusActive) throw std::runtime_error("gated Newton iterations must be encoded into a graph capture");
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    k_gate<<<1, 1, 0, s>>>(dCounters, it - 1, dP, h);
+    CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nDeps));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nDeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    CK(cudaStreamBeginCaptureToGraph(gateStream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    encNewton(gateStream, it, grips);
+    cudaGraph_t out;
+    CK(cudaStreamEndCapture(gateStream, &out));
+  }
+
+  void encSubstep(cudaStream_t s, int newtonIterations, int newtonMax, bool grips) {
     CK(cudaMemsetAsync(dCounters + CNT_UPDATE, 0, sizeof(uint32_t) * MAX_NEWTON, s));
     encPredict(s, grips);
     for (int it = 0; it < newtonIterations; ++it) encNewton(s, it, grips);
+    for (int it = newtonIterations; it < newtonMax; ++it) encGatedNewton(s, it, grips);
     encFinalize(s);
   }
 
@@ -497,14 +537,27 @@ struct btd_solver {
     return ex;
   }
 
-  cudaGraphExec_t substepGraph(int iters) {
+  // Newton iterations of a substep asked for min / max iterations (encodeSubstep, solver.ts:744-746).
+  int unconditional(int minIterations) const { return std::min(MAX_NEWTON, std::max(params.newton_iterations, minIterations)); }
+  int gatedBound(int minIterations, int maxIterations) const {
+    return std::min(MAX_NEWTON, std::max(std::max(params.newton_max, unconditional(minIterations)), maxIterations));
+  }
+
+  cudaGraphExec_t substepGraph(int iters, int itersMax) {
     const bool grips = gripsOn();
-    const int key = 2 * iters + (grips ? 1 : 0);
+    const int key = (iters * (MAX_NEWTON + 1) + itersMax) * 2 + (grips ? 1 : 0);
     auto it = substepExec.find(key);
     if (it != substepExec.end()) return it->second;
-    cudaGraphExec_t ex = capture([&](cudaStream_t s) { encSubstep(s, iters, grips); });
+    cudaGraphExec_t ex = capture([&](cudaStream_t s) { encSubstep(s, iters, itersMax, grips); });
     substepExec[key] = ex;
     return ex;
+  }
+  void runSubstep(int minIterations, int maxIterations) {
+    const int iters = unconditional(minIterations), itersMax = gatedBound(minIterations, maxIterations);
+    if (useGraphs)
+      CK(cudaGraphLaunch(substepGraph(iters, itersMax), stream));
+    else
+      runSubstepEager(iters, itersMax);
   }
 
   void pushParams() {
@@ -519,6 +572,7 @@ struct btd_solver {
     for (void* q : allocs) cudaFree(q);
     if (stream) cudaStreamDestroy(stream);
     if (bodyStream) cudaStreamDestroy(bodyStream);
+    if (gateStream) cudaStreamDestroy(gateStream);
   }
 };
 
@@ -613,6 +667,7 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
     CK(cudaGetDevice(&s->device));
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&s->bodyStream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&s->gateStream, cudaStreamNonBlocking));
     s->params = *prm;
     const int N = sc->node_count, C = sc->crossing_count;
     s->N = N;
@@ -815,7 +870,7 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
     CK(cudaMemcpyAsync(s->tails, s->tails0.data(), sizeof(float) * 4 * N, cudaMemcpyHostToDevice, st));
     if (C > 0) CK(cudaMemcpyAsync(s->damage, s->damage0.data(), 2 * (size_t)C, cudaMemcpyHostToDevice, st));
     s->sync();
-    s->substepGraph(prm->newton_iterations);
+    s->substepGraph(s->unconditional(0), s->gatedBound(0, 0));
     s->pcgExec = s->capture([&](cudaStream_t q) { s->encPCG(q); });
     s->sync();
     *out = s.release();
@@ -835,12 +890,7 @@ int btd_destroy(btd_solver* s) {
 int btd_substep(btd_solver* s, int32_t min_iterations, int32_t max_iterations) {
   GUARD({
     checkSolver(s);
-    int iters = std::min(MAX_NEWTON, std::max(s->params.newton_iterations, (int)min_iterations));
-    (void)max_iterations;
-    if (s->useGraphs)
-      CK(cudaGraphLaunch(s->substepGraph(iters), s->stream));
-    else
-      s->runSubstepEager(iters);
+    s->runSubstep(min_iterations, max_iterations);
   });
 }
 
@@ -848,9 +898,9 @@ int btd_substeps(btd_solver* s, int32_t count) {
   GUARD({
     checkSolver(s);
     if (!s->useGraphs) {
-      for (int k = 0; k < count; ++k) s->runSubstepEager(s->params.newton_iterations);
+      for (int k = 0; k < count; ++k) s->runSubstepEager(s->unconditional(0), s->gatedBound(0, 0));
     } else {
-      cudaGraphExec_t ex = s->substepGraph(s->params.newton_iterations);
+      cudaGraphExec_t ex = s->substepGraph(s->unconditional(0), s->gatedBound(0, 0));
       for (int k = 0; k < count; ++k) CK(cudaGraphLaunch(ex, s->stream));
     }
   });
@@ -1302,10 +1352,7 @@ int btd_profile_stage(btd_solver* s, int32_t which, int32_t reps, int32_t flush,
           s->encHierarchy(s->stream);
           break;
         default:
-          if (s->useGraphs)
-            CK(cudaGraphLaunch(s->substepGraph(s->params.newton_iterations), s->stream));
-          else
-            s->runSubstepEager(s->params.newton_iterations);
+          s->runSubstep(0, 0);
       }
       CK(cudaEventRecord(e1, s->stream));
       CK(cudaEventSynchronize(e1));
@@ -1341,7 +1388,9 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
     const int64_t hierarchy = 3 * (L - 1);
     const int64_t hierPerSubstep = s->params.lag_coarse ? hierarchy : hierarchy * (newton / std::max(1, substeps));
     const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips;
-    *out = (int64_t)substeps * (perSubstep + hierPerSubstep) + (int64_t)newton * perNewton + (int64_t)(pcg - newton) * (V + 4);
+    // each optional (gated) Newton iteration slot adds its gate kernel, run or not
+    const int64_t gates = s->gatedBound(0, 0) - s->unconditional(0);
+    *out = (int64_t)substeps * (perSubstep + hierPerSubstep + gates) + (int64_t)newton * perNewton + (int64_t)(pcg - newton) * (V + 4);
   });
 }
 
