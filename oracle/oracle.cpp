@@ -647,6 +647,21 @@ struct Solver {
     return true;
   }
 
+  // The z step of node n bounded against the floor from its iterate step linz (floorLowest,
+  // common.wgsl:262-265; floorBound, step.wgsl:78-86): a node comes down at most to where its weight
+  // alone would sink it into the penalty (or twice its current depth), never below half thickness.
+  double floorBoundZ(int n, double linz, double dz) const {
+    if (!floor.on) return dz;
+    double half = 0.5 * layer(n).thickness;
+    double delta = half + floor.bulge;
+    double gmag = std::sqrt(prm.gravity[0] * prm.gravity[0] + prm.gravity[1] * prm.gravity[1] + prm.gravity[2] * prm.gravity[2]);
+    double sWeight = std::sqrt(mass[n] * gmag * delta / floor.stiffness);
+    double z0 = x[3 * n + 2], zLin = z0 + linz;
+    double s = std::max(delta - (zLin - floor.z), 0.0);
+    double lowest = std::min(std::max(floor.z + delta - std::max(sWeight, 2 * s), floor.z + half), zLin);
+    return std::max(dz, lowest - z0);
+  }
+
   // nodeGradient (solver.ts(ref):387-422).
   void nodeGradient(int n, double* g) const {
     g[0] = g[1] = g[2] = 0;
@@ -905,6 +920,10 @@ struct Solver {
         pred[3 * n + q] = pinned[n] ? 0 : hv + h * h * prm.gravity[q];
         dx[3 * n + q] = hv;
       }
+    // projectStart (step.wgsl:90-95): the predicted start bounded against the floor
+    if (floor.on)
+      for (int n = 0; n < N; ++n)
+        if (!pinned[n]) dx[3 * n + 2] = floorBoundZ(n, 0.0, dx[3 * n + 2]);
   }
 
   // segTension (solver.ts(ref):647-652).
@@ -1742,8 +1761,15 @@ double Solver::newtonStep(int* pcgDone, double* rel, double* alphaOut) {
     alpha = chooseStep(e, mag);
   }
   double m = 0;
+  for (size_t q = 0; q < d.size(); ++q) d[q] *= alpha;
+  // newtonApply's floor bound (step.wgsl:97-112): the applied step is what is left of it
+  if (floor.on)
+    for (int n = 0; n < N; ++n) {
+      if (pinned[n]) continue;
+      double old = dx[3 * n + 2];
+      d[3 * n + 2] = floorBoundZ(n, old, old + d[3 * n + 2]) - old;
+    }
   for (size_t q = 0; q < d.size(); ++q) {
-    d[q] *= alpha;
     dx[q] += d[q];
     m = std::max(m, std::fabs(d[q]));
   }
