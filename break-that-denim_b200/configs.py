@@ -89,6 +89,71 @@ def config0(seed=1):
     return hanging_patch(64, 0.3, seed=seed)
 
 
+# Yarn damage: a 128 x 128 lattice over 0.3 m bundled [2, 2], so that the yarn field resolves two
+# warps and two picks per span: the central 32 x 32 cells hold 64 warp and 64 weft yarns.
+CONFIG1 = dict(n=128, size=0.3, bundle=(2, 2), region=32, yarn_ea=2e3, yarn_bending=1e-7, crossing_friction=0.3,
+               break_strain=0.08, break_sigma=0.25, grip_speed=0.2, grip_stiffness=2e4, h=1 / 120, newton_iterations=4,
+               pcg_rel_tol=1e-6, steps=120)
+
+
+def yarn_material(pitch, ea, bending, crossing_friction, areal_density=0.35, shear=200.0):
+    """A weave of linear yarns at yarn pitch `pitch`: per-yarn EA (N) and rigidity (N m^2), the areal
+    density shared by the two families, DENIM's viscosities, drag and crossing law otherwise."""
+    m = material_preset(0)
+    m.name = b"yarns"
+    m.pitch_u = pitch
+    m.pitch_v = pitch
+    for f in range(2):
+        y = m.yarns[f]
+        y.linear_density = 0.5 * areal_density * pitch
+        y.ea_low = ea
+        y.ea_high = ea
+        y.ea_compress = 0.5 * ea
+        y.bend_rigidity = bending
+        y.strength = ea * 10.0
+        y.yarns_per_span = 0
+    m.shear_stiffness = shear
+    m.crossing_friction = crossing_friction
+    return m
+
+
+def config1(seed=11):
+    """Yarn damage: CONFIG1's lattice, no pins. Outside the central region the yarns hold (break at
+    1000 % strain); inside, each yarn segment at a crossing breaks at a strain drawn from
+    lognormal(ln 0.08, 0.25), its field strength the tension T(eps) = EA eps of the linear law.
+    Returns the scene and the two grips: the edge columns i = 0, 1 and i = n - 2, n - 1."""
+    c = CONFIG1
+    n, bu, bv = c["n"], c["bundle"][0], c["bundle"][1]
+    pitch = c["size"] / (n - 1)
+    m = yarn_material(pitch / bu, c["yarn_ea"], c["yarn_bending"], c["crossing_friction"])
+    sc = compile_scene(layer_spec(m, (n - 0.5) * pitch, (n - 0.5) * pitch, bundle=(bu, bv), collar_rows=0, seed=seed))
+    assert sc.nx == n and sc.ny == n, (sc.nx, sc.ny)
+    sc.pinned[:] = 0
+    L = sc.layers[0]
+    K, M = L.field_k, L.field_m
+    # field strength of yarn family f at crossing (pick m, warp k): index 2 (m K + k) + f
+    strength = np.full((M, K, 2), c["yarn_ea"] * 10.0, np.float32)
+    lo = (n - c["region"]) // 2
+    ks, ms = slice(lo * bu, (lo + c["region"]) * bu), slice(lo * bv, (lo + c["region"]) * bv)
+    eps = np.exp(np.log(c["break_strain"]) + c["break_sigma"] * normal(seed + 1, strength[ms, ks].size))
+    strength[ms, ks] = (c["yarn_ea"] * eps).reshape(strength[ms, ks].shape)
+    sc.field_strength[:] = strength.reshape(-1)
+    left = np.array([j * n + i for j in range(n) for i in (0, 1)], np.int32)
+    right = np.array([j * n + i for j in range(n) for i in (n - 2, n - 1)], np.int32)
+    return sc, left, right
+
+
+def break_events(field, seg_flags):
+    """The break-event set (yarnField.ts:36-43, 483-492): (crossing, family) pairs whose damage code
+    separates the yarn (cut 255 or pulled out 254), and the spans that ruptured (broken, not an
+    initial defect)."""
+    f = np.asarray(field).reshape(-1)
+    sep = set(np.nonzero(f >= 254)[0].tolist())
+    flags = np.asarray(seg_flags).reshape(-1)
+    spans = set(np.nonzero(((flags & 2) != 0) & ((flags & 4) == 0))[0].tolist())
+    return sep, spans
+
+
 def solver_params(h, newton_iterations, pcg_rel_tol, pcg_cap=500, **kw):
     from .solver import default_params
 

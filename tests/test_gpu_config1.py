@@ -1,0 +1,66 @@
+"""Yarn damage (configuration 1) on the CUDA path against the oracle: a 128 x 128 lattice bundled
+[2, 2] whose central 32 x 32 cells break at lognormal strains, pulled apart by two edge grips at
+0.2 m/s. The break-event set (yarnField.ts:36-43, 483-492) - separated (crossing, family) pairs and
+ruptured spans - is the comparison: the same set when the sheet first tears, and the same to 1 % a
+further 0.1 s into the tear (the torn edges' motion then amplifies rounding differences).
+"""
+import numpy as np
+import pytest
+
+import btd_b200 as btd
+from helpers import MG, copy_state
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def jaccard(a, b):
+    return len(a & b) / max(1, len(a | b))
+
+
+def test_config1_break_events_match_oracle():
+    c = btd.configs.CONFIG1
+    sc, left, right = btd.configs.config1()
+    cpu = Oracle(sc, h=c["h"], newton_iterations=c["newton_iterations"], pcg_iterations=500, pcg_rel_tol=c["pcg_rel_tol"], **MG)
+    gpu = btd.GpuSolver(sc, btd.configs.solver_params(c["h"], c["newton_iterations"], c["pcg_rel_tol"]))
+    x0, _ = copy_state(cpu, gpu)
+    xf = x0.astype(np.float32).astype(np.float64)
+    k = c["grip_stiffness"]
+    grips = []
+    for slot, nodes, sign in ((0, left, -1.0), (1, right, 1.0)):
+        picked = int(nodes[len(nodes) // 2])
+        anchor = xf[picked].copy()
+        w = np.ones(len(nodes))
+        gpu.attach_patch(slot, picked, nodes, w, anchor.astype(np.float32), k, max_lead=1.0)
+        cpu.add_grip(nodes, w, (xf[nodes] - xf[picked]).reshape(-1), anchor, k)
+        grips.append((slot, anchor, sign))
+    first = {}
+    for s in range(1, 37):
+        for slot, anchor, sign in grips:
+            t = (anchor + np.array([sign * 0.5 * c["grip_speed"] * s * c["h"], 0, 0])).astype(np.float32)
+            gpu.set_target(t, slot=slot)
+            cpu.set_grip_goal(slot, t.astype(np.float64))
+        cpu.substep()
+        gpu.substep()
+        sep_c, sp_c = btd.configs.break_events(cpu.field(), cpu.segments()["seg_flags"])
+        sep_g, sp_g = btd.configs.break_events(gpu.field(), gpu.segments()["seg_flags"])
+        if sep_c and "cpu" not in first:
+            first["cpu"] = s
+        if sep_g and "gpu" not in first:
+            first["gpu"] = s
+        if s == 18:
+            # before any break: the same motion (converged-schedule bound, correctness.ts:271)
+            xc = cpu.x
+            assert not sep_c and not sep_g
+            assert np.abs(gpu.x.astype(np.float64) - xc).max() < 0.03 * np.abs(xc - x0).max()
+        if s == first.get("cpu") == first.get("gpu"):
+            assert sep_c == sep_g and sp_c == sp_g, (len(sep_c), len(sep_g), len(sp_c), len(sp_g))
+    assert first.get("cpu") == first.get("gpu") and first["cpu"] < 36, first
+    assert len(sep_c) > 1000 and len(sp_c) > 200, (len(sep_c), len(sp_c))
+    assert jaccard(sep_c, sep_g) >= 0.99, jaccard(sep_c, sep_g)
+    assert jaccard(sp_c, sp_g) >= 0.99, jaccard(sp_c, sp_g)
+    # every rupture lies in the weak central region
+    n, lo, r = c["n"], (c["n"] - c["region"]) // 2, c["region"]
+    nodes = np.array(sorted(sp_g)) // 2
+    i, j = nodes % n, nodes // n
+    assert ((i >= lo - 1) & (i < lo + r + 1) & (j >= lo - 1) & (j < lo + r + 1)).all()
