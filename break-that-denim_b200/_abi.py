@@ -190,6 +190,7 @@ SIGNATURES = {
     "btd_level_nodes": ([C.c_void_p, C.c_int32, _p(C.c_int32)], C.c_int),
     "btd_read_operator": ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p], C.c_int),
     "btd_read_vector": ([C.c_void_p, C.c_int32, C.c_int32, C.c_void_p], C.c_int),
+    "btd_read_delta_f64": ([C.c_void_p, C.c_void_p], C.c_int),
     "btd_write_vector": ([C.c_void_p, C.c_int32, C.c_int32, C.c_void_p], C.c_int),
     "btd_profile_stage": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, _p(C.c_float)], C.c_int),
     "btd_launch_count": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, _p(C.c_int64)], C.c_int),

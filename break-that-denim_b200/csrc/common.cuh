@@ -76,6 +76,9 @@ struct Scalars {
   double rz, rzNew, pAp, alpha, beta, r0, rr, rel;
   double e[4], m[4];
   int pcgIt, converged, lineAlphaIdx, pad;
+  int check;    // the recurrence residual met the tolerance: the true residual decides
+  int restart;  // the residual was replaced by the true one: the next direction starts afresh
+  int pad4, pad5;
   float lineAlpha;
   float pad1, pad2, pad3;
 };

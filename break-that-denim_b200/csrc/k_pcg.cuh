@@ -76,6 +76,8 @@ struct PcgArgs {
   float4* p;
   float4* Ap;
   float4* delta;
+  float4* b0;  // the right-hand side PCG started from (the true residual's b)
+  double* dd;  // the iterate accumulated in FP64, 3 per node (delta is its fp32 copy)
   Scalars* scal;
   const SimParams* P;
   uint32_t* counters;
@@ -94,7 +96,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_init(PcgArgs a) {
   double v[1] = {0.0};
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < a.F.N; n += gridDim.x * blockDim.x) {
     a.delta[n] = make_float4(0, 0, 0, 0);
+    a.dd[3 * n] = a.dd[3 * n + 1] = a.dd[3 * n + 2] = 0.0;
     a.F.X[n] = make_float4(0, 0, 0, 0);
+    a.b0[n] = a.F.B[n];
     float3 r = f3(a.F.B[n]);
     v[0] += (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
   }
@@ -106,6 +110,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_init(PcgArgs a) {
     s.rel = s.r0 > 0.0 ? 1.0 : 0.0;
     s.pcgIt = 0;
     s.converged = 0;
+    s.check = 0;
+    s.restart = 0;
   }
 }
 
@@ -119,9 +125,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_dot_rz(PcgArgs a, int first
   double out[1];
   if (gridReduce<1>(a.red, v, out) && threadIdx.x == 0) {
     Scalars& s = *a.scal;
-    if (first) {
+    if (first || s.restart) {
       s.beta = 0.0;
       s.rz = out[0];
+      s.restart = 0;
     } else {
       s.beta = safeDiv(out[0], s.rz);
       s.rz = out[0];
@@ -143,6 +150,13 @@ __global__ void k_pcg_update_p(PcgArgs a, int first) {
   a.p[n] = make_float4(p.x, p.y, p.z, 0.f);
 }
 
+// Symmetric fp32 block times an FP64 vector, in FP64.
+__device__ __forceinline__ void symVecAddD(const Sym& A, const double* x, double& y0, double& y1, double& y2) {
+  y0 += (double)A.xx * x[0] + (double)A.xy * x[1] + (double)A.xz * x[2];
+  y1 += (double)A.xy * x[0] + (double)A.yy * x[1] + (double)A.yz * x[2];
+  y2 += (double)A.xz * x[0] + (double)A.yz * x[1] + (double)A.zz * x[2];
+}
+
 // Ap = A p (fixed rows 0), p . Ap; alpha = rz / pAp (0 and stop when pAp <= 0, as pcg() breaks).
 __global__ void __launch_bounds__(RED_THREADS) k_pcg_matvec(PcgArgs a) {
   double v[1] = {0.0};
@@ -153,14 +167,22 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_matvec(PcgArgs a) {
       int i, j, l;
       nodeCoord(F, n, &i, &j, &l);
       const DLevelLayer L = F.layers[l];
-      y = FineRows::diag(F.op, F.N, n) * f3(a.p[n]);
+      // fp32 products summed in FP64: the recurrence residual then drifts from the true one by the
+      // rounding of the stored Ap only
+      double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+      const float3 pn = f3(a.p[n]);
+      const double pd[3] = {pn.x, pn.y, pn.z};
+      symVecAddD(FineRows::diag(F.op, F.N, n), pd, y0, y1, y2);
 #pragma unroll
       for (int k = 0; k < FineRows::NC; ++k) {
         int2 off = FineRows::offset(k);
         int m = levelNode(L, i + off.x, j + off.y);
         if (m < 0) continue;
-        y += FineRows::coupling(F.op, F.N, n, k) * f3(a.p[m]);
+        const float3 pm = f3(a.p[m]);
+        const double q[3] = {pm.x, pm.y, pm.z};
+        symVecAddD(FineRows::coupling(F.op, F.N, n, k), q, y0, y1, y2);
       }
+      y = make_float3((float)y0, (float)y1, (float)y2);
     }
     a.Ap[n] = make_float4(y.x, y.y, y.z, 0.f);
     float3 p = f3(a.p[n]);
@@ -179,14 +201,25 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_matvec(PcgArgs a) {
   }
 }
 
-// delta += alpha p; r -= alpha Ap; z = 0; ||r||; the convergence test sets the while condition.
+__device__ __forceinline__ void pcgStop(const PcgArgs& a, Scalars& s) {
+  a.counters[CNT_PCG_LAST] = (uint32_t)s.pcgIt;
+  atomicAdd(&a.counters[CNT_PCG_TOTAL], (uint32_t)s.pcgIt);
+  a.counters[CNT_REL] = __float_as_uint((float)s.rel);
+}
+
+// delta += alpha p (accumulated in FP64, kept in fp32 too); r -= alpha Ap; z = 0; ||r||. The
+// iteration cap, a breakdown or a zero right-hand side stop the loop (the while condition); the
+// recurrence residual meeting the tolerance hands the decision to k_pcg_true_residual.
 __global__ void __launch_bounds__(RED_THREADS) k_pcg_update_xr(PcgArgs a) {
   double v[1] = {0.0};
-  const float alpha = (float)a.scal->alpha;
+  const double alphaD = a.scal->alpha;
+  const float alpha = (float)alphaD;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < a.F.N; n += gridDim.x * blockDim.x) {
-    float3 d = f3(a.delta[n]) + alpha * f3(a.p[n]);
+    const float3 pn = f3(a.p[n]);
+    const double d0 = a.dd[3 * n] + alphaD * pn.x, d1 = a.dd[3 * n + 1] + alphaD * pn.y, d2 = a.dd[3 * n + 2] + alphaD * pn.z;
+    a.dd[3 * n] = d0, a.dd[3 * n + 1] = d1, a.dd[3 * n + 2] = d2;
     float3 r = f3(a.F.B[n]) - alpha * f3(a.Ap[n]);
-    a.delta[n] = make_float4(d.x, d.y, d.z, 0.f);
+    a.delta[n] = make_float4((float)d0, (float)d1, (float)d2, 0.f);
     a.F.B[n] = make_float4(r.x, r.y, r.z, 0.f);
     a.F.X[n] = make_float4(0, 0, 0, 0);
     v[0] += (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
@@ -198,12 +231,58 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_update_xr(PcgArgs a) {
     s.rr = out[0];
     s.rel = s.r0 > 0.0 ? sqrt(out[0]) / s.r0 : 0.0;
     s.pcgIt += 1;
-    bool stop = s.converged != 0 || s.pcgIt >= P.pcgMax || (P.pcgTol > 0.0 && s.rel <= P.pcgTol) || !(s.r0 > 0.0);
+    const bool met = P.pcgTol > 0.0 && s.rel <= P.pcgTol;
+    const bool stop = s.converged != 0 || s.pcgIt >= P.pcgMax || !(s.r0 > 0.0);
     if (stop && s.converged == 0) s.converged = 1;
+    s.check = !stop && met ? 1 : 0;
+    if (stop) pcgStop(a, s);
+    if (a.useCond) cudaGraphSetConditional(a.cond, stop ? 0u : 1u);
+  }
+}
+
+
+// The outer residual, when the recurrence residual met the tolerance: r = b0 - A delta with the
+// FP64 iterate, every product and sum in FP64, ||r|| in FP64. Met: PCG stops. Not met (the fp32
+// recurrence drifted): r replaces the recurrence residual (stored fp32) and the next direction starts
+// afresh (keeping the old one stalls: measured ~10x more iterations), so the fp32 iterations solve
+// for a correction that accumulates into the FP64 iterate - iterative refinement.
+__global__ void __launch_bounds__(RED_THREADS) k_pcg_true_residual(PcgArgs a) {
+  if (!a.scal->check) return;
+  double v[1] = {0.0};
+  const DLevel& F = a.F;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < F.N; n += gridDim.x * blockDim.x) {
+    const float3 b = f3(a.b0[n]);
+    double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+    if (!F.fixed[n]) {
+      int i, j, l;
+      nodeCoord(F, n, &i, &j, &l);
+      const DLevelLayer L = F.layers[l];
+      symVecAddD(FineRows::diag(F.op, F.N, n), a.dd + 3 * n, y0, y1, y2);
+#pragma unroll
+      for (int k = 0; k < FineRows::NC; ++k) {
+        int2 off = FineRows::offset(k);
+        int m = levelNode(L, i + off.x, j + off.y);
+        if (m < 0) continue;
+        symVecAddD(FineRows::coupling(F.op, F.N, n, k), a.dd + 3 * m, y0, y1, y2);
+      }
+    }
+    const double r0 = (double)b.x - y0, r1 = (double)b.y - y1, r2 = (double)b.z - y2;
+    a.F.B[n] = make_float4((float)r0, (float)r1, (float)r2, 0.f);
+    v[0] += r0 * r0 + r1 * r1 + r2 * r2;
+  }
+  double out[1];
+  if (gridReduce<1>(a.red, v, out) && threadIdx.x == 0) {
+    Scalars& s = *a.scal;
+    const SimParams& P = *a.P;
+    s.rr = out[0];
+    s.rel = s.r0 > 0.0 ? sqrt(out[0]) / s.r0 : 0.0;
+    s.check = 0;
+    const bool stop = s.rel <= P.pcgTol || s.pcgIt >= P.pcgMax;
     if (stop) {
-      a.counters[CNT_PCG_LAST] = (uint32_t)s.pcgIt;
-      atomicAdd(&a.counters[CNT_PCG_TOTAL], (uint32_t)s.pcgIt);
-      a.counters[CNT_REL] = __float_as_uint((float)s.rel);
+      s.converged = 1;
+      pcgStop(a, s);
+    } else {
+      s.restart = 1;
     }
     if (a.useCond) cudaGraphSetConditional(a.cond, stop ? 0u : 1u);
   }

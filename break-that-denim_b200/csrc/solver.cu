@@ -164,7 +164,8 @@ struct btd_solver {
   NodeStatic* dNodes = nullptr;
   DLayer* dLayers = nullptr;
   float4 *x = nullptr, *v = nullptr, *dx = nullptr, *pred = nullptr, *ext = nullptr, *delta = nullptr, *p = nullptr,
-         *Ap = nullptr;
+         *Ap = nullptr, *b0 = nullptr;
+  double* deltaD = nullptr;
   Seg* segs = nullptr;
   float *softening = nullptr, *failSite = nullptr, *tails = nullptr, *strain = nullptr, *strength = nullptr;
   uint8_t *damage = nullptr, *area = nullptr, *sep = nullptr, *marks = nullptr;
@@ -235,6 +236,8 @@ struct btd_solver {
     a.p = p;
     a.Ap = Ap;
     a.delta = delta;
+    a.b0 = b0;
+    a.dd = deltaD;
     a.scal = dScal;
     a.P = dP;
     a.counters = dCounters;
@@ -357,6 +360,7 @@ struct btd_solver {
     k_pcg_update_p<<<blocksFor(N, 256), 256, 0, s>>>(a, 0);
     k_pcg_matvec<<<redBlocks, RED_THREADS, 0, s>>>(a);
     k_pcg_update_xr<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    k_pcg_true_residual<<<redBlocks, RED_THREADS, 0, s>>>(a);
   }
 
   // encodePCG (solver.ts:625-644) with the device-side stop: prologue, then a while-node whose
@@ -377,6 +381,7 @@ struct btd_solver {
     k_pcg_update_p<<<blocksFor(N, 256), 256, 0, s>>>(a, 1);
     k_pcg_matvec<<<redBlocks, RED_THREADS, 0, s>>>(a);
     k_pcg_update_xr<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    k_pcg_true_residual<<<redBlocks, RED_THREADS, 0, s>>>(a);
     CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nDeps));
     cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
     cp.conditional.handle = h;
@@ -401,6 +406,7 @@ struct btd_solver {
     k_pcg_update_p<<<blocksFor(N, 256), 256, 0, s>>>(a, 1);
     k_pcg_matvec<<<redBlocks, RED_THREADS, 0, s>>>(a);
     k_pcg_update_xr<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    k_pcg_true_residual<<<redBlocks, RED_THREADS, 0, s>>>(a);
     for (;;) {
       int conv = 0;
       CK(cudaMemcpyAsync(&conv, &dScal->converged, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -740,6 +746,8 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
     s->delta = s->alloc<float4>(N);
     s->p = s->alloc<float4>(N);
     s->Ap = s->alloc<float4>(N);
+    s->b0 = s->alloc<float4>(N);
+    s->deltaD = s->alloc<double>(3 * (size_t)N);
     s->segs = s->alloc<Seg>(2 * (size_t)N);
     s->softening = s->alloc<float>(2 * (size_t)N);
     s->failSite = s->alloc<float>(2 * (size_t)N);
@@ -1379,18 +1387,18 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
     const int L = (int)s->levels.size();
     int64_t V = s->params.coarse_sweeps * colours(L - 1);
     for (int k = 0; k + 1 < L; ++k) V += 2 * colours(k) + 3;
-    // per Newton iteration: assembly, PCG prologue (init + V-cycle + 4), line search, apply; the
-    // hierarchy (weights + RAP per coarse level) on the first iteration; V-cycle + 4 per extra PCG pass
+    // per Newton iteration: assembly, PCG prologue (init + V-cycle + 5), line search, apply; the
+    // hierarchy (weights + RAP per coarse level) on the first iteration; V-cycle + 5 per extra PCG pass
     // held grips add their lead once per substep and their terms once per Newton iteration; the
     // assembly and every Galerkin product are followed by their level's line factorisation
     const int64_t grips = s->gripsOn() ? 1 : 0;
-    const int64_t perNewton = 2 + (1 + V + 4) + 1 + 1 + grips;
+    const int64_t perNewton = 2 + (1 + V + 5) + 1 + 1 + grips;
     const int64_t hierarchy = 3 * (L - 1);
     const int64_t hierPerSubstep = s->params.lag_coarse ? hierarchy : hierarchy * (newton / std::max(1, substeps));
     const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips;
     // each optional (gated) Newton iteration slot adds its gate kernel, run or not
     const int64_t gates = s->gatedBound(0, 0) - s->unconditional(0);
-    *out = (int64_t)substeps * (perSubstep + hierPerSubstep + gates) + (int64_t)newton * perNewton + (int64_t)(pcg - newton) * (V + 4);
+    *out = (int64_t)substeps * (perSubstep + hierPerSubstep + gates) + (int64_t)newton * perNewton + (int64_t)(pcg - newton) * (V + 5);
   });
 }
 
@@ -1530,6 +1538,15 @@ int btd_read_vector(btd_solver* s, int32_t which, int32_t level, float* out4) {
     size_t n;
     float4* p = vectorPtr(s, which, level, &n);
     CK(cudaMemcpyAsync(out4, p, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+  });
+}
+
+int btd_read_delta_f64(btd_solver* s, double* out3) {
+  GUARD({
+    checkSolver(s);
+    if (!out3) throw std::invalid_argument("null output");
+    CK(cudaMemcpyAsync(out3, s->deltaD, sizeof(double) * 3 * (size_t)s->N, cudaMemcpyDeviceToHost, s->stream));
     s->sync();
   });
 }

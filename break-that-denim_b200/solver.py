@@ -291,6 +291,12 @@ class GpuSolver:
         check("btd_read_vector", self._h, self.VEC[which], level, out.ctypes.data_as(C.c_void_p))
         return out[:, :3].astype(np.float64)
 
+    def delta_f64(self):
+        """The last PCG iterate accumulated in FP64, (N, 3)."""
+        out = np.zeros((self.N, 3))
+        check("btd_read_delta_f64", self._h, out.ctypes.data_as(C.c_void_p))
+        return out
+
     def write_vector(self, which, values, level=0):
         n = self.level_nodes(level) if self.VEC[which] <= 2 else self.N
         buf = np.zeros((n, 4), np.float32)

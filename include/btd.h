@@ -235,6 +235,9 @@ int btd_read_operator(btd_solver* s, int32_t level, double* out, uint8_t* fixed)
 #define BTD_VEC_DX 4
 #define BTD_VEC_PRED 5
 int btd_read_vector(btd_solver* s, int32_t which, int32_t level, float* out4);
+/* The last PCG solve's iterate as accumulated in FP64 (3 doubles per node); delta (BTD_VEC_DELTA) is
+ * its fp32 copy. The outer residual that stops PCG at pcg_rel_tol is b - A x computed from it. */
+int btd_read_delta_f64(btd_solver* s, double* out3);
 /* Zero-copy access for consumers that bind the solver's buffers (the renderer and tools read
  * GpuSolver.x, .levels[k].op etc. directly, solver.ts:198-263): device pointer and size in bytes of
  * buffer `which` (BTD_VEC_* above, or BTD_BUF_*) of `level`. The pointer stays valid until

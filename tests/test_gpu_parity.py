@@ -106,6 +106,43 @@ def test_pcg_relative_residual_stop(staged):
     assert max_abs_rel_to_scale(dg, dc) < 1e-3
 
 
+def operator_apply(A, nx, ny, d):
+    """y = A d with a level operator in the reference's 25-offset layout (offset o: di = o % 5 - 2,
+    dj = o // 5 - 2), in FP64."""
+    y = np.zeros_like(d)
+    i, j = np.meshgrid(np.arange(nx), np.arange(ny))
+    i, j = i.reshape(-1), j.reshape(-1)
+    for o in range(25):
+        di, dj = o % 5 - 2, o // 5 - 2
+        ok = (i + di >= 0) & (i + di < nx) & (j + dj >= 0) & (j + dj < ny)
+        n = np.nonzero(ok)[0]
+        m = (j[ok] + dj) * nx + (i[ok] + di)
+        y[n] += np.einsum("nab,nb->na", A[n, o], d[m])
+    return y
+
+
+def test_pcg_stops_on_the_fp64_true_residual(staged):
+    """At rel-res 1e-6 the stop is decided by the outer residual b - A delta computed in FP64 from
+    the fp32 operator and the iterate accumulated in FP64 (an fp32 iterate alone bottoms out near
+    4e-6 on this coupon): recomputed here from the read-back operator, it meets the bound."""
+    sc, cpu, gpu = staged
+    A_gpu, _ = gpu.read_operator(0)
+    b = gpu.read_vector("B")
+    gpu.set_pcg(500, 1e-6)
+    gpu.encode_pcg()
+    d = gpu.delta_f64()
+    d32 = gpu.read_vector("delta")
+    c = gpu.counter_dict()
+    gpu.set_pcg(2, 0.0)
+    gpu.write_vector("B", b)
+    r = b - operator_apply(A_gpu, sc.nx, sc.ny, d)
+    rel = np.linalg.norm(r) / np.linalg.norm(b)
+    assert rel <= 1e-6 * 1.01, rel
+    assert abs(c["rel_residual"] - rel) <= 0.05 * rel + 1e-9, (c["rel_residual"], rel)
+    # the fp32 copy that the Newton step applies is the FP64 iterate rounded
+    assert np.abs(d32 - d).max() <= 1e-6 * np.abs(d).max()
+
+
 def dynamics(cpu, gpu, steps):
     x0, _ = copy_state(cpu, gpu)
     for _ in range(steps):
