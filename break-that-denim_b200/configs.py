@@ -158,4 +158,5 @@ def solver_params(h, newton_iterations, pcg_rel_tol, pcg_cap=500, **kw):
     from .solver import default_params
 
     kw.setdefault("newton_max", newton_iterations)
+    kw.setdefault("self_contact", 0)  # the configurations without contact
     return default_params(h=h, newton_iterations=newton_iterations, pcg_iterations=pcg_cap, pcg_rel_tol=pcg_rel_tol, **kw)

@@ -22,6 +22,7 @@
 
 #include "btd.h"
 #include "common.cuh"
+#include "k_contact.cuh"
 #include "k_grip.cuh"
 #include "k_history.cuh"
 #include "k_mg.cuh"
@@ -173,6 +174,34 @@ struct btd_solver {
   std::vector<DLayer> hostLayers;
   // grips (interaction.ts attachPatch/setTarget/release): device slots + entries, host mirror of
   // the slots, the base stiffness of each (setHold scales it) and the slot holding each node
+  // self-contact (selfcontact.ts): hash table, hashed faces, candidates and bound keys, bounds,
+  // fixed-point accumulators; allocated when params.self_contact
+  unsigned* ctCells = nullptr;
+  float4* ctItems = nullptr;
+  unsigned* ctPairs = nullptr;
+  float4* cmeta = nullptr;
+  int* ctAcc = nullptr;
+  bool contactOn() const { return params.self_contact != 0 && cmeta != nullptr; }
+  ContactArgs contactArgs() const {
+    ContactArgs a;
+    a.N = N;
+    a.nodes = dNodes;
+    a.layers = dLayers;
+    a.P = dP;
+    a.pinned = levels[0].fixed;
+    a.x = x;
+    a.dx = dx;
+    a.segs = segs;
+    a.cells = ctCells;
+    a.items = ctItems;
+    a.pairs = ctPairs;
+    a.cmeta = cmeta;
+    a.acc = ctAcc;
+    a.ext = ext;
+    // SELF_CONTACT (selfcontact.ts:7-33)
+    a.law = ContactLaw{12e-3f, 3e-3f, 1.0e-3f, 500.f, 0.45f, 0.002f, 0.45f, (1u << CT_TABLE_BITS) - 1u};
+    return a;
+  }
   GripSlot* dGripSlots = nullptr;
   GripEntry* dGripEntries = nullptr;
   float4* dGripGoal = nullptr;
@@ -213,7 +242,7 @@ struct btd_solver {
     a.pred = pred;
     a.segs = segs;
     a.ext = ext;
-    a.cmeta = nullptr;
+    a.cmeta = contactOn() ? cmeta : nullptr;
     a.counters = dCounters;
     a.scal = dScal;
     return a;
@@ -269,10 +298,36 @@ struct btd_solver {
 
   // encodePredict + preSubstep (solver.ts:742): predictor, then each held grip's lead from the
   // committed positions, then the start of the projected iterate.
+  // encodePredict, preSubstep and contact detection (solver.ts:738-745): predictor, each held grip's
+  // lead from the committed positions, the face hash and contact bounds at the predicted iterate,
+  // then the start of the projected iterate.
   void encPredict(cudaStream_t s, bool grips) {
     k_predict<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs());
     if (grips) k_grip_lead<<<GRIPS, 256, 0, s>>>(gripArgs());
+    if (contactOn()) encDetect(s);
     k_project_start<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs());
+  }
+
+  // SelfContact.encodeClear + encodeDetect (selfcontact.ts:137-152).
+  void encDetect(cudaStream_t s) {
+    const ContactArgs a = contactArgs();
+    const int T = 1 << CT_TABLE_BITS;
+    CK(cudaMemsetAsync(ctCells, 0, sizeof(unsigned) * 2 * (size_t)T, s));
+    k_ct_face_count<<<blocksFor(N, 128), 128, 0, s>>>(a);
+    k_ct_scan<<<1, CT_SCAN_THREADS, 0, s>>>(ctCells, T);
+    k_ct_face_fill<<<blocksFor(N, 128), 128, 0, s>>>(a);
+    k_ct_damage_row<<<blocksFor(N, 128), 128, 0, s>>>(a);
+    k_ct_detect<<<blocksFor(N, 128), 128, 0, s>>>(a);
+    k_ct_resolve<<<blocksFor(N, 128), 128, 0, s>>>(a);
+  }
+
+  // SelfContact.encodeTerms (selfcontact.ts:155-161): contact and friction at the current iterate,
+  // written over ext (grips add theirs after).
+  void encContactTerms(cudaStream_t s) {
+    if (!contactOn()) return;
+    const ContactArgs a = contactArgs();
+    k_ct_terms<<<blocksFor(N, 128), 128, 0, s>>>(a);
+    k_ct_gather<<<blocksFor(N, 128), 128, 0, s>>>(a);
   }
 
   // preAssemble (solver.ts:690): grip terms at the current iterate into ext.
@@ -432,6 +487,7 @@ struct btd_solver {
         std::memcpy(&m, &moved, sizeof m);
         if (!(m > hostP.newtonTol)) break;
       }
+      encContactTerms(s);
       encGripTerms(s, grips);
       encAssemble(s, it == 0 || !params.lag_coarse);
       runPCGEager(s);
@@ -460,6 +516,7 @@ struct btd_solver {
 
   // encodeNewtonIteration (solver.ts:687-696).
   void encNewton(cudaStream_t s, int it, bool grips) {
+    encContactTerms(s);
     encGripTerms(s, grips);
     encAssemble(s, it == 0 || !params.lag_coarse);
     encPCG(s);
@@ -643,7 +700,7 @@ int btd_default_params(btd_params* out) {
   p.pcg_iterations = 2;
   p.coarse_sweeps = 2;
   p.max_coarsest_nodes = 400;
-  p.self_contact = 0;
+  p.self_contact = 1;
   p.pcg_rel_tol = 0;
   p.line_search = 1;
   p.lag_coarse = 1;
@@ -670,6 +727,8 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
     if (prm->pcg_iterations < 1) throw std::invalid_argument("pcg_iterations must be >= 1");
     if (prm->coarse_sweeps < 1) throw std::invalid_argument("coarse_sweeps must be >= 1");
     if (!(prm->h > 0)) throw std::invalid_argument("h must be positive");
+    if (prm->self_contact && sc->node_count >= (1 << 20))
+      throw std::invalid_argument("self-contact bound keys hold at most 2^20 - 1 nodes");
     CK(cudaGetDevice(&s->device));
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&s->bodyStream, cudaStreamNonBlocking));
@@ -739,6 +798,13 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
     s->dx = s->alloc<float4>(N);
     s->pred = s->alloc<float4>(N);
     s->ext = s->alloc<float4>(3 * (size_t)N);
+    if (prm->self_contact) {
+      s->ctCells = s->alloc<unsigned>(2 * ((size_t)1 << CT_TABLE_BITS));
+      s->ctItems = s->alloc<float4>(4 * (size_t)N);
+      s->ctPairs = s->alloc<unsigned>((CT_K + 2) * (size_t)N);
+      s->cmeta = s->alloc<float4>(2 * (size_t)N);
+      s->ctAcc = s->alloc<int>(CT_ACC * (size_t)N);
+    }
     s->dGripSlots = s->alloc<GripSlot>(GRIPS);
     s->dGripEntries = s->alloc<GripEntry>((size_t)GRIPS * GRIP_ENTRIES);
     s->dGripGoal = s->alloc<float4>(3 * GRIPS);
@@ -1392,10 +1458,12 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
     // held grips add their lead once per substep and their terms once per Newton iteration; the
     // assembly and every Galerkin product are followed by their level's line factorisation
     const int64_t grips = s->gripsOn() ? 1 : 0;
-    const int64_t perNewton = 2 + (1 + V + 5) + 1 + 1 + grips;
+    // self-contact adds detection (6 kernels) once per substep and terms + gather per Newton iteration
+    const int64_t contact = s->contactOn() ? 1 : 0;
+    const int64_t perNewton = 2 + (1 + V + 5) + 1 + 1 + grips + 2 * contact;
     const int64_t hierarchy = 3 * (L - 1);
     const int64_t hierPerSubstep = s->params.lag_coarse ? hierarchy : hierarchy * (newton / std::max(1, substeps));
-    const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips;
+    const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips + 6 * contact;
     // each optional (gated) Newton iteration slot adds its gate kernel, run or not
     const int64_t gates = s->gatedBound(0, 0) - s->unconditional(0);
     *out = (int64_t)substeps * (perSubstep + hierPerSubstep + gates) + (int64_t)newton * perNewton + (int64_t)(pcg - newton) * (V + 5);

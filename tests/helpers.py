@@ -16,6 +16,13 @@ def correctness_coupon(nu=48, nv=40, **kw):
     return btd.layer_spec(DENIM, (nu - 1) * 3 * DENIM.pitch_u, (nv - 1) * 2 * DENIM.pitch_v, **args)
 
 
+def reference_params(**kw):
+    """PARAMS of the reference's GPU parity suite: GPU_DEFAULTS without self-contact, which its f64
+    CPU solver lacks (correctness.ts:24)."""
+    kw.setdefault("self_contact", 0)
+    return btd.default_params(**kw)
+
+
 # The reference schedule matching GPU_DEFAULTS (correctness.ts:20-24).
 MG = dict(max_coarsest_nodes=400, coarse_sweeps=2, line_colors=3, lag_coarse=True, line_search=True)
 

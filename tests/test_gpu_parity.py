@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import btd_b200 as btd
-from helpers import MG, copy_state, correctness_coupon, kink_rows, max_abs_rel_to_scale
+from helpers import MG, copy_state, correctness_coupon, kink_rows, max_abs_rel_to_scale, reference_params
 from oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -22,7 +22,7 @@ def staged():
     cpu = Oracle(sc, h=1 / 120, newton_iterations=2, pcg_iterations=2, **MG)
     for _ in range(12):
         cpu.substep()
-    gpu = btd.GpuSolver(sc, btd.default_params())
+    gpu = btd.GpuSolver(sc, reference_params())
     copy_state(cpu, gpu)
     cpu.predict()
     gpu.encode_predict()
@@ -162,7 +162,7 @@ def test_dynamics_production_schedule():
     cpu = Oracle(sc, h=1 / 120, newton_iterations=2, pcg_iterations=2, **MG)
     for _ in range(12):
         cpu.substep()
-    gpu = btd.GpuSolver(sc, btd.default_params())
+    gpu = btd.GpuSolver(sc, reference_params())
     err, moved = dynamics(cpu, gpu, 60)
     assert err < 0.25 * moved, (err, moved)
 
@@ -173,7 +173,7 @@ def test_dynamics_converged_schedule():
     cpu = Oracle(sc, h=1 / 120, newton_iterations=5, pcg_iterations=3, **MG)
     for _ in range(12):
         cpu.substep()
-    gpu = btd.GpuSolver(sc, btd.default_params(newton_iterations=5, newton_max=5, pcg_iterations=3))
+    gpu = btd.GpuSolver(sc, reference_params(newton_iterations=5, newton_max=5, pcg_iterations=3))
     err, moved = dynamics(cpu, gpu, 60)
     assert err < 0.03 * moved, (err, moved)
 

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import btd_b200 as btd
-from helpers import MG, copy_state, correctness_coupon, kink_rows, max_abs_rel_to_scale
+from helpers import MG, copy_state, correctness_coupon, kink_rows, max_abs_rel_to_scale, reference_params
 from oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -23,7 +23,7 @@ def torn_pair():
     """torn (correctness.ts:278-316): a flap and a slit cut into the coupon, 12 reference substeps,
     then material moved along yarn lines (each line keeps its length) and bundles cut in alternate
     spans, so bending weights and bundle continuity leave their defaults."""
-    P = btd.default_params()
+    P = reference_params()
     sc = btd.compile_scene(correctness_coupon())
     cpu = Oracle(sc, h=P.h, gravity=tuple(P.gravity), newton_iterations=P.newton_iterations,
                  pcg_iterations=P.pcg_iterations, **MG)
@@ -110,7 +110,7 @@ def test_damage_field_on_stretched_worn_coupon():
     smoothly (strongest in the middle), then damage update, pull-out and span coupling three times at
     fixed positions. Cut (255) and pulled-out (254) codes agree but for max(2, 1 %); partial damage
     codes within 3."""
-    P = btd.default_params()
+    P = reference_params()
     wear = dict(center=(0, 0), axis=(1, 0), radii=(1, 1), amount=1, cell_size=0, feature_scale=0.01,
                 defect_threshold=2, defect_density=0, sparse_from=2)
     sc = btd.compile_scene(correctness_coupon(wear=wear, wear_strength_loss=(0.9, 0.95), compress_u=0, compress_v=0,
@@ -145,7 +145,7 @@ def test_damage_field_on_stretched_worn_coupon():
 def test_long_lines(nu, nv):
     """longLines (correctness.ts:437-471): fine operator < 2e-5, one smoothing sweep < 1e-3 and the
     PCG step < 2e-2 against the oracle on coupons with long yarn lines."""
-    P = btd.default_params()
+    P = reference_params()
     sc = btd.compile_scene(correctness_coupon(nu, nv))
     cpu = Oracle(sc, h=P.h, gravity=tuple(P.gravity), newton_iterations=1, pcg_iterations=P.pcg_iterations, **MG)
     gpu = btd.GpuSolver(sc, P)
