@@ -154,6 +154,67 @@ def break_events(field, seg_flags):
     return sep, spans
 
 
+# Contact: 256 x 256 over 0.6 m of the configuration-0 material, folded about 1-3 seeded lines and
+# dropped from 0.3 m onto the floor at z = 0, self-contact on (SELF_CONTACT), 200 steps.
+CONFIG2 = dict(n=256, size=0.6, folds=(1, 3), fold_gap=3e-3, drop=0.3, h=1 / 60, newton_iterations=4, pcg_rel_tol=1e-6,
+               steps=200, floor=0.0)
+
+
+def fold(points, normal, offset, gap):
+    """Fold a sheet about the line {p . normal = offset} of its plane: the part beyond the line turns
+    over, each point rolling on a circle about an axis along the line gap / 2 above the sheet's
+    highest point (radius = its depth below the axis), by the angle that keeps its arc length, so
+    every layer folds without stretch and lands mirrored on top, its layers gap or more apart."""
+    p = np.array(points, np.float64)
+    nrm = np.array([normal[0], normal[1], 0.0])
+    s = p @ nrm - offset
+    H = p[:, 2].max() + 0.5 * gap
+    over = s > 0
+    rho = H - p[over, 2]
+    theta = np.minimum(s[over] / rho, np.pi)
+    on_arc = s[over] < np.pi * rho
+    along = np.where(on_arc, rho * np.sin(theta), -(s[over] - np.pi * rho))
+    out = p.copy()
+    out[over] = p[over] + np.outer(along - s[over], nrm)
+    out[over, 2] = np.where(on_arc, H - rho * np.cos(theta), H + rho)
+    return out
+
+
+def config2(seed=29, n=None, size=None, folds=None, drop=None):
+    """Contact: a free sheet (no pins) of the configuration-0 material folded about k parallel lines
+    (k uniform in CONFIG2's range, direction seeded), then lifted to the drop height above the floor.
+    Each fold turns over a part of the sheet still single and uncreased - the first the far side of a
+    line 55-70 % across, later ones the near side of a line within the remaining single region - so
+    every fold is isometric (a fold across an earlier crease would have to shear its layers)."""
+    c = CONFIG2
+    n = n or c["n"]
+    size = size or c["size"]
+    pitch = size / (n - 1)
+    m = shell_material(pitch)
+    sc = compile_scene(layer_spec(m, (n - 0.5) * pitch, (n - 0.5) * pitch, collar_rows=0, seed=seed))
+    assert sc.nx == n and sc.ny == n, (sc.nx, sc.ny)
+    sc.pinned[:] = 0
+    r = splitmix64(seed, 16).astype(np.float64) / 2.0**64
+    k = folds if folds is not None else c["folds"][0] + int(r[0] * (c["folds"][1] - c["folds"][0] + 1))
+    ang = 2 * np.pi * r[1]
+    nrm = np.array([np.cos(ang), np.sin(ang)])
+    pos = sc.position.reshape(-1, 3).copy()
+    proj = pos[:, :2] @ nrm
+    a, b = proj.min(), proj.max()
+    o = a + (b - a) * (0.55 + 0.15 * r[2])
+    pos = fold(pos, nrm, o, c["fold_gap"])
+    lo, hi = a, o - (b - o)  # the single, uncreased region left
+    for q in range(1, k):
+        if hi - lo < 8 * c["fold_gap"] + 0.1 * (b - a):
+            break
+        o = lo + (hi - lo) * (0.35 + 0.3 * r[2 + q])
+        pos = fold(pos, -nrm, -o, c["fold_gap"])  # the near side, p . nrm < o
+        lo, hi = o, min(hi, o + (o - lo))
+    pos[:, 2] += (c["drop"] if drop is None else drop) - pos[:, 2].min() + c["floor"]
+    sc.position[:] = pos.reshape(-1)
+    return sc
+
+
 def solver_params(h, newton_iterations, pcg_rel_tol, pcg_cap=500, **kw):
     from .solver import default_params
 

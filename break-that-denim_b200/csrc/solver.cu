@@ -1541,6 +1541,9 @@ int btd_device_buffer(btd_solver* s, int32_t which, int32_t level, void** ptr, s
       p = s->x, b = sizeof(float4) * s->N;
     } else if (which == BTD_BUF_V) {
       p = s->v, b = sizeof(float4) * s->N;
+    } else if (which == BTD_BUF_CONTACT) {
+      if (!s->contactOn()) throw std::invalid_argument("self-contact is off: no contact bounds");
+      p = s->cmeta, b = sizeof(float4) * 2 * (size_t)s->N;
     } else if (which == BTD_BUF_OP || which == BTD_BUF_FIXED) {
       if (level < 0 || level >= (int)s->levels.size()) throw std::invalid_argument("level out of range");
       Level& L = s->levels[level];

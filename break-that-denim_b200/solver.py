@@ -267,7 +267,7 @@ class GpuSolver:
         return A.reshape(n, 25, 3, 3), fixed
 
     VEC = {"X": 0, "B": 1, "R": 2, "delta": 3, "dx": 4, "pred": 5}
-    BUF = {"op": 16, "fixed": 17, "x": 18, "v": 19}
+    BUF = {"op": 16, "fixed": 17, "x": 18, "v": 19, "contact": 20}
 
     def device_buffer(self, which, level=0):
         """(device pointer, bytes) of a solver buffer, for zero-copy consumers."""

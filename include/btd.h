@@ -248,6 +248,10 @@ int btd_read_delta_f64(btd_solver* s, double* out3);
 #define BTD_BUF_FIXED 17
 #define BTD_BUF_X 18
 #define BTD_BUF_V 19
+/* contact.meta (solver.ts:263): 2 float4 per node, the node's own bound (unit normal away from the
+ * face, largest approach along it) and the reciprocal bound of a face corner; w >= 1e8: none.
+ * Only with self_contact. */
+#define BTD_BUF_CONTACT 20
 int btd_device_buffer(btd_solver* s, int32_t which, int32_t level, void** ptr, size_t* bytes);
 /* Stage: y = A x and x . y with the fine operator of the last assembly (the PCG matvec, pcg.wgsl:268-287),
  * x and y 4 floats per node on the host. Uses the solver's own reduction scratch. */

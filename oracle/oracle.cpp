@@ -23,6 +23,7 @@ thread_local std::string g_err;
 constexpr double INF = std::numeric_limits<double>::infinity();
 
 double hyp3(double a, double b, double c) { return std::sqrt(a * a + b * b + c * c); }
+double sq3(double a, double b, double c) { return a * a + b * b + c * c; }
 
 // ---------------------------------------------------------------------------- axial.ts
 
@@ -428,6 +429,12 @@ struct Solver {
   std::vector<Grip> grips;
   std::vector<std::vector<std::pair<int, int>>> gripOf;  // per node: (grip, entry)
   FloorParams floor;
+  // self-contact (selfcontact.wgsl restated in FP64): K candidate faces per node, the bounds (8 per
+  // node: own normal + share, reciprocal direction + share; share >= 1e8: none), the terms of the
+  // current Newton iterate (3 gradient + 6 symmetric Hessian per node)
+  bool contactOn = false;
+  std::vector<int> ctCand;
+  std::vector<double> ctBound, extG, extH;
   bool historyEnabled = true;
   int brokenCount = 0, pulledOutCount = 0;
   std::vector<MGLevel> lagged;      // lagged coarse levels (newtonMultigrid.ts:579)
@@ -662,6 +669,376 @@ struct Solver {
     return std::max(dz, lowest - z0);
   }
 
+
+  // ---------------------------------------------------------------- self-contact (selfcontact.wgsl)
+  // SELF_CONTACT (selfcontact.ts:7-33) and the shader's constants (selfcontact.wgsl:21-31).
+  static constexpr double CT_CELL = 12e-3, CT_REACH = 3e-3, CT_DELTA = 1.0e-3, CT_K_PEN = 500, CT_MU = 0.45,
+                          CT_FRICTION_SPEED = 0.002, CT_BOUND_FRACTION = 0.45, CT_HARD_CORE = 0.3e-3, CT_RECIP_UNIT = 1e-5;
+  static constexpr int CT_KC = 4, CT_WINDOW = 3;
+  static constexpr unsigned CT_MASK = (1u << 17) - 1u;
+
+  void coordOf(int n, int* i, int* j, int* l) const {
+    *l = layerOf[n];
+    const Layer& L = layers[*l];
+    int k = n - L.nodeOffset;
+    *i = k % L.nx, *j = k / L.nx;
+  }
+  void curOf(int n, double* p) const {
+    for (int q = 0; q < 3; ++q) p[q] = x[3 * n + q] + dx[3 * n + q];
+  }
+  // faceValid (selfcontact.wgsl:78-88)
+  bool faceValid(int f) const {
+    int i, j, l;
+    coordOf(f, &i, &j, &l);
+    const Layer& L = layers[l];
+    if (i + 1 >= L.nx || j + 1 >= L.ny) return false;
+    int c00 = f, c10 = f + 1, c01 = f + L.nx;
+    return segActive(2 * c00) && segActive(2 * c00 + 1) && segActive(2 * c10 + 1) && segActive(2 * c01);
+  }
+  void faceCorners(int f, int* c) const {
+    int nx = layer(f).nx;
+    c[0] = f, c[1] = f + 1, c[2] = f + nx, c[3] = f + nx + 1;
+  }
+  static unsigned hashCell(long cx, long cy, long cz) {
+    unsigned h = (static_cast<unsigned>(cx) * 73856093u) ^ (static_cast<unsigned>(cy) * 19349663u) ^ (static_cast<unsigned>(cz) * 83492791u);
+    return h & CT_MASK;
+  }
+  static void cellOf(const double* p, long* c) {
+    for (int q = 0; q < 3; ++q) c[q] = static_cast<long>(std::floor(p[q] / CT_CELL));
+  }
+  // Closest point of triangle (a, b, c) to p (Ericson 5.1.5): weights w[3], squared distance.
+  static double closestTri(const double* p, const double* a, const double* b, const double* c, double* w) {
+    double ab[3], ac[3], ap[3], bp[3], cp[3];
+    for (int q = 0; q < 3; ++q) ab[q] = b[q] - a[q], ac[q] = c[q] - a[q], ap[q] = p[q] - a[q], bp[q] = p[q] - b[q], cp[q] = p[q] - c[q];
+    auto dot = [](const double* u, const double* v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
+    double d1 = dot(ab, ap), d2 = dot(ac, ap);
+    w[0] = 1, w[1] = 0, w[2] = 0;
+    if (!(d1 <= 0 && d2 <= 0)) {
+      double d3 = dot(ab, bp), d4 = dot(ac, bp), d5 = dot(ab, cp), d6 = dot(ac, cp);
+      double vc = d1 * d4 - d3 * d2, vb = d5 * d2 - d1 * d6, va = d3 * d6 - d5 * d4;
+      if (d3 >= 0 && d4 <= d3) {
+        w[0] = 0, w[1] = 1, w[2] = 0;
+      } else if (d6 >= 0 && d5 <= d6) {
+        w[0] = 0, w[1] = 0, w[2] = 1;
+      } else if (vc <= 0 && d1 >= 0 && d3 <= 0) {
+        double v = d1 / (d1 - d3);
+        w[0] = 1 - v, w[1] = v, w[2] = 0;
+      } else if (vb <= 0 && d2 >= 0 && d6 <= 0) {
+        double v = d2 / (d2 - d6);
+        w[0] = 1 - v, w[1] = 0, w[2] = v;
+      } else if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
+        double v = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        w[0] = 0, w[1] = 1 - v, w[2] = v;
+      } else {
+        double den = 1 / (va + vb + vc), wb = vb * den, wc = vc * den;
+        w[0] = 1 - wb - wc, w[1] = wb, w[2] = wc;
+      }
+    }
+    double e[3];
+    for (int q = 0; q < 3; ++q) e[q] = p[q] - (w[0] * a[q] + w[1] * b[q] + w[2] * c[q]);
+    return dot(e, e);
+  }
+  // faceHitP (selfcontact.wgsl:159-172): corner weights w4 (c00 c10 c01 c11), closest point q, distance.
+  static double faceHitP(const double* p, const double* p00, const double* p10, const double* p01, const double* p11, double* w4, double* q) {
+    double w1[3], w2[3];
+    double t1 = closestTri(p, p00, p10, p11, w1), t2 = closestTri(p, p00, p11, p01, w2);
+    double d;
+    if (t1 <= t2) {
+      w4[0] = w1[0], w4[1] = w1[1], w4[2] = 0, w4[3] = w1[2];
+      d = std::sqrt(t1);
+    } else {
+      w4[0] = w2[0], w4[1] = 0, w4[2] = w2[2], w4[3] = w2[1];
+      d = std::sqrt(t2);
+    }
+    for (int k = 0; k < 3; ++k) q[k] = w4[0] * p00[k] + w4[1] * p10[k] + w4[2] * p01[k] + w4[3] * p11[k];
+    return d;
+  }
+  double faceHit(const double* p, const int* c, bool start, double* w4, double* q) const {
+    double P[4][3];
+    for (int k = 0; k < 4; ++k)
+      for (int z = 0; z < 3; ++z) P[k][z] = x[3 * c[k] + z] + (start ? 0.0 : dx[3 * c[k] + z]);
+    return faceHitP(p, P[0], P[1], P[2], P[3], w4, q);
+  }
+  static double segDist(const double* q, const double* a, const double* b) {
+    double e[3], qa[3];
+    for (int k = 0; k < 3; ++k) e[k] = b[k] - a[k], qa[k] = q[k] - a[k];
+    double ee = std::max(e[0] * e[0] + e[1] * e[1] + e[2] * e[2], 1e-20);
+    double t = std::min(std::max((qa[0] * e[0] + qa[1] * e[1] + qa[2] * e[2]) / ee, 0.0), 1.0);
+    return hyp3(qa[0] - t * e[0], qa[1] - t * e[1], qa[2] - t * e[2]);
+  }
+  static void cross3(const double* u, const double* v, double* o) {
+    o[0] = u[1] * v[2] - u[2] * v[1], o[1] = u[2] * v[0] - u[0] * v[2], o[2] = u[0] * v[1] - u[1] * v[0];
+  }
+  // Segment (o, o + d) against triangle (a, b, c) (Moeller-Trumbore): parameter of the crossing or 2.
+  static double segTri(const double* o, const double* d, const double* a, const double* b, const double* c) {
+    double e1[3], e2[3], p[3], sv[3], qv[3];
+    for (int k = 0; k < 3; ++k) e1[k] = b[k] - a[k], e2[k] = c[k] - a[k], sv[k] = o[k] - a[k];
+    cross3(d, e2, p);
+    double det = e1[0] * p[0] + e1[1] * p[1] + e1[2] * p[2];
+    if (std::fabs(det) < 1e-18) return 2;
+    double inv = 1 / det;
+    double u = (sv[0] * p[0] + sv[1] * p[1] + sv[2] * p[2]) * inv;
+    if (u < 0 || u > 1) return 2;
+    cross3(sv, e1, qv);
+    double v = (d[0] * qv[0] + d[1] * qv[1] + d[2] * qv[2]) * inv;
+    if (v < 0 || u + v > 1) return 2;
+    double t = (e2[0] * qv[0] + e2[1] * qv[1] + e2[2] * qv[2]) * inv;
+    return t >= 0 && t <= 1 ? t : 2;
+  }
+  double pathCrossing(const double* o, const double* d, const int* c) const {
+    double A0[3], B0[3], E0[3], G0[3], A1[3], B1[3], E1[3], G1[3];
+    for (int z = 0; z < 3; ++z) {
+      A0[z] = x[3 * c[0] + z], B0[z] = x[3 * c[1] + z], E0[z] = x[3 * c[2] + z], G0[z] = x[3 * c[3] + z];
+      A1[z] = A0[z] + dx[3 * c[0] + z], B1[z] = B0[z] + dx[3 * c[1] + z], E1[z] = E0[z] + dx[3 * c[2] + z], G1[z] = G0[z] + dx[3 * c[3] + z];
+    }
+    double t = std::min(segTri(o, d, A0, B0, G0), segTri(o, d, A0, G0, E0));
+    return std::min(t, std::min(segTri(o, d, A1, B1, G1), segTri(o, d, A1, G1, E1)));
+  }
+  bool rowHolds(const Layer& L, int j, int i0, int i1) const {
+    for (int i = std::min(i0, i1); i < std::max(i0, i1); ++i)
+      if (!segActive(2 * (L.nodeOffset + j * L.nx + i))) return false;
+    return true;
+  }
+  bool columnHolds(const Layer& L, int i, int j0, int j1) const {
+    for (int j = std::min(j0, j1); j < std::max(j0, j1); ++j)
+      if (!segActive(2 * (L.nodeOffset + j * L.nx + i) + 1)) return false;
+    return true;
+  }
+  // latticeLinked (selfcontact.wgsl:290-296)
+  bool latticeLinked(const Layer& L, int ni, int nj, int fi, int fj) const {
+    int ci = std::min(std::max(ni, fi), fi + 1), cj = std::min(std::max(nj, fj), fj + 1);
+    if (rowHolds(L, nj, ni, ci) && columnHolds(L, ci, nj, cj)) return true;
+    return columnHolds(L, ni, nj, cj) && rowHolds(L, cj, ni, ci);
+  }
+
+  // faceCount / scan / faceFill, damageRow, detect, resolveBounds (selfcontact.wgsl:186-478), with
+  // the same hash and table, so that hash collisions bring the same extra faces.
+  void contactDetect() {
+    const size_t T = size_t(CT_MASK) + 1;
+    std::vector<std::vector<int>> cells(T);
+    struct Item { double m1[3], r, m0[3]; };
+    std::vector<Item> items(N);
+    for (int f = 0; f < N; ++f) {
+      if (!faceValid(f)) continue;
+      int c[4];
+      faceCorners(f, c);
+      double P0[4][3], P1[4][3];
+      Item& it = items[f];
+      for (int z = 0; z < 3; ++z) it.m0[z] = it.m1[z] = 0;
+      for (int k = 0; k < 4; ++k)
+        for (int z = 0; z < 3; ++z) {
+          P0[k][z] = x[3 * c[k] + z];
+          P1[k][z] = P0[k][z] + dx[3 * c[k] + z];
+          it.m0[z] += 0.25 * P0[k][z];
+          it.m1[z] += 0.25 * P1[k][z];
+        }
+      double r0 = 0, r1 = 0;
+      for (int k = 0; k < 4; ++k) {
+        r0 = std::max(r0, sq3(P0[k][0] - it.m0[0], P0[k][1] - it.m0[1], P0[k][2] - it.m0[2]));
+        r1 = std::max(r1, sq3(P1[k][0] - it.m1[0], P1[k][1] - it.m1[1], P1[k][2] - it.m1[2]));
+      }
+      it.r = std::sqrt(std::max(r0, r1));
+      long k1[3], k0[3];
+      cellOf(it.m1, k1);
+      cellOf(it.m0, k0);
+      unsigned h1 = hashCell(k1[0], k1[1], k1[2]);
+      cells[h1].push_back(f);
+      if (!(k0[0] == k1[0] && k0[1] == k1[1] && k0[2] == k1[2])) cells[hashCell(k0[0], k0[1], k0[2])].push_back(f);
+    }
+    std::vector<uint8_t> rowMark(N, 0);
+    for (int n = 0; n < N; ++n) {
+      int i, j, l;
+      coordOf(n, &i, &j, &l);
+      const Layer& L = layers[l];
+      for (int a = std::max(i - CT_WINDOW, 0); a <= std::min(i + CT_WINDOW, L.nx - 1); ++a) {
+        int m = L.nodeOffset + j * L.nx + a;
+        if ((segFlags[2 * m] & SEG_BROKEN) || (segFlags[2 * m + 1] & SEG_BROKEN)) rowMark[n] = 1;
+      }
+    }
+    ctCand.assign(CT_KC * size_t(N), -1);
+    ctBound.assign(8 * size_t(N), 0.0);
+    std::vector<unsigned long long> recipKey(N, 0);
+    for (int n = 0; n < N; ++n) {
+      ctBound[8 * n + 3] = 1e9;
+      ctBound[8 * n + 7] = 1e9;
+      if (pinned[n]) continue;
+      double p[3], p0[3], path[3];
+      curOf(n, p);
+      for (int z = 0; z < 3; ++z) p0[z] = x[3 * n + z], path[z] = p[z] - p0[z];
+      bool moving = sq3(path[0], path[1], path[2]) > CT_HARD_CORE * CT_HARD_CORE;
+      int best[CT_KC];
+      double bestD[CT_KC];
+      for (int k = 0; k < CT_KC; ++k) best[k] = -1, bestD[k] = 1e9;
+      double d0min = 1e9, n0[3] = {0, 0, 0};
+      int f0 = -1;
+      double tc = 2;
+      int fc = -1;
+      long lo[3], hi[3];
+      for (int z = 0; z < 3; ++z) {
+        lo[z] = static_cast<long>(std::floor(std::min(p[z], p0[z]) / CT_CELL - 0.5));
+        hi[z] = std::min(static_cast<long>(std::floor(std::max(p[z], p0[z]) / CT_CELL + 0.5)), lo[z] + 3);
+      }
+      int ni, nj, nl;
+      coordOf(n, &ni, &nj, &nl);
+      const Layer& NL = layers[nl];
+      bool damaged = false;
+      for (int b = std::max(nj - CT_WINDOW, 0); b <= std::min(nj + CT_WINDOW, NL.ny - 1); ++b)
+        if (rowMark[NL.nodeOffset + b * NL.nx + ni]) damaged = true;
+      // ties on a shared edge go to the lower face index (an unsigned comparison: -1 is none)
+      auto lowerIdx = [](int a, int b) { return static_cast<unsigned>(a) < static_cast<unsigned>(b); };
+      for (long cz = lo[2]; cz <= hi[2]; ++cz)
+        for (long cy = lo[1]; cy <= hi[1]; ++cy)
+          for (long cx = lo[0]; cx <= hi[0]; ++cx)
+            for (int f : cells[hashCell(cx, cy, cz)]) {
+              const Item& it = items[f];
+              bool nearNow = hyp3(p[0] - it.m1[0], p[1] - it.m1[1], p[2] - it.m1[2]) - it.r < CT_REACH;
+              bool nearStart = hyp3(p0[0] - it.m0[0], p0[1] - it.m0[1], p0[2] - it.m0[2]) - it.r < std::min(d0min, 0.5 * CT_CELL);
+              bool onPath = moving && std::min(segDist(it.m0, p0, p), segDist(it.m1, p0, p)) < it.r;
+              if (!nearNow && !nearStart && !onPath) continue;
+              int fi, fj, fl;
+              coordOf(f, &fi, &fj, &fl);
+              int di = fi - ni, dj = fj - nj;
+              if (fl == nl && di >= -3 && di <= 2 && dj >= -3 && dj <= 2 && (!damaged || latticeLinked(NL, ni, nj, ni + di, nj + dj)))
+                continue;
+              int cf[4];
+              faceCorners(f, cf);
+              double w4[4], q[3];
+              if (nearStart) {
+                double d = faceHit(p0, cf, true, w4, q);
+                if ((d < d0min || (d == d0min && lowerIdx(f, f0))) && d > 1e-9) {
+                  d0min = d;
+                  for (int z = 0; z < 3; ++z) n0[z] = (p0[z] - q[z]) / d;
+                  f0 = f;
+                }
+              }
+              if (onPath) {
+                double t = pathCrossing(p0, path, cf);
+                if (t < tc || (t == tc && t <= 1 && lowerIdx(f, fc))) tc = t, fc = f;
+              }
+              if (!nearNow) continue;
+              double d = faceHit(p, cf, false, w4, q);
+              if (d >= CT_REACH) continue;
+              int cand = f;
+              double cd = d;
+              for (int k = 0; k < CT_KC; ++k) {
+                if (cand == best[k]) break;
+                if (cd < bestD[k] || (cd == bestD[k] && lowerIdx(cand, best[k]))) {
+                  std::swap(best[k], cand);
+                  std::swap(bestD[k], cd);
+                }
+              }
+            }
+      for (int k = 0; k < CT_KC; ++k) ctCand[CT_KC * n + k] = best[k];
+      double nb[3] = {n0[0], n0[1], n0[2]}, db = d0min;
+      int fb = f0;
+      if (fc >= 0 && fc != f0) {
+        int c[4];
+        faceCorners(fc, c);
+        double e1[3], e2[3], nrm[3];
+        for (int z = 0; z < 3; ++z) e1[z] = x[3 * c[1] + z] - x[3 * c[0] + z], e2[z] = x[3 * c[2] + z] - x[3 * c[0] + z];
+        cross3(e1, e2, nrm);
+        double ln = hyp3(nrm[0], nrm[1], nrm[2]);
+        if (ln > 1e-12) {
+          for (int z = 0; z < 3; ++z) nrm[z] /= ln;
+          double side = (p0[0] - x[3 * c[0]]) * nrm[0] + (p0[1] - x[3 * c[0] + 1]) * nrm[1] + (p0[2] - x[3 * c[0] + 2]) * nrm[2];
+          for (int z = 0; z < 3; ++z) nb[z] = side >= 0 ? nrm[z] : -nrm[z];
+          db = std::fabs(side);
+          fb = fc;
+        }
+      }
+      if (fb < 0 || (fb == f0 && db >= 0.5 * CT_CELL)) continue;
+      double share = CT_BOUND_FRACTION * std::max(db - CT_HARD_CORE, 0.0);
+      for (int z = 0; z < 3; ++z) ctBound[8 * n + z] = nb[z];
+      ctBound[8 * n + 3] = share;
+      // reciprocal key: the tightest share quantised to 10 um wins (ties: the higher node)
+      unsigned long long qs = 4095u - std::min<unsigned long long>(4095u, static_cast<unsigned long long>(share / CT_RECIP_UNIT));
+      unsigned long long key = (qs << 20) | static_cast<unsigned long long>(n + 1);
+      int c[4];
+      faceCorners(fb, c);
+      for (int k = 0; k < 4; ++k) recipKey[c[k]] = std::max(recipKey[c[k]], key);
+    }
+    for (int n = 0; n < N; ++n) {
+      unsigned long long key = recipKey[n];
+      if (key == 0) continue;
+      int j = static_cast<int>(key & 0xFFFFFu) - 1;
+      double share = static_cast<double>(4095u - (key >> 20)) * CT_RECIP_UNIT;
+      for (int z = 0; z < 3; ++z) ctBound[8 * n + 4 + z] = -ctBound[8 * j + z];
+      ctBound[8 * n + 7] = share;
+    }
+  }
+
+  // terms (selfcontact.wgsl:493-545): penalty and friction at the current iterate into extG/extH
+  // (node stiffness doubled, each corner's 2 w H), and the trust region of the own bound.
+  void contactTerms() {
+    extG.assign(3 * size_t(N), 0.0);
+    extH.assign(6 * size_t(N), 0.0);
+    const double gmag = hyp3(prm.gravity[0], prm.gravity[1], prm.gravity[2]);
+    auto addTerm = [&](int m, const double* g, const double* H, double s) {
+      for (int z = 0; z < 3; ++z) extG[3 * m + z] += s * g[z];
+      for (int z = 0; z < 6; ++z) extH[6 * m + z] += H[z];
+    };
+    for (int n = 0; n < N; ++n) {
+      double p[3];
+      curOf(n, p);
+      const double* own = &ctBound[8 * n];
+      double reach = 1e9;
+      double sWeight = std::sqrt(mass[n] * gmag * CT_DELTA / CT_K_PEN);
+      for (int k = 0; k < CT_KC; ++k) {
+        int f = ctCand[CT_KC * n + k];
+        if (f < 0) continue;
+        int c[4];
+        faceCorners(f, c);
+        double w4[4], q[3];
+        double d = faceHit(p, c, false, w4, q);
+        if (d <= 1e-9) continue;
+        double nn[3] = {(p[0] - q[0]) / d, (p[1] - q[1]) / d, (p[2] - q[2]) / d};
+        double al = nn[0] * own[0] + nn[1] * own[1] + nn[2] * own[2];
+        if (al > 0.1) reach = std::min(reach, (d - CT_DELTA + std::max(sWeight, 2 * std::max(CT_DELTA - d, 0.0))) / al);
+        if (d >= CT_DELTA) continue;
+        double sd = CT_DELTA - d;
+        double lam = CT_K_PEN * sd * sd / CT_DELTA;
+        double rel[3];
+        for (int z = 0; z < 3; ++z)
+          rel[z] = dx[3 * n + z] - (w4[0] * dx[3 * c[0] + z] + w4[1] * dx[3 * c[1] + z] + w4[2] * dx[3 * c[2] + z] + w4[3] * dx[3 * c[3] + z]);
+        double rn = rel[0] * nn[0] + rel[1] * nn[1] + rel[2] * nn[2];
+        double ut[3] = {rel[0] - rn * nn[0], rel[1] - rn * nn[1], rel[2] - rn * nn[2]};
+        double kf = CT_MU * lam / std::max(hyp3(ut[0], ut[1], ut[2]), CT_FRICTION_SPEED * prm.h);
+        double g[3] = {-lam * nn[0] + kf * ut[0], -lam * nn[1] + kf * ut[1], -lam * nn[2] + kf * ut[2]};
+        double kn = 2 * CT_K_PEN * sd / CT_DELTA;
+        double H[6] = {kn * nn[0] * nn[0] + kf * (1 - nn[0] * nn[0]), (kn - kf) * nn[0] * nn[1], (kn - kf) * nn[0] * nn[2],
+                       kn * nn[1] * nn[1] + kf * (1 - nn[1] * nn[1]), (kn - kf) * nn[1] * nn[2], kn * nn[2] * nn[2] + kf * (1 - nn[2] * nn[2])};
+        double H2[6];
+        for (int z = 0; z < 6; ++z) H2[z] = 2 * H[z];
+        addTerm(n, g, H2, 1.0);
+        for (int k2 = 0; k2 < 4; ++k2) {
+          if (w4[k2] <= 0) continue;
+          double Hw[6];
+          for (int z = 0; z < 6; ++z) Hw[z] = 2 * w4[k2] * H[z];
+          addTerm(c[k2], g, Hw, -w4[k2]);
+        }
+      }
+      // (a node's terms read only its own bound, so it is tightened in place)
+      if (reach < 1e9 && (own[0] != 0 || own[1] != 0 || own[2] != 0)) {
+        double approach = -(dx[3 * n] * own[0] + dx[3 * n + 1] * own[1] + dx[3 * n + 2] * own[2]);
+        ctBound[8 * n + 3] = std::min(own[3], approach + reach);
+      }
+    }
+  }
+
+  // A half-space bound: the step may move against m by at most m[3] (step.wgsl:62-65).
+  static void boundStep(double* d, const double* m) {
+    double approach = -(d[0] * m[0] + d[1] * m[1] + d[2] * m[2]);
+    if (approach > m[3])
+      for (int z = 0; z < 3; ++z) d[z] += (approach - m[3]) * m[z];
+  }
+  // feasible (step.wgsl:67-75): own, reciprocal, own.
+  void feasible(int n, double* d) const {
+    if (!contactOn) return;
+    boundStep(d, &ctBound[8 * n]);
+    boundStep(d, &ctBound[8 * n + 4]);
+    boundStep(d, &ctBound[8 * n]);
+  }
+
   // nodeGradient (solver.ts(ref):387-422).
   void nodeGradient(int n, double* g) const {
     g[0] = g[1] = g[2] = 0;
@@ -670,6 +1047,8 @@ struct Solver {
     double w = mass[n] / (h * h);
     for (int q = 0; q < 3; ++q) g[q] += w * (dx[3 * n + q] - pred[3 * n + q]);
     gripTerm(n, g);
+    if (contactOn && !extG.empty())
+      for (int q = 0; q < 3; ++q) g[q] += extG[3 * n + q];
     double D[9], Dg[3];
     airDrag(n, D);
     dragMul(D, &dx[3 * n], Dg);
@@ -752,6 +1131,13 @@ struct Solver {
         double g[3] = {0, 0, 0};
         double kg = gripTerm(n, g);
         if (kg > 0) quad(dot(g, dn), kg * dot(dn, dn));
+        if (contactOn && !extG.empty()) {
+          const double* eg = &extG[3 * n];
+          const double* eh = &extH[6 * n];
+          double Hd[3] = {eh[0] * dn[0] + eh[1] * dn[1] + eh[2] * dn[2], eh[1] * dn[0] + eh[3] * dn[1] + eh[4] * dn[2],
+                          eh[2] * dn[0] + eh[4] * dn[1] + eh[5] * dn[2]};
+          if (eg[0] != 0 || eg[1] != 0 || eg[2] != 0 || eh[0] != 0 || eh[3] != 0 || eh[5] != 0) quad(dot(eg, dn), dot(dn, Hd));
+        }
         double Dd[9], t1[3], t2[3];
         airDrag(n, Dd);
         dragMul(Dd, d0, t1);
@@ -920,10 +1306,15 @@ struct Solver {
         pred[3 * n + q] = pinned[n] ? 0 : hv + h * h * prm.gravity[q];
         dx[3 * n + q] = hv;
       }
-    // projectStart (step.wgsl:90-95): the predicted start bounded against the floor
-    if (floor.on)
-      for (int n = 0; n < N; ++n)
-        if (!pinned[n]) dx[3 * n + 2] = floorBoundZ(n, 0.0, dx[3 * n + 2]);
+    // contact detection at the predicted iterate (SelfContact.encodeDetect, solver.ts:743)
+    if (contactOn) contactDetect();
+    // projectStart (step.wgsl:90-95): the predicted start made feasible and bounded against the floor
+    if (floor.on || contactOn)
+      for (int n = 0; n < N; ++n) {
+        if (pinned[n]) continue;
+        feasible(n, &dx[3 * n]);
+        dx[3 * n + 2] = floorBoundZ(n, 0.0, dx[3 * n + 2]);
+      }
   }
 
   // segTension (solver.ts(ref):647-652).
@@ -1303,19 +1694,38 @@ std::shared_ptr<StencilOperator> Solver::assembleFineOperator() const {
       scatterPair(A, p, q, H);
     }
   }
-  if (floor.on) {
+  // contact's diagonal blocks, the floor's, then the active bounds (contact and the floor's hard
+  // limit) where the forces still press on, at ACTIVE_BOUND times the block's trace
+  // (assemble.wgsl:142, 191-209, 304-322)
+  if (floor.on || contactOn) {
     for (int n = 0; n < N; ++n) {
       if (A.fixed[n]) continue;
       double g[3], Hf[3];
       nodeGradient(n, g);
-      double gg[3] = {0, 0, 0};
-      bool core;
-      if (!floorTerm(n, gg, Hf, &core)) continue;
       double* Dn = &A.A[(static_cast<size_t>(n) * STENCIL + CENTER) * 9];
-      Dn[0] += Hf[0];
-      Dn[4] += Hf[1];
-      Dn[8] += Hf[2];
-      if (core && g[2] > 0) Dn[8] += 100.0 * (Dn[0] + Dn[4] + Dn[8]);
+      if (contactOn && !extH.empty()) {
+        const double* eh = &extH[6 * n];
+        double B[9] = {eh[0], eh[1], eh[2], eh[1], eh[3], eh[4], eh[2], eh[4], eh[5]};
+        for (int z = 0; z < 9; ++z) Dn[z] += B[z];
+      }
+      double gg[3] = {0, 0, 0};
+      bool core = false;
+      if (floorTerm(n, gg, Hf, &core)) {
+        Dn[0] += Hf[0];
+        Dn[4] += Hf[1];
+        Dn[8] += Hf[2];
+      }
+      const double kAct = 100.0 * (Dn[0] + Dn[4] + Dn[8]);
+      if (contactOn && !ctBound.empty())
+        for (int b = 0; b < 2; ++b) {
+          const double* m = &ctBound[8 * n + 4 * b];
+          if (m[3] >= 1e8 || (m[0] == 0 && m[1] == 0 && m[2] == 0)) continue;
+          double app = -(dx[3 * n] * m[0] + dx[3 * n + 1] * m[1] + dx[3 * n + 2] * m[2]);
+          if (app >= m[3] - 1e-3 * std::fabs(m[3]) && g[0] * m[0] + g[1] * m[1] + g[2] * m[2] > 0)
+            for (int r = 0; r < 3; ++r)
+              for (int c = 0; c < 3; ++c) Dn[3 * r + c] += kAct * m[r] * m[c];
+        }
+      if (core && g[2] > 0) Dn[8] += kAct;
     }
   }
   return Ap;
@@ -1740,6 +2150,7 @@ double chooseStep(const double* e, const double* m) {
 
 // newtonStepPCG (newtonMultigrid.ts:610-645).
 double Solver::newtonStep(int* pcgDone, double* rel, double* alphaOut) {
+  if (contactOn) contactTerms();
   auto A = assembleFineOperator();
   std::vector<double> b(3 * static_cast<size_t>(N));
   rhs(b.data());
@@ -1762,12 +2173,14 @@ double Solver::newtonStep(int* pcgDone, double* rel, double* alphaOut) {
   }
   double m = 0;
   for (size_t q = 0; q < d.size(); ++q) d[q] *= alpha;
-  // newtonApply's floor bound (step.wgsl:97-112): the applied step is what is left of it
-  if (floor.on)
+  // newtonApply's contact and floor bounds (step.wgsl:97-112): the applied step is what is left of it
+  if (floor.on || contactOn)
     for (int n = 0; n < N; ++n) {
       if (pinned[n]) continue;
-      double old = dx[3 * n + 2];
-      d[3 * n + 2] = floorBoundZ(n, old, old + d[3 * n + 2]) - old;
+      double nd[3] = {dx[3 * n] + d[3 * n], dx[3 * n + 1] + d[3 * n + 1], dx[3 * n + 2] + d[3 * n + 2]};
+      feasible(n, nd);
+      nd[2] = floorBoundZ(n, dx[3 * n + 2], nd[2]);
+      for (int z = 0; z < 3; ++z) d[3 * n + z] = nd[z] - dx[3 * n + z];
     }
   for (size_t q = 0; q < d.size(); ++q) {
     dx[q] += d[q];
@@ -1799,6 +2212,7 @@ ora_solver* ora_create(const btd_scene* sc, const ora_params* p) {
     auto* o = new ora_solver();
     Solver& S = o->s;
     S.prm = *p;
+    S.contactOn = p->self_contact != 0;
     if (p->threads > 0) omp_set_num_threads(p->threads);
     int N = sc->node_count, C = sc->crossing_count;
     S.N = N;

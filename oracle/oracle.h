@@ -36,6 +36,7 @@ typedef struct ora_params {
   int32_t lag_coarse;
   int32_t line_search;
   int32_t threads;           /* OpenMP threads (0: all) */
+  int32_t self_contact;      /* node-face self-contact restated from selfcontact.wgsl (the f64 reference has none) */
 } ora_params;
 
 typedef struct ora_solver ora_solver;
