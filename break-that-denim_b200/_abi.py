@@ -160,6 +160,7 @@ SIGNATURES = {
     "btd_destroy": ([C.c_void_p], C.c_int),
     "btd_substep": ([C.c_void_p, C.c_int32, C.c_int32], C.c_int),
     "btd_substeps": ([C.c_void_p, C.c_int32], C.c_int),
+    "btd_batch_substeps": ([C.c_void_p, C.c_int32, C.c_int32], C.c_int),
     "btd_synchronize": ([C.c_void_p], C.c_int),
     "btd_set_state": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "btd_get_state": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),

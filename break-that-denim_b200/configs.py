@@ -215,6 +215,74 @@ def config2(seed=29, n=None, size=None, folds=None, drop=None):
     return sc
 
 
+# Batch: independent hanging patches, all seeded: side uniform in [16, 128] nodes at configuration
+# 0's pitch, stiffness factor uniform in (0.5, 2) on stretch, shear and bending, a central yarn region
+# of 0-30 % of the area whose crossings break at lognormal(ln 0.08, 0.25) strains, and one grip on a
+# 3 x 3 patch in the lower third pulled at 0.05-0.2 m/s in a random direction.
+CONFIG3 = dict(count=512, sides=(16, 128), pitch=0.3 / 63, stiffness=(0.5, 2.0), region=(0.0, 0.3), grip_speed=(0.05, 0.2),
+               grip_stiffness=50.0, grip_lead=0.006, h=1 / 60, newton_iterations=4, pcg_rel_tol=1e-6)
+
+
+def _scaled_patch(n, pitch, f, seed, cache):
+    """hanging_patch(n) with stretch, shear and bending scaled by f: the compiled scene of each size is
+    made once and copied, its layer's material scaled (the compile itself does not depend on them),
+    the jitter drawn with the patch's own seed."""
+    if n not in cache:
+        cache[n] = hanging_patch(n, (n - 1) * pitch, seed=1, jitter=0.0)
+    sc = cache[n].copy()
+    for mat in (sc.layers[0].material, sc.layers[0].weave):
+        for y in mat.yarns:
+            y.ea_low *= f
+            y.ea_high *= f
+            y.ea_compress *= f
+            y.bend_rigidity *= f
+        mat.shear_stiffness *= f
+    free = sc.pinned == 0
+    pos = sc.position.reshape(-1, 3)
+    pos[free] += 1e-4 * normal(seed, 3 * int(free.sum())).reshape(-1, 3)
+    sc.position[:] = pos.reshape(-1)
+    return sc
+
+
+def config3(seed=31, count=None, sides=None):
+    """The batch: a list of patches, each (scene, grip) with grip = dict(picked, nodes, weights,
+    velocity, stiffness, max_lead)."""
+    c = CONFIG3
+    count = count or c["count"]
+    lo, hi = sides or c["sides"]
+    r = splitmix64(seed, 8 * count).astype(np.float64) / 2.0**64
+    out = []
+    cache = {}
+    for b in range(count):
+        u = r[8 * b: 8 * b + 8]
+        n = lo + int(u[0] * (hi - lo + 1))
+        f = c["stiffness"][0] + (c["stiffness"][1] - c["stiffness"][0]) * u[1]
+        pitch = c["pitch"]
+        sc = _scaled_patch(n, pitch, f, seed * 1000 + b, cache)
+        # the yarn region: a central square of the given share of the cells
+        share = c["region"][0] + (c["region"][1] - c["region"][0]) * u[2]
+        side = int(round(np.sqrt(share) * (n - 1)))
+        ea = np.array([8e3 * f * pitch, 4e3 * f * pitch])
+        strength = np.repeat((10.0 * ea)[None, :], sc.C, axis=0).astype(np.float32)
+        if side > 0:
+            a0 = (n - side) // 2
+            ii, jj = np.meshgrid(np.arange(a0, a0 + side), np.arange(a0, a0 + side))
+            cross = (jj * n + ii).reshape(-1)
+            eps = np.exp(np.log(0.08) + 0.25 * normal(seed * 1000 + b, 2 * cross.size)).reshape(-1, 2)
+            strength[cross] = (eps * ea[None, :]).astype(np.float32)
+        sc.field_strength[:] = strength.reshape(-1)
+        gi = int(n // 4 + u[3] * (n // 2))
+        gj = int(1 + u[4] * max(1, n // 3 - 2))
+        gi, gj = min(max(gi, 1), n - 2), min(max(gj, 1), n - 2)
+        nodes = np.array([(gj + dj) * n + gi + di for dj in (-1, 0, 1) for di in (-1, 0, 1)], np.int32)
+        ang, el = 2 * np.pi * u[5], np.pi * (u[6] - 0.5)
+        speed = c["grip_speed"][0] + (c["grip_speed"][1] - c["grip_speed"][0]) * u[7]
+        vel = speed * np.array([np.cos(el) * np.cos(ang), np.cos(el) * np.sin(ang), np.sin(el)])
+        out.append((sc, dict(picked=int(gj * n + gi), nodes=nodes, weights=np.ones(9), velocity=vel,
+                             stiffness=c["grip_stiffness"] * f, max_lead=c["grip_lead"])))
+    return out
+
+
 def solver_params(h, newton_iterations, pcg_rel_tol, pcg_cap=500, **kw):
     from .solver import default_params
 

@@ -148,4 +148,8 @@ __global__ void k_grip_init(GripArgs a, int g) {
   e.offset = make_float4(o.x, o.y, o.z, 0.f);
 }
 
+// A grip slot's new value, carried as a launch argument (stream-ordered, no host buffer to keep
+// alive or stage).
+__global__ void k_grip_set_slot(GripSlot* slots, int g, GripSlot v) { slots[g] = v; }
+
 }  // namespace btd

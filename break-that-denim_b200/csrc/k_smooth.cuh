@@ -93,7 +93,7 @@ __host__ __device__ constexpr size_t smoothSmemBytes(int len, int T) {
 // Tile of a level whose lines reach len nodes: the whole line when it fits, else 256 or 128 nodes.
 template <class Rows>
 __host__ inline int smoothTile(int len) {
-  constexpr size_t cap = 227 * 1024;
+  constexpr size_t cap = 226 * 1024;  // the opt-in 227 KB less the kernel's static shared memory
   if (smoothSmemBytes<Rows>(len, len) <= cap) return len;
   if (len > 256 && smoothSmemBytes<Rows>(len, 256) <= cap) return 256;
   return 128;

@@ -426,7 +426,9 @@ struct btd_solver {
     const cudaGraphNode_t* deps = nullptr;
     size_t nDeps = 0;
     CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nDeps));
-    if (st != cudaStreamCaptureStatusActive) throw std::runtime_error("PCG must be encoded into a graph capture");
+    if (st != cudaStreamCaptureStatusActive)
+      throw std::runtime_error("PCG must be encoded into a graph capture (capture status " + std::to_string((int)st) + ", last error " +
+                               cudaGetErrorString(cudaPeekAtLastError()) + ")");
     cudaGraphConditionalHandle h;
     CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
     PcgArgs a = pcgArgs(h, 1);
@@ -896,7 +898,8 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
       L.pw = s->alloc<float4>(L.N);
       const size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine, L.tile) : smoothSmemBytes<CoarseRows>(L.maxLine, L.tile);
       const size_t fsmem = L.fine ? factorSmemBytes<FineRows>(L.maxLine) : factorSmemBytes<CoarseRows>(L.maxLine);
-      if (L.maxLine > SM_MAX_LINE || smem > 227 * 1024 || fsmem > 227 * 1024)
+      // (227 KB of opt-in shared memory a block, less the kernels' few bytes of static shared memory)
+      if (L.maxLine > SM_MAX_LINE || smem > 226 * 1024 || fsmem > 226 * 1024)
         throw std::invalid_argument("yarn lines of " + std::to_string(L.maxLine) + " nodes exceed the smoother's shared memory");
       if (L.fine)
         smemFine = std::max(smemFine, smem), fsmemFine = std::max(fsmemFine, fsmem);
@@ -904,18 +907,33 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
         smemCoarse = std::max(smemCoarse, smem), fsmemCoarse = std::max(fsmemCoarse, fsmem);
     }
 
-    // the smoother's dynamic shared memory: the largest line of each row layout
-    if (smemFine) {
-      CK(cudaFuncSetAttribute(k_smooth<FineRows, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemFine));
-      CK(cudaFuncSetAttribute(k_smooth<FineRows, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemFine));
+    // the smoother's dynamic shared memory: a kernel's limit is an attribute of the function, shared
+    // by every solver of the process, so it is raised once to what the device allows beside the
+    // kernel's static shared memory (a permission, not an allocation; each launch asks for what its
+    // level's lines need, checked against the same bound above)
+    {
+      static std::once_flag smemOnce;
+      static cudaError_t smemErr = cudaSuccess;
+      std::call_once(smemOnce, [] {
+        int dev = 0, optin = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        auto set = [&](const void* f) {
+          cudaFuncAttributes fa;
+          if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, f);
+          if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+        };
+        set((const void*)k_smooth<FineRows, 0>);
+        set((const void*)k_smooth<FineRows, 1>);
+        set((const void*)k_smooth<CoarseRows, 0>);
+        set((const void*)k_smooth<CoarseRows, 1>);
+        set((const void*)k_line_factor<FineRows>);
+        set((const void*)k_line_factor<CoarseRows>);
+        smemErr = e;
+      });
+      CK(smemErr);
+      (void)smemFine, (void)smemCoarse, (void)fsmemFine, (void)fsmemCoarse;
     }
-    if (smemCoarse) {
-      CK(cudaFuncSetAttribute(k_smooth<CoarseRows, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemCoarse));
-      CK(cudaFuncSetAttribute(k_smooth<CoarseRows, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemCoarse));
-    }
-    if (fsmemFine) CK(cudaFuncSetAttribute(k_line_factor<FineRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmemFine));
-    if (fsmemCoarse)
-      CK(cudaFuncSetAttribute(k_line_factor<CoarseRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmemCoarse));
 
     // ---- parameters
     SimParams& P = s->hostP;
@@ -977,6 +995,28 @@ int btd_substeps(btd_solver* s, int32_t count) {
       cudaGraphExec_t ex = s->substepGraph(s->unconditional(0), s->gatedBound(0, 0));
       for (int k = 0; k < count; ++k) CK(cudaGraphLaunch(ex, s->stream));
     }
+  });
+}
+
+int btd_batch_substeps(btd_solver* const* solvers, int32_t count, int32_t substeps) {
+  GUARD({
+    if (!solvers || count < 0 || substeps < 0) throw std::invalid_argument("bad batch");
+    std::vector<cudaGraphExec_t> graphs(count, nullptr);
+    for (int b = 0; b < count; ++b) {
+      btd_solver* s = solvers[b];
+      checkSolver(s);
+      if (s->useGraphs) graphs[b] = s->substepGraph(s->unconditional(0), s->gatedBound(0, 0));
+    }
+    // round robin: every patch's next substep is queued before any patch's one after, so all
+    // streams have work from the start
+    for (int k = 0; k < substeps; ++k)
+      for (int b = 0; b < count; ++b) {
+        btd_solver* s = solvers[b];
+        if (graphs[b])
+          CK(cudaGraphLaunch(graphs[b], s->stream));
+        else
+          s->runSubstepEager(s->unconditional(0), s->gatedBound(0, 0));
+      }
   });
 }
 
@@ -1274,7 +1314,8 @@ static void checkSlot(btd_solver* s, int32_t slot) {
 }
 
 static void pushGrip(btd_solver* s, int32_t slot) {
-  CK(cudaMemcpyAsync(s->dGripSlots + slot, &s->hostGrip[slot], sizeof(GripSlot), cudaMemcpyHostToDevice, s->stream));
+  k_grip_set_slot<<<1, 1, 0, s->stream>>>(s->dGripSlots, slot, s->hostGrip[slot]);
+  CK(cudaGetLastError());
 }
 
 // release (interaction.ts:302-313): the slot's count drops to zero; without contact the grips own

@@ -302,3 +302,9 @@ class GpuSolver:
         buf = np.zeros((n, 4), np.float32)
         buf[:, :3] = np.asarray(values).reshape(n, 3)
         check("btd_write_vector", self._h, self.VEC[which], level, buf.ctypes.data_as(C.c_void_p))
+
+
+def batch_substeps(solvers, substeps):
+    """btd_batch_substeps: `substeps` substeps of every solver, concurrently on their own streams."""
+    arr = (C.c_void_p * len(solvers))(*[s._h for s in solvers])
+    check("btd_batch_substeps", arr, len(solvers), substeps)

@@ -166,6 +166,12 @@ int btd_destroy(btd_solver* s);
 int btd_substep(btd_solver* s, int32_t min_iterations, int32_t max_iterations);
 /* The engine's per-frame loop of substeps (worker.ts:664-674), stream-ordered, one launch each. */
 int btd_substeps(btd_solver* s, int32_t count);
+/* A batch of independent solvers (one patch each; the batched configuration): `substeps` substeps
+ * of every solver, each on its own stream, queued round robin with no host synchronisation, so the
+ * patches run concurrently on the GPU. Each patch's results are those of btd_substeps on it alone.
+ * With more patches than CUDA_DEVICE_MAX_CONNECTIONS (8 unless the process sets it, at most 32)
+ * streams share hardware queues. Synchronise each solver (btd_synchronize) before reading it. */
+int btd_batch_substeps(btd_solver* const* solvers, int32_t count, int32_t substeps);
 /* Wait for all submitted work (the reference's onSubmittedWorkDone). */
 /* Wait for the solver's stream (onSubmittedWorkDone). Returns BTD_E_TIMEOUT, once, when a bounded
  * device-side wait (a staging copy's completion) ran out since the last call: the kernels never hang
