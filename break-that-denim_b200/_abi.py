@@ -144,6 +144,7 @@ class Params(C.Structure):
         ("pcg_rel_tol", C.c_double),
         ("line_search", C.c_int32),
         ("lag_coarse", C.c_int32),
+        ("overlap_launches", C.c_int32),
     ]
 
 

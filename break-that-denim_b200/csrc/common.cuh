@@ -140,6 +140,15 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
 __device__ __forceinline__ bool finite1(float v) { return (__float_as_uint(v) & 0x7f800000u) != 0x7f800000u; }
 __device__ __forceinline__ bool finite3(float3 v) { return finite1(v.x) && finite1(v.y) && finite1(v.z); }
 
+// Programmatic dependent launch. A kernel launched with programmatic stream serialisation may start
+// while the kernel before it on the stream still runs; pdlWait() returns once that kernel has
+// completed and its writes are visible (at once for a kernel launched without the attribute), and
+// pdlLaunchNext() lets the next kernel start. Every kernel of the PCG loop calls them in that order,
+// first, so what a kernel may read before its own wait is what kernels two or more launches back
+// wrote (the smoother's line factors), never its predecessor's output.
+__device__ __forceinline__ void pdlWait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdlLaunchNext() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 // ---------------------------------------------------------------------------------------------- M3
 
 // General 3x3 (row-major) for the line solves.

@@ -180,11 +180,12 @@ __global__ void __launch_bounds__(RAP_THREADS) k_rap(DLevel F, DLevel C) {
   C.fixed[I] = fixedRow ? 1u : 0u;
 }
 
-// r = b - A x on level F (residual, multigrid.wgsl:182-199); fixed rows give 0. Loads are issued
-// unconditionally (neighbour index clamped, outside couplings zero) so they overlap: the fine row
-// in one round trip, the coarse row one stencil row of 5 blocks at a time.
-template <class Rows>
-__global__ void k_residual(DLevel F) {
+// r = b - A x on the fine level (residual, multigrid.wgsl:182-199); fixed rows give 0. Loads are
+// issued unconditionally (neighbour index clamped, outside couplings zero) so they overlap: the
+// whole row in one round trip.
+__global__ void k_residual_fine(DLevel F) {
+  pdlWait();
+  pdlLaunchNext();
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= F.N) return;
   if (F.fixed[n]) {
@@ -195,72 +196,106 @@ __global__ void k_residual(DLevel F) {
   nodeCoord(F, n, &i, &j, &l);
   const DLevelLayer L = F.layers[l];
   float3 r = f3(F.B[n]);
-  if constexpr (Rows::NC == 12) {
-    float4 pl[FINE_PLANES];
+  float4 pl[FINE_PLANES];
 #pragma unroll
-    for (int p = 0; p < FINE_PLANES; ++p) pl[p] = __ldg(&F.op[(size_t)p * F.N + n]);
-    float3 xm[12];
-    bool ok[12];
+  for (int p = 0; p < FINE_PLANES; ++p) pl[p] = __ldg(&F.op[(size_t)p * F.N + n]);
+  float3 xm[12];
+  bool ok[12];
 #pragma unroll
-    for (int q = 0; q < 12; ++q) {
-      const int2 o = fineOffset(q);
-      const int ii = i + o.x, jj = j + o.y;
-      ok[q] = ii >= 0 && jj >= 0 && ii < L.nx && jj < L.ny;
-      xm[q] = f3(F.X[ok[q] ? L.offset + jj * L.nx + ii : n]);
-    }
-    const float3 xn = f3(F.X[n]);
-    const float* row = reinterpret_cast<const float*>(pl);
-    r -= Sym{row[0], row[1], row[2], row[3], row[4], row[5]} * xn;
+  for (int q = 0; q < 12; ++q) {
+    const int2 o = fineOffset(q);
+    const int ii = i + o.x, jj = j + o.y;
+    ok[q] = ii >= 0 && jj >= 0 && ii < L.nx && jj < L.ny;
+    xm[q] = f3(F.X[ok[q] ? L.offset + jj * L.nx + ii : n]);
+  }
+  const float3 xn = f3(F.X[n]);
+  const float* row = reinterpret_cast<const float*>(pl);
+  r -= Sym{row[0], row[1], row[2], row[3], row[4], row[5]} * xn;
 #pragma unroll
-    for (int q = 0; q < 12; ++q) {
-      if (!ok[q]) continue;
-      if (q < 8) {
-        const float* b = row + 6 * q + 6;
-        r -= Sym{b[0], b[1], b[2], b[3], b[4], b[5]} * xm[q];
-      } else {
-        r -= row[54 + q - 8] * xm[q];
-      }
-    }
-  } else {
-#pragma unroll
-    for (int dj = -2; dj <= 2; ++dj) {
-      const int f0 = 30 * (dj + 2), p0 = f0 >> 2, sh = f0 & 3;
-      float4 pl[9];
-#pragma unroll
-      for (int p = 0; p < 9; ++p) pl[p] = p0 + p < COARSE_PLANES ? __ldg(&F.op[(size_t)(p0 + p) * F.N + n]) : make_float4(0, 0, 0, 0);
-      float3 xm[5];
-      bool ok[5];
-#pragma unroll
-      for (int di = -2; di <= 2; ++di) {
-        const int ii = i + di, jj = j + dj;
-        ok[di + 2] = ii >= 0 && jj >= 0 && ii < L.nx && jj < L.ny;
-        xm[di + 2] = f3(F.X[ok[di + 2] ? L.offset + jj * L.nx + ii : n]);
-      }
-      const float* row = reinterpret_cast<const float*>(pl) + sh;
-#pragma unroll
-      for (int di = -2; di <= 2; ++di) {
-        if (!ok[di + 2]) continue;
-        const float* b = row + 6 * (di + 2);
-        r -= Sym{b[0], b[1], b[2], b[3], b[4], b[5]} * xm[di + 2];
-      }
+  for (int q = 0; q < 12; ++q) {
+    if (!ok[q]) continue;
+    if (q < 8) {
+      const float* b = row + 6 * q + 6;
+      r -= Sym{b[0], b[1], b[2], b[3], b[4], b[5]} * xm[q];
+    } else {
+      r -= row[54 + q - 8] * xm[q];
     }
   }
   F.R[n] = make_float4(r.x, r.y, r.z, 0.f);
 }
 
-// b_c = P^T r_f and x_c = 0 (restrictResidual, multigrid.wgsl:204-232): the up to 3 x 3 fine nodes of
-// coarse node I, all loads issued together.
-__global__ void k_restrict(DLevel F, DLevel C) {
-  int I = blockIdx.x * blockDim.x + threadIdx.x;
-  if (I >= C.N) return;
+// Row dj = R - 2 of the coarse stencil at node n = (i, j): sum over di of A(n, di, dj) x (di = -2..2).
+template <int R>
+__device__ __forceinline__ float3 coarseRowSum(const DLevel& F, const DLevelLayer& L, int n, int i, int j) {
+  constexpr int f0 = 30 * R, p0 = f0 >> 2, sh = f0 & 3, dj = R - 2;
+  float4 pl[9];
+#pragma unroll
+  for (int p = 0; p < 9; ++p) pl[p] = p0 + p < COARSE_PLANES ? __ldg(&F.op[(size_t)(p0 + p) * F.N + n]) : make_float4(0, 0, 0, 0);
+  float3 xm[5];
+  bool ok[5];
+#pragma unroll
+  for (int di = -2; di <= 2; ++di) {
+    const int ii = i + di, jj = j + dj;
+    ok[di + 2] = ii >= 0 && jj >= 0 && ii < L.nx && jj < L.ny;
+    xm[di + 2] = f3(F.X[ok[di + 2] ? L.offset + jj * L.nx + ii : n]);
+  }
+  const float* row = reinterpret_cast<const float*>(pl) + sh;
+  float3 s = make_float3(0, 0, 0);
+#pragma unroll
+  for (int di = -2; di <= 2; ++di) {
+    if (!ok[di + 2]) continue;
+    const float* bk = row + 6 * (di + 2);
+    s += Sym{bk[0], bk[1], bk[2], bk[3], bk[4], bk[5]} * xm[di + 2];
+  }
+  return s;
+}
+
+// The same on a coarse level, eight lanes a node: lane dj + 2 (dj = -2..2) sums stencil row dj
+// (5 blocks: 9 row planes and 5 unknowns, one round trip), lanes 5-7 hold zero, the group adds its
+// partial sums by shuffles in a fixed order and lane 0 writes b minus the sum (0 on a fixed row).
+// Every lane of the warp calls it (the shuffles); `valid` is false past the level's last node.
+__device__ __forceinline__ void coarseResidualLane(const DLevel& F, const DLevelLayer& L, int n, int i, int j, int lane8, bool valid) {
+  float3 s = make_float3(0, 0, 0);
+  float4 b = make_float4(0, 0, 0, 0);
+  uint32_t fx = 0u;
+  if (valid && lane8 == 0) b = F.B[n], fx = F.fixed[n];
+  if (valid) switch (lane8) {
+      case 0: s = coarseRowSum<0>(F, L, n, i, j); break;
+      case 1: s = coarseRowSum<1>(F, L, n, i, j); break;
+      case 2: s = coarseRowSum<2>(F, L, n, i, j); break;
+      case 3: s = coarseRowSum<3>(F, L, n, i, j); break;
+      case 4: s = coarseRowSum<4>(F, L, n, i, j); break;
+      default: break;
+    }
+#pragma unroll
+  for (int m = 4; m >= 1; m >>= 1) {
+    s.x += __shfl_xor_sync(0xffffffffu, s.x, m);
+    s.y += __shfl_xor_sync(0xffffffffu, s.y, m);
+    s.z += __shfl_xor_sync(0xffffffffu, s.z, m);
+  }
+  if (valid && lane8 == 0) F.R[n] = fx ? make_float4(0, 0, 0, 0) : make_float4(b.x - s.x, b.y - s.y, b.z - s.z, 0.f);
+}
+
+// Eight threads a node (blockDim a multiple of 32).
+__global__ void k_residual_coarse(DLevel F) {
+  pdlWait();
+  pdlLaunchNext();
+  const int it = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = it < 8 * F.N;
+  const int n = valid ? it >> 3 : 0;
+  int i = 0, j = 0, l = 0;
+  if (valid) nodeCoord(F, n, &i, &j, &l);
+  coarseResidualLane(F, F.layers[valid ? l : 0], n, i, j, it & 7, valid);
+}
+
+// b_c = P^T r_f and x_c = 0 (restrictResidual, multigrid.wgsl:204-232) for coarse node I at (ci, cj)
+// of its layer, whose fine layer is Lf: the up to 3 x 3 fine nodes, all loads issued together.
+__device__ __forceinline__ void restrictAt(const DLevel& F, const DLevel& C, const DLevelLayer& Lf, int I, int ci, int cj) {
   C.X[I] = make_float4(0, 0, 0, 0);
   if (C.fixed[I]) {
     C.B[I] = make_float4(0, 0, 0, 0);
     return;
   }
-  int ci, cj, l;
-  nodeCoord(C, I, &ci, &cj, &l);
-  const DLevelLayer Lf = F.layers[l];
   const int fi0 = coarseToFine(ci, Lf.nx), fj0 = coarseToFine(cj, Lf.ny);
   float4 w4[9], r4[9];
   uint32_t fx[9];
@@ -285,14 +320,19 @@ __global__ void k_restrict(DLevel F, DLevel C) {
   C.B[I] = make_float4(s.x, s.y, s.z, 0.f);
 }
 
-// x_f += P x_c (prolongAdd, multigrid.wgsl:237-258).
-__global__ void k_prolong(DLevel F, DLevel C) {
-  int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= F.N || F.fixed[a]) return;
-  int i, j, l;
-  nodeCoord(F, a, &i, &j, &l);
-  const DLevelLayer Lf = F.layers[l];
-  const DLevelLayer Lc = C.layers[l];
+__global__ void k_restrict(DLevel F, DLevel C) {
+  pdlWait();
+  pdlLaunchNext();
+  int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= C.N) return;
+  int ci, cj, l;
+  nodeCoord(C, I, &ci, &cj, &l);
+  restrictAt(F, C, F.layers[l], I, ci, cj);
+}
+
+// x_f += P x_c (prolongAdd, multigrid.wgsl:237-258) at fine node a = (i, j) of layers Lf / Lc.
+__device__ __forceinline__ void prolongAt(const DLevel& F, const DLevel& C, const DLevelLayer& Lf, const DLevelLayer& Lc, int a, int i, int j) {
+  if (F.fixed[a]) return;
   const Bracket bi = bracketOf(i, Lf.nx), bj = bracketOf(j, Lf.ny);
   const float4 w = F.pw[a];
   const float4 x = F.X[a];
@@ -306,6 +346,16 @@ __global__ void k_prolong(DLevel F, DLevel C) {
     if (wk != 0.f) s += wk * xc[q];
   }
   F.X[a] = make_float4(x.x + s.x, x.y + s.y, x.z + s.z, 0.f);
+}
+
+__global__ void k_prolong(DLevel F, DLevel C) {
+  pdlWait();
+  pdlLaunchNext();
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= F.N) return;
+  int i, j, l;
+  nodeCoord(F, a, &i, &j, &l);
+  prolongAt(F, C, F.layers[l], C.layers[l], a, i, j);
 }
 
 }  // namespace btd

@@ -93,6 +93,8 @@ __device__ __forceinline__ double safeDiv(double a, double b) {
 
 // delta = 0, z = 0; r0 = ||r|| (r = b: the solve starts from zero).
 __global__ void __launch_bounds__(RED_THREADS) k_pcg_init(PcgArgs a) {
+  pdlWait();
+  pdlLaunchNext();
   double v[1] = {0.0};
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < a.F.N; n += gridDim.x * blockDim.x) {
     a.delta[n] = make_float4(0, 0, 0, 0);
@@ -117,6 +119,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_init(PcgArgs a) {
 
 // rz' = r . z; first: rz = rz', beta unused; else beta = rz' / rz, rz = rz'.
 __global__ void __launch_bounds__(RED_THREADS) k_pcg_dot_rz(PcgArgs a, int first) {
+  pdlWait();
+  pdlLaunchNext();
   double v[1] = {0.0};
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < a.F.N; n += gridDim.x * blockDim.x) {
     float3 r = f3(a.F.B[n]), z = f3(a.F.X[n]);
@@ -138,6 +142,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_dot_rz(PcgArgs a, int first
 
 // p = z + beta p (first: p = z).
 __global__ void k_pcg_update_p(PcgArgs a, int first) {
+  pdlWait();
+  pdlLaunchNext();
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= a.F.N) return;
   float3 z = f3(a.F.X[n]);
@@ -159,6 +165,8 @@ __device__ __forceinline__ void symVecAddD(const Sym& A, const double* x, double
 
 // Ap = A p (fixed rows 0), p . Ap; alpha = rz / pAp (0 and stop when pAp <= 0, as pcg() breaks).
 __global__ void __launch_bounds__(RED_THREADS) k_pcg_matvec(PcgArgs a) {
+  pdlWait();
+  pdlLaunchNext();
   double v[1] = {0.0};
   const DLevel& F = a.F;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < F.N; n += gridDim.x * blockDim.x) {
@@ -211,6 +219,8 @@ __device__ __forceinline__ void pcgStop(const PcgArgs& a, Scalars& s) {
 // iteration cap, a breakdown or a zero right-hand side stop the loop (the while condition); the
 // recurrence residual meeting the tolerance hands the decision to k_pcg_true_residual.
 __global__ void __launch_bounds__(RED_THREADS) k_pcg_update_xr(PcgArgs a) {
+  pdlWait();
+  pdlLaunchNext();
   double v[1] = {0.0};
   const double alphaD = a.scal->alpha;
   const float alpha = (float)alphaD;
@@ -247,6 +257,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_update_xr(PcgArgs a) {
 // afresh (keeping the old one stalls: measured ~10x more iterations), so the fp32 iterations solve
 // for a correction that accumulates into the FP64 iterate - iterative refinement.
 __global__ void __launch_bounds__(RED_THREADS) k_pcg_true_residual(PcgArgs a) {
+  pdlWait();
+  pdlLaunchNext();
   if (!a.scal->check) return;
   double v[1] = {0.0};
   const DLevel& F = a.F;

@@ -637,10 +637,17 @@ __global__ void __launch_bounds__(SM_SWEEP_THREADS) k_smooth(DLevel L, LineGeom 
   } else {
     a = lineAt(g, blockIdx.x);
   }
-  if (threadIdx.x == 0) mbarInit(&bar, 1);
+  // the line's factors and coupling copies (written by the factorisation, launches back) stream in
+  // while the kernel before this one may still run; its unknowns are read after the wait
+  if (threadIdx.x == 0) {
+    mbarInit(&bar, 1);
+    issueLineCopies<Rows>(a, fac, T, sm4, &bar);
+  }
+  pdlWait();
+  pdlLaunchNext();
   __syncthreads();
   unsigned phase = 0;
-  sweepLine<Rows, FAM>(L, a, fac, T, err, sm4, &bar, phase, false);
+  sweepLine<Rows, FAM>(L, a, fac, T, err, sm4, &bar, phase, true);
 }
 
 }  // namespace btd

@@ -366,6 +366,23 @@ struct btd_solver {
   }
 
   // One sweep of level k: the six colours, v-lines first (reversed for the post-smoother).
+  // A kernel of the PCG loop on `s`: with programmatic stream serialisation when the solver overlaps
+  // launches (each such kernel waits for its predecessor before reading its output; pdlWait).
+  template <typename... P, typename... A>
+  void launch(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &at;
+    cfg.numAttrs = params.overlap_launches ? 1 : 0;
+    CK(cudaLaunchKernelEx(&cfg, k, args...));
+  }
+
   void encSmooth(cudaStream_t s, int k, bool reverse) {
     Level& L = levels[k];
     const size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine, L.tile) : smoothSmemBytes<CoarseRows>(L.maxLine, L.tile);
@@ -377,14 +394,14 @@ struct btd_solver {
       const LineGeom& g = L.geom[c];
       if (L.fine) {
         if (c < 3)
-          k_smooth<FineRows, 1><<<count, L.threads, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+          launch(k_smooth<FineRows, 1>, count, L.threads, smem, s, d, g, (const int4*)L.dLines, (const int*)L.dFacBase, (const float4*)L.fac, L.tile, dCounters + CNT_ERROR);
         else
-          k_smooth<FineRows, 0><<<count, L.threads, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+          launch(k_smooth<FineRows, 0>, count, L.threads, smem, s, d, g, (const int4*)L.dLines, (const int*)L.dFacBase, (const float4*)L.fac, L.tile, dCounters + CNT_ERROR);
       } else {
         if (c < 3)
-          k_smooth<CoarseRows, 1><<<count, L.threads, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+          launch(k_smooth<CoarseRows, 1>, count, L.threads, smem, s, d, g, (const int4*)L.dLines, (const int*)L.dFacBase, (const float4*)L.fac, L.tile, dCounters + CNT_ERROR);
         else
-          k_smooth<CoarseRows, 0><<<count, L.threads, smem, s>>>(d, g, L.dLines, L.dFacBase, L.fac, L.tile, dCounters + CNT_ERROR);
+          launch(k_smooth<CoarseRows, 0>, count, L.threads, smem, s, d, g, (const int4*)L.dLines, (const int*)L.dFacBase, (const float4*)L.fac, L.tile, dCounters + CNT_ERROR);
       }
     }
   }
@@ -400,22 +417,22 @@ struct btd_solver {
     Level& Cl = levels[k + 1];
     encSmooth(s, k, false);
     if (F.fine)
-      k_residual<FineRows><<<blocksFor(F.N, 128), 128, 0, s>>>(F.dev());
+      launch(k_residual_fine, blocksFor(F.N, 128), 128, 0, s, F.dev());
     else
-      k_residual<CoarseRows><<<blocksFor(F.N, 128), 128, 0, s>>>(F.dev());
-    k_restrict<<<blocksFor(Cl.N, 128), 128, 0, s>>>(F.dev(), Cl.dev());
+      launch(k_residual_coarse, blocksFor(8 * F.N, 128), 128, 0, s, F.dev());
+    launch(k_restrict, blocksFor(Cl.N, 128), 128, 0, s, F.dev(), Cl.dev());
     encVCycle(s, k + 1);
-    k_prolong<<<blocksFor(F.N, 128), 128, 0, s>>>(F.dev(), Cl.dev());
+    launch(k_prolong, blocksFor(F.N, 128), 128, 0, s, F.dev(), Cl.dev());
     encSmooth(s, k, true);
   }
 
   void encPcgBody(cudaStream_t s, const PcgArgs& a) {
     encVCycle(s, 0);
-    k_pcg_dot_rz<<<redBlocks, RED_THREADS, 0, s>>>(a, 0);
-    k_pcg_update_p<<<blocksFor(N, 256), 256, 0, s>>>(a, 0);
-    k_pcg_matvec<<<redBlocks, RED_THREADS, 0, s>>>(a);
-    k_pcg_update_xr<<<redBlocks, RED_THREADS, 0, s>>>(a);
-    k_pcg_true_residual<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    launch(k_pcg_dot_rz, redBlocks, RED_THREADS, 0, s, a, 0);
+    launch(k_pcg_update_p, blocksFor(N, 256), 256, 0, s, a, 0);
+    launch(k_pcg_matvec, redBlocks, RED_THREADS, 0, s, a);
+    launch(k_pcg_update_xr, redBlocks, RED_THREADS, 0, s, a);
+    launch(k_pcg_true_residual, redBlocks, RED_THREADS, 0, s, a);
   }
 
   // encodePCG (solver.ts:625-644) with the device-side stop: prologue, then a while-node whose
@@ -434,11 +451,11 @@ struct btd_solver {
     PcgArgs a = pcgArgs(h, 1);
     k_pcg_init<<<redBlocks, RED_THREADS, 0, s>>>(a);
     encVCycle(s, 0);
-    k_pcg_dot_rz<<<redBlocks, RED_THREADS, 0, s>>>(a, 1);
-    k_pcg_update_p<<<blocksFor(N, 256), 256, 0, s>>>(a, 1);
-    k_pcg_matvec<<<redBlocks, RED_THREADS, 0, s>>>(a);
-    k_pcg_update_xr<<<redBlocks, RED_THREADS, 0, s>>>(a);
-    k_pcg_true_residual<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    launch(k_pcg_dot_rz, redBlocks, RED_THREADS, 0, s, a, 1);
+    launch(k_pcg_update_p, blocksFor(N, 256), 256, 0, s, a, 1);
+    launch(k_pcg_matvec, redBlocks, RED_THREADS, 0, s, a);
+    launch(k_pcg_update_xr, redBlocks, RED_THREADS, 0, s, a);
+    launch(k_pcg_true_residual, redBlocks, RED_THREADS, 0, s, a);
     CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nDeps));
     cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
     cp.conditional.handle = h;
@@ -459,11 +476,11 @@ struct btd_solver {
     PcgArgs a = pcgArgs(0, 0);
     k_pcg_init<<<redBlocks, RED_THREADS, 0, s>>>(a);
     encVCycle(s, 0);
-    k_pcg_dot_rz<<<redBlocks, RED_THREADS, 0, s>>>(a, 1);
-    k_pcg_update_p<<<blocksFor(N, 256), 256, 0, s>>>(a, 1);
-    k_pcg_matvec<<<redBlocks, RED_THREADS, 0, s>>>(a);
-    k_pcg_update_xr<<<redBlocks, RED_THREADS, 0, s>>>(a);
-    k_pcg_true_residual<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    launch(k_pcg_dot_rz, redBlocks, RED_THREADS, 0, s, a, 1);
+    launch(k_pcg_update_p, blocksFor(N, 256), 256, 0, s, a, 1);
+    launch(k_pcg_matvec, redBlocks, RED_THREADS, 0, s, a);
+    launch(k_pcg_update_xr, redBlocks, RED_THREADS, 0, s, a);
+    launch(k_pcg_true_residual, redBlocks, RED_THREADS, 0, s, a);
     for (;;) {
       int conv = 0;
       CK(cudaMemcpyAsync(&conv, &dScal->converged, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -706,6 +723,7 @@ int btd_default_params(btd_params* out) {
   p.pcg_rel_tol = 0;
   p.line_search = 1;
   p.lag_coarse = 1;
+  p.overlap_launches = 1;
   *out = p;
   return BTD_OK;
 }
@@ -871,7 +889,6 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
       }
       cur = nxt;
     }
-    size_t smemFine = 0, smemCoarse = 0, fsmemFine = 0, fsmemCoarse = 0;
     for (size_t k = 0; k < s->levels.size(); ++k) {
       Level& L = s->levels[k];
       L.dLayers = s->alloc<DLevelLayer>(L.layers.size());
@@ -901,10 +918,6 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
       // (227 KB of opt-in shared memory a block, less the kernels' few bytes of static shared memory)
       if (L.maxLine > SM_MAX_LINE || smem > 226 * 1024 || fsmem > 226 * 1024)
         throw std::invalid_argument("yarn lines of " + std::to_string(L.maxLine) + " nodes exceed the smoother's shared memory");
-      if (L.fine)
-        smemFine = std::max(smemFine, smem), fsmemFine = std::max(fsmemFine, fsmem);
-      else
-        smemCoarse = std::max(smemCoarse, smem), fsmemCoarse = std::max(fsmemCoarse, fsmem);
     }
 
     // the smoother's dynamic shared memory: a kernel's limit is an attribute of the function, shared
@@ -932,7 +945,6 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
         smemErr = e;
       });
       CK(smemErr);
-      (void)smemFine, (void)smemCoarse, (void)fsmemFine, (void)fsmemCoarse;
     }
 
     // ---- parameters

@@ -144,6 +144,9 @@ typedef struct btd_params {
   double pcg_rel_tol;        /* extension: stop at ||r_k|| / ||r_0|| <= tol (0: fixed count) */
   int32_t line_search;       /* choose the step among {1, 1/2, 1/4, 1/8} (energy.wgsl); 1 in the reference */
   int32_t lag_coarse;        /* reuse the coarse levels after a substep's first Newton iteration; 1 */
+  int32_t overlap_launches;  /* extension: kernels of the PCG loop start while their predecessor drains
+                                (programmatic dependent launch; the smoother stages its line factors
+                                meanwhile); 0 serialises them; 1 */
 } btd_params;
 
 /* GPU_DEFAULTS (solver.ts:61-72). */

@@ -45,6 +45,7 @@ def test_default_params_are_the_reference_gpu_defaults():
     assert abs(p.h - 1 / 120) < 1e-15 and p.newton_iterations == 2 and p.pcg_iterations == 2
     assert p.coarse_sweeps == 2 and p.max_coarsest_nodes == 400 and p.line_search == 1 and p.lag_coarse == 1
     assert p.newton_max == 2 and abs(p.newton_tolerance - 1e-5) < 1e-12 and p.self_contact == 1
+    assert p.overlap_launches == 1  # extension: launch overlap only, same results
 
 
 def _has_device():
