@@ -182,8 +182,13 @@ __device__ __forceinline__ M3 m3Add(const M3& x, const M3& y) {
 }
 
 // Float f of planes strided by `stride` float4 (plane f / 4).
+// Float f of a row staged as float4 planes (plane f / 4, stride `stride`): the whole float4 is loaded
+// (one conflict-free 128-bit access a lane; the loads of a plane's other floats are the same load),
+// where a 32-bit load of one float of each lane's float4 would meet a 4-way bank conflict.
 __device__ __forceinline__ float colF(const float4* col, int f, int stride = SM_THREADS) {
-  return reinterpret_cast<const float*>(col + (f >> 2) * stride)[f & 3];
+  const float4 v = col[(f >> 2) * stride];
+  const int c = f & 3;
+  return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
 }
 __device__ __forceinline__ Sym colSym(const float4* col, int f, int stride = SM_THREADS) {
   return {colF(col, f, stride), colF(col, f + 1, stride), colF(col, f + 2, stride),
@@ -226,17 +231,21 @@ struct Coupling<CoarseRows> {
 };
 
 // Chunk t of a line of len nodes cut into P chunks: [ks, ke]; idx is a node's padded position.
+// The chunk of node k is found by multiplying with rounded reciprocals: for k < 2^12, (k + 1/2) / m
+// lies at least 1/(2m) from an integer and the rounding error of the product is below 1e-4, so the
+// truncation is exact (an integer division would cost a dependent instruction sequence per node).
 struct Chunks {
   int P, base, extra, S;
-  __host__ __device__ Chunks(int len)
-      : P(linePartitions(len)), base(len / linePartitions(len)), extra(len % linePartitions(len)), S(chunkSlot(len)) {}
-  __host__ __device__ Chunks(int P_, int base_, int extra_, int S_) : P(P_), base(base_), extra(extra_), S(S_) {}
-  __host__ __device__ Chunks() : P(1), base(1), extra(0), S(1) {}
+  float rb1, rb;  // 1 / (base + 1), 1 / base
+  __host__ __device__ Chunks(int len) : Chunks(linePartitions(len), len / linePartitions(len), len % linePartitions(len), chunkSlot(len)) {}
+  __host__ __device__ Chunks(int P_, int base_, int extra_, int S_)
+      : P(P_), base(base_), extra(extra_), S(S_), rb1(1.0f / (float)(base_ + 1)), rb(1.0f / (float)base_) {}
+  __host__ __device__ Chunks() : Chunks(1, 1, 0, 1) {}
   __device__ int start(int t) const { return t * base + min(t, extra); }
   __device__ int size(int t) const { return base + (t < extra ? 1 : 0); }
   __device__ int of(int k) const {
     const int cut = extra * (base + 1);
-    return k < cut ? k / (base + 1) : extra + (k - cut) / base;
+    return k < cut ? (int)(((float)k + 0.5f) * rb1) : extra + (int)(((float)(k - cut) + 0.5f) * rb);
   }
   __device__ int idx(int k) const {
     const int t = of(k);
@@ -436,7 +445,8 @@ struct LineGeom {
 
 // One CTA per line, blockDim.x threads (a multiple of 32, up to SM_SWEEP_THREADS).
 constexpr int SM_SWEEP_THREADS = 256;
-__host__ inline int sweepThreads(int maxLine) { return std::min(SM_SWEEP_THREADS, std::max(64, (maxLine + 31) / 32 * 32)); }
+// At least 128: the dense end-unknown product has 3Q <= 96 outputs, one a thread, in one round.
+__host__ inline int sweepThreads(int maxLine) { return std::min(SM_SWEEP_THREADS, std::max(128, (maxLine + 31) / 32 * 32)); }
 
 // One line of a sweep, its geometry resolved.
 struct LineAt {
@@ -622,7 +632,7 @@ __device__ __forceinline__ void sweepLine(const DLevel& L, const LineAt& a, cons
 
 
 template <class Rows, int FAM>
-__global__ void __launch_bounds__(SM_SWEEP_THREADS) k_smooth(DLevel L, LineGeom g, const int4* __restrict__ lines, const int* __restrict__ base,
+__global__ void __launch_bounds__(SM_SWEEP_THREADS, 1) k_smooth(DLevel L, LineGeom g, const int4* __restrict__ lines, const int* __restrict__ base,
                                                        const float4* __restrict__ fac, int T, uint32_t* err) {
   __shared__ uint64_t bar;
   extern __shared__ float4 sm4[];
