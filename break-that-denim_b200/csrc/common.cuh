@@ -382,6 +382,8 @@ __device__ __forceinline__ void storeSymAt(float* row, int f, Sym s) {
 struct DLevel {
   int N;
   int nLayers;
+  DLevelLayer one;  // the level's layer when it has a single one (nx = 0 otherwise): positions follow
+                    // from the node index, with no table lookup
   const DLevelLayer* __restrict__ layers;
   const uint2* __restrict__ coord;  // (i | j << 16, layer)
   float4* op;

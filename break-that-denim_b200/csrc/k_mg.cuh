@@ -36,6 +36,18 @@ __device__ __forceinline__ void nodeCoord(const DLevel& L, int n, int* i, int* j
   *j = c.x >> 16;
   *l = c.y;
 }
+// Node n's position and layer index: by arithmetic on a single-layer level, else from the table.
+__device__ __forceinline__ void nodeAt(const DLevel& L, int n, int* i, int* j, int* l) {
+  if (L.one.nx > 0) {
+    const int m = n - L.one.offset;
+    *j = m / L.one.nx;
+    *i = m - *j * L.one.nx;
+    *l = 0;
+  } else {
+    nodeCoord(L, n, i, j, l);
+  }
+}
+__device__ __forceinline__ DLevelLayer layerOf(const DLevel& L, int l) { return L.one.nx > 0 ? L.one : L.layers[l]; }
 
 constexpr float LINK_MIN_INTACT = 0.02f;
 
@@ -188,13 +200,10 @@ __global__ void k_residual_fine(DLevel F) {
   pdlLaunchNext();
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= F.N) return;
-  if (F.fixed[n]) {
-    F.R[n] = make_float4(0, 0, 0, 0);
-    return;
-  }
   int i, j, l;
-  nodeCoord(F, n, &i, &j, &l);
-  const DLevelLayer L = F.layers[l];
+  nodeAt(F, n, &i, &j, &l);
+  const DLevelLayer L = layerOf(F, l);
+  const uint32_t fixedRow = F.fixed[n];
   float3 r = f3(F.B[n]);
   float4 pl[FINE_PLANES];
 #pragma unroll
@@ -221,7 +230,7 @@ __global__ void k_residual_fine(DLevel F) {
       r -= row[54 + q - 8] * xm[q];
     }
   }
-  F.R[n] = make_float4(r.x, r.y, r.z, 0.f);
+  F.R[n] = fixedRow ? make_float4(0, 0, 0, 0) : make_float4(r.x, r.y, r.z, 0.f);
 }
 
 // Row dj = R - 2 of the coarse stencil at node n = (i, j): sum over di of A(n, di, dj) x (di = -2..2).
@@ -284,18 +293,15 @@ __global__ void k_residual_coarse(DLevel F) {
   const bool valid = it < 8 * F.N;
   const int n = valid ? it >> 3 : 0;
   int i = 0, j = 0, l = 0;
-  if (valid) nodeCoord(F, n, &i, &j, &l);
-  coarseResidualLane(F, F.layers[valid ? l : 0], n, i, j, it & 7, valid);
+  if (valid) nodeAt(F, n, &i, &j, &l);
+  coarseResidualLane(F, layerOf(F, l), n, i, j, it & 7, valid);
 }
 
 // b_c = P^T r_f and x_c = 0 (restrictResidual, multigrid.wgsl:204-232) for coarse node I at (ci, cj)
 // of its layer, whose fine layer is Lf: the up to 3 x 3 fine nodes, all loads issued together.
 __device__ __forceinline__ void restrictAt(const DLevel& F, const DLevel& C, const DLevelLayer& Lf, int I, int ci, int cj) {
   C.X[I] = make_float4(0, 0, 0, 0);
-  if (C.fixed[I]) {
-    C.B[I] = make_float4(0, 0, 0, 0);
-    return;
-  }
+  const uint32_t fixedRow = C.fixed[I];
   const int fi0 = coarseToFine(ci, Lf.nx), fj0 = coarseToFine(cj, Lf.ny);
   float4 w4[9], r4[9];
   uint32_t fx[9];
@@ -317,7 +323,7 @@ __device__ __forceinline__ void restrictAt(const DLevel& F, const DLevel& C, con
     const Bracket bai = bracketOf(ai, Lf.nx), baj = bracketOf(aj, Lf.ny);
     s += pwSlot(w4[q], (bai.lo == ci ? 0 : 1) + 2 * (baj.lo == cj ? 0 : 1)) * f3(r4[q]);
   }
-  C.B[I] = make_float4(s.x, s.y, s.z, 0.f);
+  C.B[I] = fixedRow ? make_float4(0, 0, 0, 0) : make_float4(s.x, s.y, s.z, 0.f);
 }
 
 __global__ void k_restrict(DLevel F, DLevel C) {
@@ -326,13 +332,13 @@ __global__ void k_restrict(DLevel F, DLevel C) {
   int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= C.N) return;
   int ci, cj, l;
-  nodeCoord(C, I, &ci, &cj, &l);
-  restrictAt(F, C, F.layers[l], I, ci, cj);
+  nodeAt(C, I, &ci, &cj, &l);
+  restrictAt(F, C, layerOf(F, l), I, ci, cj);
 }
 
 // x_f += P x_c (prolongAdd, multigrid.wgsl:237-258) at fine node a = (i, j) of layers Lf / Lc.
 __device__ __forceinline__ void prolongAt(const DLevel& F, const DLevel& C, const DLevelLayer& Lf, const DLevelLayer& Lc, int a, int i, int j) {
-  if (F.fixed[a]) return;
+  const uint32_t fixedRow = F.fixed[a];
   const Bracket bi = bracketOf(i, Lf.nx), bj = bracketOf(j, Lf.ny);
   const float4 w = F.pw[a];
   const float4 x = F.X[a];
@@ -345,7 +351,7 @@ __device__ __forceinline__ void prolongAt(const DLevel& F, const DLevel& C, cons
     const float wk = pwSlot(w, q);
     if (wk != 0.f) s += wk * xc[q];
   }
-  F.X[a] = make_float4(x.x + s.x, x.y + s.y, x.z + s.z, 0.f);
+  if (!fixedRow) F.X[a] = make_float4(x.x + s.x, x.y + s.y, x.z + s.z, 0.f);
 }
 
 __global__ void k_prolong(DLevel F, DLevel C) {
@@ -354,8 +360,8 @@ __global__ void k_prolong(DLevel F, DLevel C) {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= F.N) return;
   int i, j, l;
-  nodeCoord(F, a, &i, &j, &l);
-  prolongAt(F, C, F.layers[l], C.layers[l], a, i, j);
+  nodeAt(F, a, &i, &j, &l);
+  prolongAt(F, C, layerOf(F, l), layerOf(C, l), a, i, j);
 }
 
 }  // namespace btd

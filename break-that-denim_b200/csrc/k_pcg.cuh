@@ -170,11 +170,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_matvec(PcgArgs a) {
   double v[1] = {0.0};
   const DLevel& F = a.F;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < F.N; n += gridDim.x * blockDim.x) {
+    // the row's loads do not wait for its fixed flag (a fixed row's product is dropped)
     float3 y = make_float3(0, 0, 0);
-    if (!F.fixed[n]) {
+    const uint32_t fixedRow = F.fixed[n];
+    {
       int i, j, l;
-      nodeCoord(F, n, &i, &j, &l);
-      const DLevelLayer L = F.layers[l];
+      nodeAt(F, n, &i, &j, &l);
+      const DLevelLayer L = layerOf(F, l);
       // fp32 products summed in FP64: the recurrence residual then drifts from the true one by the
       // rounding of the stored Ap only
       double y0 = 0.0, y1 = 0.0, y2 = 0.0;
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_matvec(PcgArgs a) {
         const double q[3] = {pm.x, pm.y, pm.z};
         symVecAddD(FineRows::coupling(F.op, F.N, n, k), q, y0, y1, y2);
       }
-      y = make_float3((float)y0, (float)y1, (float)y2);
+      if (!fixedRow) y = make_float3((float)y0, (float)y1, (float)y2);
     }
     a.Ap[n] = make_float4(y.x, y.y, y.z, 0.f);
     float3 p = f3(a.p[n]);
@@ -265,10 +267,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_true_residual(PcgArgs a) {
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < F.N; n += gridDim.x * blockDim.x) {
     const float3 b = f3(a.b0[n]);
     double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-    if (!F.fixed[n]) {
+    const uint32_t fixedRow = F.fixed[n];
+    {
       int i, j, l;
-      nodeCoord(F, n, &i, &j, &l);
-      const DLevelLayer L = F.layers[l];
+      nodeAt(F, n, &i, &j, &l);
+      const DLevelLayer L = layerOf(F, l);
       symVecAddD(FineRows::diag(F.op, F.N, n), a.dd + 3 * n, y0, y1, y2);
 #pragma unroll
       for (int k = 0; k < FineRows::NC; ++k) {
@@ -278,6 +281,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_true_residual(PcgArgs a) {
         symVecAddD(FineRows::coupling(F.op, F.N, n, k), a.dd + 3 * m, y0, y1, y2);
       }
     }
+    if (fixedRow) y0 = y1 = y2 = 0.0;
     const double r0 = (double)b.x - y0, r1 = (double)b.y - y1, r2 = (double)b.z - y2;
     a.F.B[n] = make_float4((float)r0, (float)r1, (float)r2, 0.f);
     v[0] += r0 * r0 + r1 * r1 + r2 * r2;

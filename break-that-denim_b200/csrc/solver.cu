@@ -71,6 +71,7 @@ struct Level {
     DLevel d;
     d.N = N;
     d.nLayers = (int)layers.size();
+    d.one = layers.size() == 1 ? layers[0] : DLevelLayer{0, 0, 0, 0};
     d.layers = dLayers;
     d.coord = dCoord;
     d.op = op;
