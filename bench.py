@@ -22,6 +22,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "break-that-denim_b200")
 METRIC = "Newton steps/s at rel-res 1e-6: learned-precond vs plain MG-PCG, 1 B200"
@@ -35,7 +37,14 @@ WORKLOADS = {
     "config0-64": dict(n=64, size=0.3, h=1 / 60, newton=4, rel=1e-6,
                        desc="64x64-vertex hanging shell patch (0.3 m), dt 1/60, 4 projected-Newton, 3-level MG-PCG to rel-res 1e-6"),
 }
+BATCH = "batch-512"
+WORKLOADS[BATCH] = dict(n=None, size=None, h=1 / 60, newton=4, rel=1e-6,
+                        desc="512 independent hanging patches (the batched configuration): sides uniform in [16, 128] nodes at "
+                             "the config-0 pitch, stiffness factors U(0.5, 2), central yarn regions of 0-30 % with lognormal "
+                             "break strains, one edge grip each pulled at 0.05-0.2 m/s, all seeded; dt 1/60, 4 projected-Newton, "
+                             "MG-PCG to rel-res 1e-6; sharded across GPUs by estimated bytes")
 DEFAULT_WORKLOAD = "hanging-256"
+HIST_EDGES = [0, 5, 10, 15, 20, 25, 30, 40, 60, 100, 500]
 MG = dict(max_coarsest_nodes=400, coarse_sweeps=2, line_colors=3, lag_coarse=True, line_search=True)
 
 
@@ -120,10 +129,43 @@ def cpu_sample(btd, w, substeps, threads=0):
     return substeps * w["newton"] / dt, dt, cores
 
 
+def batch_cpu_sample(btd, patches=2):
+    """The oracle on the first `patches` patches of the batch, one substep each, grips held."""
+    sys.path.insert(0, ROOT)
+    from oracle import Oracle
+
+    c = btd.configs.CONFIG3
+    dt = 0.0
+    newton = 0
+    for sc, g in btd.configs.config3(only=list(range(patches))):
+        o = Oracle(sc, h=c["h"], newton_iterations=c["newton_iterations"], pcg_iterations=500, pcg_rel_tol=c["pcg_rel_tol"], **MG)
+        x = o.x
+        nodes = np.asarray(g["nodes"])
+        anchor = x[g["picked"]].copy()
+        o.add_grip(nodes, np.asarray(g["weights"], np.float64), (x[nodes] - x[g["picked"]]).reshape(-1), anchor, g["stiffness"])
+        o.set_grip_goal(0, anchor + c["h"] * g["velocity"])
+        t = time.perf_counter()
+        o.substep()
+        dt += time.perf_counter() - t
+        newton += c["newton_iterations"]
+    return newton / dt, dt, os.cpu_count() or 1
+
+
 def run_reference(args, w, rank):
     if rank != 0:
         return
     btd = package()
+    if args.workload == BATCH:
+        value, dt, cores = batch_cpu_sample(btd, max(1, args.steps))
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Newton steps/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(1, args.steps), "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": args.workload, "description": w["desc"]},
+                "cpu_baseline": {"value": value, "unit": "Newton steps/s", "cores": cores, "kind": "port",
+                                 "sample": f"one substep of each of the first {max(1, args.steps)} patches"},
+                "e2e": {"value": value, "unit": "Newton steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
     for _ in range(args.warmup):
         pass  # the CPU solver has no warm-up state worth timing; warm-up steps run inside the sample below
     steps = max(1, args.steps)
@@ -137,7 +179,145 @@ def run_reference(args, w, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, w, rank, world, local, dist):
+    """The batched configuration: this rank's shard of the patches (by estimated bytes), each a solver
+    on its own stream and graph, driven one substep of every patch at a time (grip targets set, then
+    btd_batch_substeps); the per-patch Newton and PCG counts gathered to rank 0 at the end."""
+    import torch
+
+    btd = package()
+    c = btd.configs.CONFIG3
+    sides = btd.configs.config3_sides(count=args.patches)
+    mine = btd.configs.shard_patches(sides, world)[rank]
+    t_setup = time.perf_counter()
+    patches = btd.configs.config3(count=args.patches, only=mine)
+    params = btd.configs.solver_params(c["h"], c["newton_iterations"], c["pcg_rel_tol"])
+    solvers, anchors = [], []
+    for sc, g in patches:
+        s = btd.GpuSolver(sc, params)
+        a = s.x[g["picked"]].astype(np.float32)
+        s.attach_patch(0, g["picked"], g["nodes"], g["weights"], a, g["stiffness"], max_lead=g["max_lead"])
+        solvers.append(s)
+        anchors.append(a)
+    t_setup = time.perf_counter() - t_setup
+    step = [0]
+
+    def advance():
+        step[0] += 1
+        for s, a, (_, g) in zip(solvers, anchors, patches):
+            s.set_target((a + step[0] * c["h"] * g["velocity"]).astype(np.float32))
+        btd.batch_substeps(solvers, 1)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        for s in solvers:
+            s.synchronize()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        advance()
+    barrier()
+    for s in solvers:
+        s.clear_counters()
+    idx = local
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        idx = vis.split(",")[local]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(idx) as clocks:
+        ev0.record()
+        for _ in range(args.steps):
+            advance()
+        for s in solvers:
+            s.synchronize()
+        torch.cuda.synchronize()
+        ev1.record()
+        ev1.synchronize()
+    t_dev = ev0.elapsed_time(ev1) / 1e3
+    stats = {}
+    for b, s in zip(mine, solvers):
+        cd = s.counter_dict()
+        stats[b] = (int(cd["newton"]), int(cd["pcg_total"]), sides[b])
+    launches = sum(s.launch_count(args.steps, stats[b][0], stats[b][1]) for b, s in zip(mine, solvers))
+
+    # end to end through the C ABI: every patch's state in from pinned host buffers, the batch
+    # substep, every state out
+    lib_check = btd._abi.check
+    host = []
+    for s in solvers:
+        xh = torch.empty((s.N, 4), dtype=torch.float32, pin_memory=True)
+        vh = torch.empty((s.N, 4), dtype=torch.float32, pin_memory=True)
+        lib_check("btd_get_state", s._h, xh.data_ptr(), vh.data_ptr())
+        host.append((xh, vh))
+    for s in solvers:
+        s.clear_counters()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for s, (xh, vh) in zip(solvers, host):
+            lib_check("btd_set_state", s._h, xh.data_ptr(), vh.data_ptr())
+        btd.batch_substeps(solvers, 1)
+        for s, (xh, vh) in zip(solvers, host):
+            lib_check("btd_get_state", s._h, xh.data_ptr(), vh.data_ptr())
+    barrier()
+    t_e2e = time.perf_counter() - t0
+    newton_e2e = sum(s.counter_dict()["newton"] for s in solvers)
+    bytes_step = sum(2 * 16 * s.N for s in solvers)
+
+    gathered = [stats]
+    if dist is not None:
+        t = torch.tensor([t_dev, t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev, t_e2e = float(t[0].item()), float(t[1].item())
+        e = torch.tensor([newton_e2e, bytes_step, launches], device="cuda", dtype=torch.float64)
+        dist.all_reduce(e)
+        newton_e2e, bytes_step, launches = float(e[0].item()), float(e[1].item()), float(e[2].item())
+        gathered = [None] * world
+        dist.all_gather_object(gathered, stats)
+    for s in solvers:
+        s.close()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    merged = {}
+    for d in gathered:
+        merged.update(d)
+    newton = sum(v[0] for v in merged.values())
+    per = np.array([v[1] / max(1, v[0]) for v in merged.values()])
+    hist, _ = np.histogram(per, bins=HIST_EDGES)
+    line = {
+        "metric": METRIC, "value": newton / t_dev, "unit": "Newton steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "description": w["desc"], "patches": len(merged),
+                   "nodes": int(sum(v[2] ** 2 for v in merged.values())),
+                   "substeps_per_s": len(merged) * args.steps / t_dev,
+                   "pcg_iterations_per_newton": float(per.mean()),
+                   "pcg_iterations_per_newton_histogram": {"edges": HIST_EDGES, "patches": hist.tolist()},
+                   "l2": "inputs larger than L2 (every patch's state and operators, about 1.5 GB)",
+                   "setup_s": t_setup, "parallelism": f"patches sharded x{world}"},
+        "e2e": {"value": newton_e2e / t_e2e, "unit": "Newton steps/s", "h2d_bytes_per_step": int(bytes_step),
+                "d2h_bytes_per_step": int(bytes_step)},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        v_cpu, dt_cpu, cores = batch_cpu_sample(btd)
+        line["cpu_baseline"] = {"value": v_cpu, "unit": "Newton steps/s", "cores": cores, "kind": "port",
+                                "sample": f"one substep of each of the first 2 patches, {dt_cpu:.1f} s"}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
+    # the batched workload runs one stream a patch: let up to 32 of them reach the GPU's hardware
+    # queues at once (the default is 8); read when CUDA initialises, so set before it does
+    if BATCH in sys.argv:
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -146,6 +326,7 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--eager", action="store_true", help="launch kernel by kernel (for per-kernel profilers)")
+    ap.add_argument("--patches", type=int, default=512, help="patches of the batch workload")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     w = WORKLOADS[args.workload]
@@ -167,6 +348,9 @@ def main():
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    if args.workload == BATCH:
+        run_batch(args, w, rank, world, local, dist)
+        return
     btd = package()
     sc = build_scene(btd, w)
     params = btd.configs.solver_params(w["h"], w["newton"], w["rel"])

@@ -244,16 +244,39 @@ def _scaled_patch(n, pitch, f, seed, cache):
     return sc
 
 
-def config3(seed=31, count=None, sides=None):
+def config3_sides(seed=31, count=None, sides=None):
+    """The patches' lattice sides (nodes a side) of config3, without building them."""
+    c = CONFIG3
+    count = count or c["count"]
+    lo, hi = sides or c["sides"]
+    r = splitmix64(seed, 8 * count).astype(np.float64) / 2.0**64
+    return [lo + int(r[8 * b] * (hi - lo + 1)) for b in range(count)]
+
+
+def shard_patches(sides, world):
+    """Patches of a batch dealt to `world` GPUs by estimated bytes (proportional to the node count):
+    largest first, each to the least loaded rank (ties to the lowest rank), so every rank gets the
+    same list whatever its own index. Returns one sorted index list a rank."""
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    for b in sorted(range(len(sides)), key=lambda b: (-sides[b] ** 2, b)):
+        k = min(range(world), key=lambda q: (load[q], q))
+        load[k] += sides[b] ** 2
+        out[k].append(b)
+    return [sorted(o) for o in out]
+
+
+def config3(seed=31, count=None, sides=None, only=None):
     """The batch: a list of patches, each (scene, grip) with grip = dict(picked, nodes, weights,
-    velocity, stiffness, max_lead)."""
+    velocity, stiffness, max_lead); with `only`, the patches of those indices (each patch depends on
+    its index alone)."""
     c = CONFIG3
     count = count or c["count"]
     lo, hi = sides or c["sides"]
     r = splitmix64(seed, 8 * count).astype(np.float64) / 2.0**64
     out = []
     cache = {}
-    for b in range(count):
+    for b in (range(count) if only is None else only):
         u = r[8 * b: 8 * b + 8]
         n = lo + int(u[0] * (hi - lo + 1))
         f = c["stiffness"][0] + (c["stiffness"][1] - c["stiffness"][0]) * u[1]
