@@ -129,6 +129,18 @@ def cpu_sample(btd, w, substeps, threads=0):
     return substeps * w["newton"] / dt, dt, cores
 
 
+def across_ranks(dist, values, op="max", device="cuda"):
+    """Every rank's `values` combined over the ranks (the max of the device times: the job takes as
+    long as its slowest rank; the sum of counts); unchanged on a single process."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return [float(v) for v in t.tolist()]
+
+
 def batch_cpu_sample(btd, patches=2):
     """The oracle on the first `patches` patches of the batch, one substep each, grips held."""
     sys.path.insert(0, ROOT)
@@ -268,12 +280,8 @@ def run_batch(args, w, rank, world, local, dist):
 
     gathered = [stats]
     if dist is not None:
-        t = torch.tensor([t_dev, t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_dev, t_e2e = float(t[0].item()), float(t[1].item())
-        e = torch.tensor([newton_e2e, bytes_step, launches], device="cuda", dtype=torch.float64)
-        dist.all_reduce(e)
-        newton_e2e, bytes_step, launches = float(e[0].item()), float(e[1].item()), float(e[2].item())
+        t_dev, t_e2e = across_ranks(dist, [t_dev, t_e2e], "max")
+        newton_e2e, bytes_step, launches = across_ranks(dist, [newton_e2e, bytes_step, launches], "sum")
         gathered = [None] * world
         dist.all_gather_object(gathered, stats)
     for s in solvers:
@@ -384,9 +392,7 @@ def main():
     pcg_total = c["pcg_total"]
     t_dev = ms_step * args.steps / 1e3
     if dist is not None:
-        t = torch.tensor([t_dev], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_dev = float(t.item())
+        t_dev = across_ranks(dist, [t_dev], "max")[0]
     value = world * newton_total / t_dev
     launches = gpu.launch_count(args.steps, newton_total, pcg_total)
 
@@ -408,9 +414,7 @@ def main():
     t_e2e = time.perf_counter() - t0
     newton_e2e = gpu.counter_dict()["newton"]
     if dist is not None:
-        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+        t_e2e = across_ranks(dist, [t_e2e], "max")[0]
     e2e = world * newton_e2e / t_e2e
 
     # ---- roofline of the dominant kernel (fine-level smoother sweep), live, cold L2 per launch

@@ -68,3 +68,40 @@ def test_per_patch_statistics_gather_over_two_ranks():
         p.join(timeout=60)
         assert p.exitcode == 0
     assert got == list(range(40))
+
+
+def _bench_rank(rank, world, port, out):
+    import importlib.util
+    import sys
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(root, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    sys.modules["bench_under_test"] = bench
+    spec.loader.exec_module(bench)
+    # replicas: rank r took 1 + r seconds for 10 Newton steps; the job time is the slowest rank's
+    t = bench.across_ranks(dist, [1.0 + rank, 0.5 * (1 + rank)], "max", device="cpu")
+    n = bench.across_ranks(dist, [10.0], "sum", device="cpu")
+    if rank == 0:
+        out.put((t, n))
+    dist.destroy_process_group()
+
+
+def test_replica_timing_is_the_slowest_rank_over_two_ranks():
+    """bench.py --gpus N runs N replicas (one patch does not shard): value = all ranks' Newton steps
+    over the slowest rank's device time; the reduction over two gloo ranks."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_bench_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    t, n = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert t == [2.0, 1.0] and n == [20.0]
