@@ -2,8 +2,8 @@
 
 The oracle restates the reference's own CPU solver (src/simulation/reference/solver.ts and
 newtonMultigrid.ts with laws.ts, axial.ts, lattice.ts, yarnField.ts) in C++. Only tests/,
-__graft_entry__.smoke() and bench.py's CPU-baseline leg use it, as the checker; the product never
-imports it.
+__graft_entry__.smoke() and bench.py's CPU-baseline leg use it, to compare against and to time;
+the product never imports it.
 """
 import ctypes as C
 import os
