@@ -436,7 +436,9 @@ def main():
         btd._abi.check("btd_get_state", h, xh.data_ptr(), vh.data_ptr())
     barrier()
     t_e2e = time.perf_counter() - t0
-    newton_e2e = gpu.counter_dict()["newton"]
+    cd_e2e = gpu.counter_dict()
+    newton_e2e = cd_e2e["newton"]
+    pcg_e2e = cd_e2e["pcg_total"] / max(1, cd_e2e["newton"])
     if dist is not None:
         t_e2e = across_ranks(dist, [t_e2e], "max")[0]
     e2e = world * newton_e2e / t_e2e
@@ -469,7 +471,9 @@ def main():
                    "newton_per_step": w["newton"], "pcg_iterations_per_newton": pcg_total / max(1, newton_total),
                    "l2": "flushed before every timed step (256 MiB rewrite outside the events)",
                    "parallelism": f"replicas x{world}"},
-        "e2e": {"value": e2e, "unit": "Newton steps/s", "h2d_bytes_per_step": 2 * 16 * N, "d2h_bytes_per_step": 2 * 16 * N},
+        "e2e": {"value": e2e, "unit": "Newton steps/s", "h2d_bytes_per_step": 2 * 16 * N, "d2h_bytes_per_step": 2 * 16 * N,
+                "pcg_iterations_per_newton": pcg_e2e,
+                "loop": "each step: the state in from pinned host memory (the same state every step), one substep, the state out"},
         "gpu_launches": int(launches),
         "roofline": {"kernel": "k_smooth<FineRows> (fine yarn-line sweep, 6 colour launches)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
