@@ -473,7 +473,7 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e, "unit": "Newton steps/s", "h2d_bytes_per_step": 2 * 16 * N, "d2h_bytes_per_step": 2 * 16 * N,
                 "pcg_iterations_per_newton": pcg_e2e,
-                "loop": "each step: the state in from pinned host memory (the same state every step), one substep, the state out"},
+                "loop": "each step: the state in from pinned host memory (the previous step's output), one substep, the state out"},
         "gpu_launches": int(launches),
         "roofline": {"kernel": "k_smooth<FineRows> (fine yarn-line sweep, 6 colour launches)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
