@@ -178,6 +178,7 @@ SIGNATURES = {
     "btd_set_graph_mode": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_read_counters": ([C.c_void_p, C.c_void_p, C.c_int32], C.c_int),
     "btd_clear_counters": ([C.c_void_p], C.c_int),
+    "btd_settle_drape": ([C.c_void_p], C.c_int),
     "btd_stage_predict": ([C.c_void_p], C.c_int),
     "btd_stage_assemble": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_stage_vcycle": ([C.c_void_p], C.c_int),

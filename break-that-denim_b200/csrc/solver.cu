@@ -1208,6 +1208,42 @@ int btd_read_counters(btd_solver* s, uint32_t* out, int32_t n) {
   });
 }
 
+// settleDrape (settle.ts:24-62): 420 substeps of 5 Newton iterations with a fixed 2 PCG iterations,
+// history off (pre-tension must not tear), velocities cleared after every tenth of the first 360
+// (kinetic damping), then velocities and counters cleared; the solver's settings come back after.
+int btd_settle_drape(btd_solver* s) {
+  GUARD({
+    checkSolver(s);
+    constexpr int SETTLE_STEPS = 420, SETTLE_DAMPED = 360, SETTLE_NEWTON = 5, SETTLE_PCG = 2;
+    const SimParams savedP = s->hostP;
+    const btd_params savedPrm = s->params;
+    auto restore = [&] {
+      s->hostP = savedP;
+      s->params = savedPrm;
+      s->pushParams();
+    };
+    s->hostP.pcgMax = SETTLE_PCG;
+    s->hostP.pcgTol = 0.0;
+    s->hostP.historyOn = 0;
+    s->params.pcg_iterations = SETTLE_PCG;
+    s->params.pcg_rel_tol = 0.0;
+    s->pushParams();
+    try {
+      for (int k = 0; k < SETTLE_STEPS; ++k) {
+        s->runSubstep(SETTLE_NEWTON, SETTLE_NEWTON);
+        if (k % 10 == 9 && k < SETTLE_DAMPED) CK(cudaMemsetAsync(s->v, 0, sizeof(float4) * s->N, s->stream));
+      }
+      CK(cudaMemsetAsync(s->v, 0, sizeof(float4) * s->N, s->stream));
+      CK(cudaMemsetAsync(s->dCounters, 0, sizeof(uint32_t) * CNT_SIZE, s->stream));
+    } catch (...) {
+      restore();
+      throw;
+    }
+    restore();
+    s->sync();
+  });
+}
+
 int btd_clear_counters(btd_solver* s) {
   GUARD({
     checkSolver(s);

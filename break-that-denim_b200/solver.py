@@ -67,6 +67,11 @@ class GpuSolver:
     def synchronize(self):
         check("btd_synchronize", self._h)
 
+    def settle_drape(self):
+        """settleDrape (settle.ts:24-62): 420 damped substeps of 5 Newton / 2 PCG iterations, history
+        off; the solver's settings are restored afterwards."""
+        check("btd_settle_drape", self._h)
+
     # ---- state I/O
     def set_state(self, position, velocity=None):
         """setState (solver.ts:833-837): positions (N, 3) or (N, 4) (w >= 0.5 retires a node); velocities or zero."""

@@ -211,6 +211,13 @@ int btd_set_graph_mode(btd_solver* s, int32_t use_graphs);
 /* Extension: PCG cap and relative-residual stop (0 = fixed count as the reference). */
 int btd_set_pcg(btd_solver* s, int32_t max_iterations, double rel_tol);
 
+/* settleDrape (settle.ts:24-62): settle the authored drape before interaction - 420 substeps of 5
+ * Newton iterations with a fixed 2 PCG iterations each, history off, velocities cleared after every
+ * tenth of the first 360 substeps, then velocities and counters cleared. The solver's Newton, PCG and
+ * history settings are restored afterwards. Blocking. The drape file (settle.ts:4-22: a 16-byte
+ * header [magic 0x50415244, version 1, node count, sceneHash] then 4 floats a node) is host code
+ * around btd_get_state / btd_set_state and btd_scene_hash. */
+int btd_settle_drape(btd_solver* s);
 /* Counters (solver.ts:218-225); n <= BTD_COUNTERS. btd_clear_counters zeroes them. */
 int btd_read_counters(btd_solver* s, uint32_t* out, int32_t n);
 int btd_clear_counters(btd_solver* s);

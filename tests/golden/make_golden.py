@@ -5,6 +5,7 @@ drape_header.json: the header of the reference's precomputed drape (public/drape
 drape_collar.npz: the drape's positions of the mounted collar nodes (scene.ts:309 pins 2 rows on
 every side); settling never moves mounted nodes, so these are the compiled initial positions
 rounded to float32, a known answer for the scene compiler.
+drape_settled.npz: the drape's positions of every ninth free node, the reference's settled state.
 """
 import json
 import os
@@ -26,4 +27,8 @@ j, i = np.divmod(np.arange(n), nx)
 collar = (i < cr) | (j < cr) | (i >= nx - cr) | (j >= ny - cr)
 idx = np.nonzero(collar)[0].astype(np.int32)
 np.savez_compressed(os.path.join(HERE, "drape_collar.npz"), index=idx, position=pos[idx, :3].copy())
-print("wrote", len(idx), "collar nodes, hash", hex(h))
+# drape_settled.npz: the settled positions of every ninth free node (the reference's own GPU solve of
+# settleDrape, settle.ts:24-62), for the end-to-end check of btd_settle_drape
+free = np.nonzero(~collar)[0][::9].astype(np.int32)
+np.savez_compressed(os.path.join(HERE, "drape_settled.npz"), index=free, position=pos[free, :3].copy())
+print("wrote", len(idx), "collar nodes,", len(free), "settled free nodes, hash", hex(h))
