@@ -52,6 +52,17 @@ def lib():
             "ora_potential": ([vp], C.c_double),
             "ora_yarn_material_length": ([vp], C.c_double),
             "ora_solve_penta": ([C.c_int32, vp, vp, vp, vp, vp, C.c_double], C.c_int),
+            "ora_law_axial": ([vp, C.c_double, vp], None),
+            "ora_law_strain_at_tension": ([vp, C.c_double], C.c_double),
+            "ora_law_yarn_damage": ([vp] + [C.c_double] * 5, C.c_double),
+            "ora_law_bend_psi": ([C.c_double, C.c_double, vp], None),
+            "ora_law_bend_psi_delta": ([C.c_double] * 4, C.c_double),
+            "ora_law_bend_geometry": ([C.c_double, C.c_double, vp], None),
+            "ora_law_bend_scale": ([C.c_double, C.c_double, C.c_uint32, C.c_uint32, C.c_int32], C.c_double),
+            "ora_law_shear_jam": ([C.c_double], C.c_double),
+            "ora_law_cell_area": ([C.c_double] * 4, C.c_double),
+            "ora_law_shear": ([C.c_double] * 4 + [vp], None),
+            "ora_law_constants": ([vp], None),
         }
         for name, (a, r) in sig.items():
             getattr(h, name).argtypes = a
@@ -278,3 +289,71 @@ class Oracle:
         done, rel = C.c_int32(), C.c_double()
         _call("ora_pcg", C.c_void_p(self._h), _ptr(b), _ptr(x), iterations, C.c_double(rel_tol), C.byref(done), C.byref(rel))
         return x.reshape(-1, 3), done.value, rel.value
+
+
+class laws:
+    """The oracle's constitutive laws on their own (axial.ts, laws.ts), for the reference's unit-test
+    properties; a yarn is (eaLow, eaHigh, crimpStrain, eaCompress)."""
+
+    @staticmethod
+    def _y(y):
+        return _ptr(np.ascontiguousarray(y, np.float64))
+
+    @staticmethod
+    def axial(y, eps):
+        """(tension, stiffness, energy density) at strain eps (axial.ts:16-42)."""
+        out = np.zeros(3)
+        lib().ora_law_axial(laws._y(y), eps, _ptr(out))
+        return tuple(out)
+
+    @staticmethod
+    def strain_at_tension(y, t):
+        return lib().ora_law_strain_at_tension(laws._y(y), t)
+
+    @staticmethod
+    def yarn_damage(y, yarns, area, peak, soft, eps):
+        return lib().ora_law_yarn_damage(laws._y(y), yarns, area, peak, soft, eps)
+
+    @staticmethod
+    def bend_psi(q, a):
+        out = np.zeros(3)
+        lib().ora_law_bend_psi(q, a, _ptr(out))
+        return tuple(out)
+
+    @staticmethod
+    def bend_psi_delta(q0, q1, dq, a):
+        return lib().ora_law_bend_psi_delta(q0, q1, dq, a)
+
+    @staticmethod
+    def bend_geometry(La, Lc):
+        """(wa, wc, kPerB, fold) (laws.ts:54-58)."""
+        out = np.zeros(4)
+        lib().ora_law_bend_geometry(La, Lc, _ptr(out))
+        return tuple(out)
+
+    @staticmethod
+    def bend_scale(ia, ic, mask_a, mask_c, B):
+        return lib().ora_law_bend_scale(ia, ic, mask_a, mask_c, B)
+
+    @staticmethod
+    def shear_jam(area):
+        return lib().ora_law_shear_jam(area)
+
+    @staticmethod
+    def cell_area(cu, tu, cv, rv):
+        return lib().ora_law_cell_area(cu, tu, cv, rv)
+
+    @staticmethod
+    def shear(ks, Ld, l, jam=None):
+        """(force, stiffness, energy) (laws.ts:140-159); jam defaults to SHEAR_JAM."""
+        out = np.zeros(3)
+        lib().ora_law_shear(ks, Ld, l, laws.constants()[1] if jam is None else jam, _ptr(out))
+        return tuple(out)
+
+    @staticmethod
+    def constants():
+        """(BEND_S0, SHEAR_JAM, SHEAR_RAMP)."""
+        out = np.zeros(3)
+        lib().ora_law_constants(_ptr(out))
+        return tuple(out)
+

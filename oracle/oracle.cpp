@@ -2511,4 +2511,32 @@ int ora_solve_penta(int32_t n, const double* D, const double* E, const double* F
   return 0;
 }
 
+// ---- the constitutive laws on their own (axial.ts, laws.ts), so the reference's unit-test properties
+// can be checked on the restatement; yarn = {eaLow, eaHigh, crimpStrain, eaCompress}.
+static Yarn lawYarn(const double* y) {
+  Yarn p{};
+  p.eaLow = y[0], p.eaHigh = y[1], p.crimpStrain = y[2], p.eaCompress = y[3];
+  p.yarnsPerSpan = 1;
+  return p;
+}
+void ora_law_axial(const double* y, double eps, double* tke) {
+  const Yarn p = lawYarn(y);
+  tke[0] = axialTension(p, eps), tke[1] = axialStiffness(p, eps), tke[2] = axialEnergyDensity(p, eps);
+}
+double ora_law_strain_at_tension(const double* y, double t) { return strainAtTension(lawYarn(y), t); }
+double ora_law_yarn_damage(const double* y, double yarns, double area, double peak, double soft, double eps) {
+  return yarnDamage(lawYarn(y), yarns, area, peak, soft, eps);
+}
+void ora_law_bend_psi(double q, double a, double* out3) { bendPsi(q, a, out3); }
+double ora_law_bend_psi_delta(double q0, double q1, double dq, double a) { return bendPsiDelta(q0, q1, dq, a); }
+void ora_law_bend_geometry(double La, double Lc, double* out4) {
+  const BendGeometry g = bendGeometry(La, Lc);
+  out4[0] = g.wa, out4[1] = g.wc, out4[2] = g.kPerB, out4[3] = g.fold;
+}
+double ora_law_bend_scale(double ia, double ic, uint32_t maskA, uint32_t maskC, int32_t B) { return bendScale(ia, ic, maskA, maskC, B); }
+double ora_law_shear_jam(double area) { return shearJam(area); }
+double ora_law_cell_area(double cu, double tu, double cv, double rv) { return cellArea(cu, tu, cv, rv); }
+void ora_law_shear(double ks, double Ld, double l, double jam, double* fke) { shearLaw(ks, Ld, l, jam, fke); }
+void ora_law_constants(double* out3) { out3[0] = BEND_S0, out3[1] = SHEAR_JAM, out3[2] = SHEAR_RAMP; }
+
 }  // extern "C"

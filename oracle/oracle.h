@@ -100,6 +100,19 @@ int ora_pcg(ora_solver* s, const double* b, double* x, int32_t iterations, doubl
 int ora_solve_penta(int32_t n, const double* D, const double* E, const double* F, const double* r, double* x,
                     double shift);
 
+/* The constitutive laws on their own (axial.ts, laws.ts); yarn = {eaLow, eaHigh, crimpStrain, eaCompress}. */
+void ora_law_axial(const double* yarn, double eps, double* tension_stiffness_energy);
+double ora_law_strain_at_tension(const double* yarn, double t);
+double ora_law_yarn_damage(const double* yarn, double yarns, double area, double peak, double soft, double eps);
+void ora_law_bend_psi(double q, double a, double* psi3);
+double ora_law_bend_psi_delta(double q0, double q1, double dq, double a);
+void ora_law_bend_geometry(double La, double Lc, double* wa_wc_kperb_fold);
+double ora_law_bend_scale(double ia, double ic, uint32_t maskA, uint32_t maskC, int32_t B);
+double ora_law_shear_jam(double area);
+double ora_law_cell_area(double cu, double tu, double cv, double rv);
+void ora_law_shear(double ks, double Ld, double l, double jam, double* force_stiffness_energy);
+void ora_law_constants(double* bend_s0_shear_jam_shear_ramp);
+
 #ifdef __cplusplus
 }
 #endif
