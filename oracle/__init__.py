@@ -63,6 +63,18 @@ def lib():
             "ora_law_cell_area": ([C.c_double] * 4, C.c_double),
             "ora_law_shear": ([C.c_double] * 4 + [vp], None),
             "ora_law_constants": ([vp], None),
+            "ora_field_layer": ([vp, C.c_int32, vp], C.c_int),
+            "ora_field_span_crossing": ([vp] + [C.c_int32] * 6, C.c_int32),
+            "ora_field_own_span": ([vp] + [C.c_int32] * 4 + [vp], C.c_int32),
+            "ora_field_interpolated_strain": ([vp] + [C.c_int32] * 4 + [vp], C.c_double),
+            "ora_field_couple": ([vp], C.c_int32),
+            "ora_field_update": ([vp, vp], C.c_int),
+            "ora_field_pull_out": ([vp, vp], C.c_int32),
+            "ora_field_recoil_length": ([vp] + [C.c_double] * 9, C.c_double),
+            "ora_field_share_reach": ([vp, C.c_int32, C.c_int32], C.c_int32),
+            "ora_field_share_factor": ([vp, C.c_int32, vp] + [C.c_int32] * 4 + [C.c_double], C.c_double),
+            "ora_field_share_cap": ([C.c_int32] + [C.c_double] * 5, C.c_double),
+            "ora_field_constants": ([vp], None),
         }
         for name, (a, r) in sig.items():
             getattr(h, name).argtypes = a
@@ -174,6 +186,44 @@ class Oracle:
 
     def set_field(self, damage):
         _call("ora_set_field", C.c_void_p(self._h), _ptr(np.ascontiguousarray(damage, np.uint8)))
+
+    # ---- the yarn damage field's steps on this solver's field and spans (yarnField.ts)
+    def field_layer(self, layer=0):
+        """dict(offset, K, M, bu, bv, nx, ny, node_offset) of a layer's field."""
+        out = np.zeros(8, np.int32)
+        _call("ora_field_layer", C.c_void_p(self._h), layer, _ptr(out))
+        return dict(zip(("offset", "K", "M", "bu", "bv", "nx", "ny", "node_offset"), (int(v) for v in out)))
+
+    def span_crossing(self, i, j, f, q, p, layer=0):
+        """spanCrossing (yarnField.ts:201-204): the absolute crossing index."""
+        return lib().ora_field_span_crossing(C.c_void_p(self._h), layer, i, j, f, q, p)
+
+    def own_span(self, k, m, f, layer=0):
+        """ownSpan (yarnField.ts:187-196): (i, j), or None."""
+        ij = np.zeros(2, np.int32)
+        ok = lib().ora_field_own_span(C.c_void_p(self._h), layer, k, m, f, _ptr(ij))
+        return (int(ij[0]), int(ij[1])) if ok else None
+
+    def interpolated_strain(self, f, k, m, strain, layer=0):
+        return lib().ora_field_interpolated_strain(C.c_void_p(self._h), layer, f, k, m, _ptr(np.ascontiguousarray(strain, np.float64)))
+
+    def couple_spans(self):
+        """coupleSpans (yarnField.ts:443-499) on the current field and spans; returns the ruptures."""
+        return lib().ora_field_couple(C.c_void_p(self._h))
+
+    def update_field(self, strain):
+        """updateField (yarnField.ts:323-415) with the given strain of every span (2 per node)."""
+        _call("ora_field_update", C.c_void_p(self._h), _ptr(np.ascontiguousarray(strain, np.float64)))
+
+    def pull_out(self, strain):
+        """pullOut (yarnField.ts:125-152) with the given strains; returns the crossings pulled."""
+        return lib().ora_field_pull_out(C.c_void_p(self._h), _ptr(np.ascontiguousarray(strain, np.float64)))
+
+    def share_reach(self, f, layer=0):
+        return lib().ora_field_share_reach(C.c_void_p(self._h), layer, f)
+
+    def share_factor(self, sep, f, k, m, reach, cap=float("inf"), layer=0):
+        return lib().ora_field_share_factor(C.c_void_p(self._h), layer, _ptr(np.ascontiguousarray(sep, np.uint8)), f, k, m, reach, cap)
 
     def set_history(self, on):
         _call("ora_set_history", C.c_void_p(self._h), int(on))
@@ -356,4 +406,20 @@ class laws:
         out = np.zeros(3)
         lib().ora_law_constants(_ptr(out))
         return tuple(out)
+
+
+def recoil_length(yarn, B, area, peak, eps, mu, n0, wrap, t_cross, pitch):
+    """recoilLength (yarnField.ts:109-115); yarn = (eaLow, eaHigh, crimpStrain, eaCompress)."""
+    return lib().ora_field_recoil_length(_ptr(np.ascontiguousarray(yarn, np.float64)), B, area, peak, eps, mu, n0, wrap, t_cross, pitch)
+
+
+def share_cap(reach, mu, n0, wrap, t_cross, peak):
+    return lib().ora_field_share_cap(reach, mu, n0, wrap, t_cross, peak)
+
+
+def field_constants():
+    """(SHARE.fraction, DAMAGE_CUT, DAMAGE_PULLED)."""
+    out = np.zeros(3)
+    lib().ora_field_constants(_ptr(out))
+    return float(out[0]), int(out[1]), int(out[2])
 

@@ -2539,4 +2539,64 @@ double ora_law_cell_area(double cu, double tu, double cv, double rv) { return ce
 void ora_law_shear(double ks, double Ld, double l, double jam, double* fke) { shearLaw(ks, Ld, l, jam, fke); }
 void ora_law_constants(double* out3) { out3[0] = BEND_S0, out3[1] = SHEAR_JAM, out3[2] = SHEAR_RAMP; }
 
+// ---- the yarn damage field's steps on a solver's own field and spans (yarnField.ts), so the
+// reference's unit-test properties can be checked on the restatement.
+// layer info: fOffset, K, M, bu, bv, nx, ny, nodeOffset
+int ora_field_layer(ora_solver* o, int32_t l, int32_t* out8) {
+  if (l < 0 || l >= (int)o->s.layers.size()) {
+    g_err = "layer out of range";
+    return -1;
+  }
+  const Layer& L = o->s.layers[l];
+  const int32_t v[8] = {L.fOffset, L.K, L.M, L.bu, L.bv, L.nx, L.ny, L.nodeOffset};
+  std::copy(v, v + 8, out8);
+  return 0;
+}
+int32_t ora_field_span_crossing(ora_solver* o, int32_t l, int32_t i, int32_t j, int32_t f, int32_t q, int32_t p) {
+  return spanCrossing(o->s.layers[l], i, j, f, q, p);
+}
+// ownSpan (yarnField.ts:187-196): the span (i, j) of family f that crossing (k, m) of the layer's
+// field belongs to; returns 0 when it belongs to none.
+int32_t ora_field_own_span(ora_solver* o, int32_t l, int32_t k, int32_t m, int32_t f, int32_t* ij) {
+  const Layer& L = o->s.layers[l];
+  auto fdiv = [](int a, int b) { return static_cast<int>(std::floor(static_cast<double>(a) / b)); };
+  int i, j;
+  bool ok;
+  if (f == 1) {
+    i = fdiv(k, L.bu), j = fdiv(m - L.bv / 2, L.bv);
+    ok = i < L.nx && j >= 0 && j <= L.ny - 2;
+  } else {
+    j = fdiv(m, L.bv), i = fdiv(k - L.bu / 2, L.bu);
+    ok = j < L.ny && i >= 0 && i <= L.nx - 2;
+  }
+  ij[0] = i, ij[1] = j;
+  return ok ? 1 : 0;
+}
+double ora_field_interpolated_strain(ora_solver* o, int32_t l, int32_t f, int32_t k, int32_t m, const double* strain) {
+  return interpolatedStrain(o->s.layers[l], f, k, m, strain);
+}
+int32_t ora_field_couple(ora_solver* o) { return o->s.coupleSpans(); }
+int ora_field_update(ora_solver* o, const double* strain) {
+  std::copy(strain, strain + o->s.strain.size(), o->s.strain.begin());
+  o->s.updateField();
+  return 0;
+}
+int32_t ora_field_pull_out(ora_solver* o, const double* strain) {
+  std::copy(strain, strain + o->s.strain.size(), o->s.strain.begin());
+  return o->s.pullOut();
+}
+double ora_field_recoil_length(const double* yarn, double B, double area, double peak, double eps, double mu, double n0, double wrap,
+                               double tCross, double pitch) {
+  return recoilLength(lawYarn(yarn), B, area, peak, eps, mu, n0, wrap, tCross, pitch);
+}
+int32_t ora_field_share_reach(ora_solver* o, int32_t l, int32_t f) { return shareReach(o->s.layers[l], f); }
+double ora_field_share_factor(ora_solver* o, int32_t l, const uint8_t* sep, int32_t f, int32_t k, int32_t m, int32_t reach, double cap) {
+  return shareFactor(o->s.layers[l], sep, f, k, m, reach, cap);
+}
+double ora_field_share_cap(int32_t reach, double mu, double n0, double wrap, double tCross, double peak) {
+  return shareCap(reach, mu, n0, wrap, tCross, peak);
+}
+// SHARE_FRACTION, DAMAGE_CUT, DAMAGE_PULLED
+void ora_field_constants(double* out3) { out3[0] = SHARE_FRACTION, out3[1] = DAMAGE_CUT, out3[2] = DAMAGE_PULLED; }
+
 }  // extern "C"

@@ -113,6 +113,21 @@ double ora_law_cell_area(double cu, double tu, double cv, double rv);
 void ora_law_shear(double ks, double Ld, double l, double jam, double* force_stiffness_energy);
 void ora_law_constants(double* bend_s0_shear_jam_shear_ramp);
 
+/* The yarn damage field's steps on a solver's own field and spans (yarnField.ts). */
+int ora_field_layer(ora_solver* o, int32_t layer, int32_t* foff_K_M_bu_bv_nx_ny_nodeoff);
+int32_t ora_field_span_crossing(ora_solver* o, int32_t layer, int32_t i, int32_t j, int32_t f, int32_t q, int32_t p);
+int32_t ora_field_own_span(ora_solver* o, int32_t layer, int32_t k, int32_t m, int32_t f, int32_t* ij);
+double ora_field_interpolated_strain(ora_solver* o, int32_t layer, int32_t f, int32_t k, int32_t m, const double* strain);
+int32_t ora_field_couple(ora_solver* o);
+int ora_field_update(ora_solver* o, const double* strain);
+int32_t ora_field_pull_out(ora_solver* o, const double* strain);
+double ora_field_recoil_length(const double* yarn, double B, double area, double peak, double eps, double mu, double n0, double wrap,
+                               double t_cross, double pitch);
+int32_t ora_field_share_reach(ora_solver* o, int32_t layer, int32_t f);
+double ora_field_share_factor(ora_solver* o, int32_t layer, const uint8_t* sep, int32_t f, int32_t k, int32_t m, int32_t reach, double cap);
+double ora_field_share_cap(int32_t reach, double mu, double n0, double wrap, double t_cross, double peak);
+void ora_field_constants(double* share_fraction_cut_pulled);
+
 #ifdef __cplusplus
 }
 #endif
