@@ -119,6 +119,12 @@ def label_pieces(bits, freed, lattice):
     return piece_of, np.array(start, np.uint32), nodes[:tail].copy(), h
 
 
+def grip_core(nodes, weights):
+    """The core of a grip patch (interaction.ts:231-237): its nodes held with weight 0.5 or more -
+    the anchors that grip gives an analysis while it is held and not being let go."""
+    return [int(n) for n, w in zip(nodes, weights) if w >= 0.5]
+
+
 class Topology:
     """The analysis of topology.ts run to completion on a solver (GpuSolver, or anything with
     scene, state(), set_state() and segments()): read the spans and positions back, free the nodes

@@ -122,3 +122,70 @@ def test_an_analysis_writes_detached_nodes_back_to_the_solver():
     assert set(np.nonzero(s.x[:, 3] == 1.0)[0]) == island and (s.v == 1).all()
     assert topo.analyze() == 0 and not topo.changed  # already detached: the same pieces
     assert topo.start.tolist() == [0, 9]
+
+
+def test_two_claw_centre_piece_classification_on_the_product_scene():
+    """tests/gpu/twohand-topology.ts (classification checks) on the host analysis: on the default
+    scene, a 9 x 3 strip left in the scene (everything else retired) with only its own spans, held by
+    two claws at its ends (each with a weak rim entry on the centre, which is no anchor); the centre
+    three columns are cut free on both sides in either order or at once: after one cut the centre
+    stays held by the other hand, after both it is detached as one piece and the held sides are kept;
+    with both hands let go the whole strip detaches."""
+    from btd_b200.topology import grip_core
+
+    sc = btd.compile_scene(btd.default_spec())
+    nx = sc.layers[0].nx
+    node = lambda i, j: (50 + j) * nx + 50 + i
+    strip = [node(k % 9, k // 9) for k in range(27)]
+    centre = [n for n in strip if 53 <= n % nx <= 55]
+    lat = Lattice(sc.layers, sc.N)
+    w = np.full(sc.N, 2.0)
+    w[strip] = 0.0
+
+    def setup():
+        flags = sc.seg_flags.astype(np.uint32) | SEG_BROKEN
+        for j in range(3):
+            for i in range(9):
+                if i < 8:
+                    flags[2 * node(i, j)] = SEG_EXISTS
+                if j < 2:
+                    flags[2 * node(i, j) + 1] = SEG_EXISTS
+        return flags, w.copy()
+
+    def cut(flags, side):
+        for j in range(3):
+            flags[2 * node(2 if side == 0 else 5, j)] |= SEG_BROKEN
+
+    cores = [grip_core([node(0 if slot == 0 else 8, 1), centre[slot]], [1, 0.25]) for slot in (0, 1)]
+    assert cores == [[node(0, 1)], [node(8, 1)]]  # the rim entries are no anchors
+
+    def analyze(flags, ww, anchors):
+        bits = pack_bits(flags, ww)
+        freed = search(bits, sc.pinned, anchors, lat)
+        ww[(freed == 1) & (ww <= 0.5)] = 1.0
+        return label_pieces(bits, freed, lat)
+
+    def verify(ww, pieces):
+        piece_of = pieces[0]
+        assert all(ww[n] == (1.0 if n in centre else 0.0) for n in strip)
+        assert piece_of[centre[0]] != NO_PIECE and all(piece_of[n] == piece_of[centre[0]] for n in centre)
+        assert all(piece_of[n] == NO_PIECE for n in strip if n not in centre)
+
+    anchors = cores[0] + cores[1]
+    for first in (0, 1):
+        flags, ww = setup()
+        analyze(flags, ww, anchors)
+        cut(flags, first)
+        analyze(flags, ww, anchors)
+        assert all(ww[n] == 0.0 for n in centre)  # still held by the other hand
+        cut(flags, 1 - first)
+        verify(ww, analyze(flags, ww, anchors))
+    flags, ww = setup()
+    analyze(flags, ww, anchors)
+    cut(flags, 0)
+    cut(flags, 1)
+    verify(ww, analyze(flags, ww, anchors))
+    flags, ww = setup()
+    analyze(flags, ww, anchors)
+    analyze(flags, ww, [])  # both hands let go
+    assert all(ww[n] == 1.0 for n in strip)
