@@ -163,6 +163,21 @@ def across_ranks(dist, values, op="max", device="cuda"):
     return [float(v) for v in t.tolist()]
 
 
+def cpu_sample_single_core(btd, w):
+    """The oracle on one host thread, bounded: the first substep's prediction and first Newton
+    iteration of the workload (a whole substep takes tens of seconds on one core at 256 x 256)."""
+    sys.path.insert(0, ROOT)
+    from oracle import Oracle
+
+    sc = build_scene(btd, w)
+    o = Oracle(sc, h=w["h"], newton_iterations=w["newton"], pcg_iterations=500, pcg_rel_tol=w["rel"], threads=1, **MG)
+    t = time.perf_counter()
+    o.predict()
+    o.newton_step()
+    dt = time.perf_counter() - t
+    return 1.0 / dt, dt
+
+
 def batch_cpu_sample(btd, patches=2):
     """The oracle on the first `patches` patches of the batch, one substep each, grips held."""
     sys.path.insert(0, ROOT)
@@ -487,6 +502,10 @@ def main():
                 else f"1 substep ({w['newton']} Newton) of the workload from its initial state")
         line["cpu_baseline"] = {"value": v_cpu, "unit": "Newton steps/s", "cores": cores, "kind": "port",
                                 "sample": f"{what}, {dt_cpu:.1f} s"}
+        if not w.get("contact"):
+            v1, dt1 = cpu_sample_single_core(btd, w)
+            line["cpu_baseline_single_core"] = {"value": v1, "unit": "Newton steps/s", "cores": 1, "kind": "port",
+                                                "sample": f"the first substep's prediction and first Newton iteration, {dt1:.1f} s"}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
