@@ -1025,6 +1025,131 @@ struct Solver {
     }
   }
 
+  // ---- cross-layer contact (contact.ts:7-19, contact.wgsl): a scene of several layers gets node-node
+  // contact between its layers in place of self-contact (solver.ts:364), when crossLayer is set.
+  // Detection once per substep on a (cell, layer) hash with the same hash and table as the shader
+  // (so collisions bring the same extra candidates), the K nearest foreign nodes within the contact
+  // distance and a quarter cell, and a directional bound; terms per Newton iterate from the pairs.
+  bool crossLayer = false;
+  static constexpr double XC_CELL = 1.0e-3, XC_K_PEN = 3000, XC_MU = 0.45, XC_FRICTION_SPEED = 0.002, XC_BOUND_FRACTION = 0.45;
+  static constexpr unsigned XC_MASK = (1u << 20) - 1u;
+  double xcDist[4] = {0, 0, 0, 0};  // midsurface contact distance of layer pairs 0-1, 0-2, 1-2; same layer
+  // hashCell (contact.wgsl:31-34)
+  static unsigned xcHash(long cx, long cy, long cz, unsigned l) {
+    unsigned h = (static_cast<unsigned>(cx) * 73856093u) ^ (static_cast<unsigned>(cy) * 19349663u) ^
+                 (static_cast<unsigned>(cz) * 83492791u) ^ (l * 2654435761u);
+    return h & XC_MASK;
+  }
+  // pairDistance (contact.wgsl:36-42)
+  double xcPair(int la, int lb) const {
+    if (la == lb) return xcDist[3];
+    const int s = la + lb;
+    return s == 1 ? xcDist[0] : s == 2 ? xcDist[1] : xcDist[2];
+  }
+  // hashCount / scan / hashFill / detect (contact.wgsl:46-129), the cells filled in node order
+  void crossDetect() {
+    const size_t T = size_t(XC_MASK) + 1;
+    std::vector<unsigned> key(N);
+    std::vector<unsigned> start(T + 1, 0);
+    for (int n = 0; n < N; ++n) {
+      double p[3];
+      curOf(n, p);
+      long c[3];
+      for (int q = 0; q < 3; ++q) c[q] = static_cast<long>(std::floor(p[q] / XC_CELL));
+      key[n] = xcHash(c[0], c[1], c[2], static_cast<unsigned>(layerOf[n]));
+      ++start[key[n] + 1];
+    }
+    for (size_t h = 0; h < T; ++h) start[h + 1] += start[h];
+    std::vector<int> items(N);
+    std::vector<unsigned> fill(start.begin(), start.end() - 1);
+    for (int n = 0; n < N; ++n) items[fill[key[n]]++] = n;
+    ctCand.assign(CT_KC * size_t(N), -1);
+    ctBound.assign(8 * size_t(N), 0.0);
+    for (int n = 0; n < N; ++n) {
+      double p[3];
+      curOf(n, p);
+      const int ln = layerOf[n];
+      int best[CT_KC];
+      double bestD[CT_KC];
+      for (int k = 0; k < CT_KC; ++k) best[k] = -1, bestD[k] = 1e9;
+      double dmin = 1e9, nmin[3] = {0, 0, 0};
+      long c[3];
+      for (int q = 0; q < 3; ++q) c[q] = static_cast<long>(std::floor(p[q] / XC_CELL));
+      for (int lo = 0; lo < static_cast<int>(layers.size()); ++lo) {
+        if (lo == ln) continue;
+        const double r = xcPair(ln, lo);
+        for (int dz = -1; dz <= 1; ++dz)
+          for (int dy = -1; dy <= 1; ++dy)
+            for (int dxc = -1; dxc <= 1; ++dxc) {
+              const unsigned h = xcHash(c[0] + dxc, c[1] + dy, c[2] + dz, static_cast<unsigned>(lo));
+              for (unsigned q = start[h]; q < start[h + 1]; ++q) {
+                const int m = items[q];
+                if (layerOf[m] != lo) continue;
+                double pm[3];
+                curOf(m, pm);
+                const double d = hyp3(p[0] - pm[0], p[1] - pm[1], p[2] - pm[2]);
+                if (d - r < dmin && d > 1e-9) {
+                  dmin = d - r;
+                  for (int z = 0; z < 3; ++z) nmin[z] = (p[z] - pm[z]) / d;
+                }
+                if (d >= r + 0.25 * XC_CELL) continue;
+                int cand = m;
+                double cd = d - r;
+                for (int k = 0; k < CT_KC; ++k)
+                  if (cd < bestD[k]) std::swap(best[k], cand), std::swap(bestD[k], cd);
+              }
+            }
+      }
+      for (int k = 0; k < CT_KC; ++k) ctCand[CT_KC * n + k] = best[k];
+      // the directional bound: approach the nearest foreign node by a share of its clearance plus
+      // half the contact distance (of the 0-1 pair, as the shader takes it); no reciprocal bound
+      if (dmin < 1e8) {
+        for (int z = 0; z < 3; ++z) ctBound[8 * n + z] = nmin[z];
+        ctBound[8 * n + 3] = XC_BOUND_FRACTION * (std::max(0.0, dmin) + 0.5 * xcDist[0]);
+      } else {
+        ctBound[8 * n + 3] = 1e9;
+      }
+      ctBound[8 * n + 7] = 1e9;
+    }
+  }
+  // terms (contact.wgsl:131-164): linear penalty and lagged-normal regularised Coulomb friction on the
+  // relative tangential step, each node's own terms into extG / extH
+  void crossTerms() {
+    extG.assign(3 * size_t(N), 0.0);
+    extH.assign(6 * size_t(N), 0.0);
+    const double epsU = XC_FRICTION_SPEED * prm.h;
+    for (int n = 0; n < N; ++n) {
+      double p[3];
+      curOf(n, p);
+      double g[3] = {0, 0, 0}, H[6] = {0, 0, 0, 0, 0, 0};
+      for (int k = 0; k < CT_KC; ++k) {
+        const int m = ctCand[CT_KC * n + k];
+        if (m < 0) continue;
+        double pm[3];
+        curOf(m, pm);
+        const double dv[3] = {p[0] - pm[0], p[1] - pm[1], p[2] - pm[2]};
+        const double d = hyp3(dv[0], dv[1], dv[2]);
+        const double r = xcPair(layerOf[n], layerOf[m]);
+        if (d >= r || d <= 1e-9) continue;
+        const double nn[3] = {dv[0] / d, dv[1] / d, dv[2] / d};
+        const double lam = XC_K_PEN * (r - d);
+        double rel[3];
+        for (int z = 0; z < 3; ++z) rel[z] = dx[3 * n + z] - dx[3 * m + z];
+        const double rn = rel[0] * nn[0] + rel[1] * nn[1] + rel[2] * nn[2];
+        const double ut[3] = {rel[0] - rn * nn[0], rel[1] - rn * nn[1], rel[2] - rn * nn[2]};
+        const double kf = XC_MU * lam / std::max(hyp3(ut[0], ut[1], ut[2]), epsU);
+        for (int z = 0; z < 3; ++z) g[z] += -lam * nn[z] + kf * ut[z];
+        const int idx[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+        for (int q = 0; q < 6; ++q) {
+          const int a = idx[q][0], b = idx[q][1];
+          H[q] += XC_K_PEN * nn[a] * nn[b] + kf * ((a == b ? 1.0 : 0.0) - nn[a] * nn[b]);
+        }
+      }
+      for (int z = 0; z < 3; ++z) extG[3 * n + z] = g[z];
+      for (int z = 0; z < 6; ++z) extH[6 * n + z] = H[z];
+    }
+  }
+
   // A half-space bound: the step may move against m by at most m[3] (step.wgsl:62-65).
   static void boundStep(double* d, const double* m) {
     double approach = -(d[0] * m[0] + d[1] * m[1] + d[2] * m[2]);
@@ -1307,7 +1432,7 @@ struct Solver {
         dx[3 * n + q] = hv;
       }
     // contact detection at the predicted iterate (SelfContact.encodeDetect, solver.ts:743)
-    if (contactOn) contactDetect();
+    if (contactOn) crossLayer ? crossDetect() : contactDetect();
     // projectStart (step.wgsl:90-95): the predicted start made feasible and bounded against the floor
     if (floor.on || contactOn)
       for (int n = 0; n < N; ++n) {
@@ -2150,7 +2275,7 @@ double chooseStep(const double* e, const double* m) {
 
 // newtonStepPCG (newtonMultigrid.ts:610-645).
 double Solver::newtonStep(int* pcgDone, double* rel, double* alphaOut) {
-  if (contactOn) contactTerms();
+  if (contactOn) crossLayer ? crossTerms() : contactTerms();
   auto A = assembleFineOperator();
   std::vector<double> b(3 * static_cast<size_t>(N));
   rhs(b.data());
@@ -2213,6 +2338,15 @@ ora_solver* ora_create(const btd_scene* sc, const ora_params* p) {
     Solver& S = o->s;
     S.prm = *p;
     S.contactOn = p->self_contact != 0;
+    S.crossLayer = p->cross_layer != 0 && sc->n_layers > 1;
+    {
+      // contact distance of a layer pair: the mean of their thicknesses (contact.ts:49-50)
+      auto thick = [&](int l) { return l < sc->n_layers ? sc->layers[l].material.thickness : 0.0; };
+      S.xcDist[0] = 0.5 * (thick(0) + thick(1));
+      S.xcDist[1] = 0.5 * (thick(0) + thick(2));
+      S.xcDist[2] = 0.5 * (thick(1) + thick(2));
+      S.xcDist[3] = 0.0;
+    }
     if (p->threads > 0) omp_set_num_threads(p->threads);
     int N = sc->node_count, C = sc->crossing_count;
     S.N = N;

@@ -37,6 +37,9 @@ typedef struct ora_params {
   int32_t line_search;
   int32_t threads;           /* OpenMP threads (0: all) */
   int32_t self_contact;      /* node-face self-contact restated from selfcontact.wgsl (the f64 reference has none) */
+  int32_t cross_layer;       /* with contact on, a scene of several layers gets the cross-layer node contact of
+                                contact.wgsl in place of self-contact, as the reference does (solver.ts:364);
+                                0 keeps self-contact on every scene */
 } ora_params;
 
 typedef struct ora_solver ora_solver;
