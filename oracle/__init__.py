@@ -248,6 +248,16 @@ class Oracle:
     def set_grip_goal(self, grip, goal):
         _call("ora_set_grip_goal", C.c_void_p(self._h), grip, _ptr(np.ascontiguousarray(goal, np.float64)))
 
+    def set_pieces(self, piece_of, start, nodes):
+        """setPieces (solver.ts:664-677): the detached pieces whose rigid modes the solve carries; an
+        empty set (start of one entry) removes them."""
+        piece_of = np.ascontiguousarray(piece_of, np.uint32)
+        start = np.ascontiguousarray(start, np.uint32)
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        count = max(0, len(start) - 1)
+        _call("ora_set_pieces", C.c_void_p(self._h), _ptr(piece_of), _ptr(start), count,
+              _ptr(nodes) if len(nodes) else None)
+
     def set_floor(self, z, bulge=0.3e-3, stiffness=1300.0, friction=0.35, friction_speed=0.002, enabled=True):
         _call("ora_set_floor", C.c_void_p(self._h), int(enabled), C.c_double(z), C.c_double(bulge), C.c_double(stiffness),
               C.c_double(friction), C.c_double(friction_speed))

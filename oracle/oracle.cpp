@@ -1150,6 +1150,44 @@ struct Solver {
     }
   }
 
+  // ---- detached pieces' rigid modes (rigid_frame.wgsl, rigid_apply.wgsl, rigid_spin.wgsl; solver.ts:612-716).
+  // A detached piece's rigid motion is resisted by its inertia, drag and contact alone, against yarn
+  // couplings far stiffer, and the multigrid hierarchy does not carry those near-null modes. Each
+  // piece's six rigid modes Z (translation, rotation about its mass centroid) give PCG an exact start
+  // x0 = Z E^-1 Z^T b with E = Z^T A Z built from what each term puts on a rigid motion (the external
+  // blocks fully, the internal terms only on rotation as their tension's geometric stiffness); the
+  // line search and update move a piece's nodes along the rotation of that start rather than its
+  // tangent, and each substep starts a spinning piece on its rotation continued over the substep.
+  // Pieces are set from outside (Topology.setPieces); with none, nothing here runs.
+  static constexpr uint32_t NO_PIECE = 0xFFFFFFFFu;
+  static constexpr int MAX_PIECES = 4096;  // solver.ts:86
+  std::vector<uint32_t> pieceOf, pieceStart, pieceNodes;
+  int pieceCount = 0;
+  std::vector<double> pieceFrame;  // 40 per piece: centroid (3), valid, E^-1 row-major (36)
+  std::vector<double> pieceStep;   // 6 per piece: rigid step (t, w), or (centroid, spin rotation) in the predictor
+  std::vector<double> curveW, curveR;  // 3 per node: the piece's rotation in the direction and the node's arm
+  std::vector<uint8_t> curveOn;
+  bool inPiece(int n) const { return pieceCount > 0 && pieceOf[n] < static_cast<uint32_t>(pieceCount); }
+  void rigidRotation(std::vector<double>& kr) const;
+  void rigidFrame(const std::vector<double>& kx);
+  void rigidStart(const double* b, double* x0);
+  void curveSet();
+  void spinStart();
+  // rotationCurve (common.wgsl:274-283): R(th) r - r - th x r, what rotating r by th adds to its tangent step
+  static void rotationCurve(const double* th, const double* r, double* out) {
+    const double phi = hyp3(th[0], th[1], th[2]);
+    if (phi < 1e-9) {
+      out[0] = out[1] = out[2] = 0;
+      return;
+    }
+    const double k[3] = {th[0] / phi, th[1] / phi, th[2] / phi};
+    double kr[3], kkr[3];
+    cross3(k, r, kr);
+    cross3(k, kr, kkr);
+    const double a = std::sin(phi) - phi, c = 1 - std::cos(phi);
+    for (int z = 0; z < 3; ++z) out[z] = a * kr[z] + c * kkr[z];
+  }
+
   // A half-space bound: the step may move against m by at most m[3] (step.wgsl:62-65).
   static void boundStep(double* d, const double* m) {
     double approach = -(d[0] * m[0] + d[1] * m[1] + d[2] * m[2]);
@@ -1242,14 +1280,43 @@ struct Solver {
         for (int q = 0; q < 3; ++q) o3[q] = pinned[m] ? 0.0 : d[3 * m + q];
       };
       auto dot = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
-      auto lenChange = [&](const double* e0, const double* de, double a, double l0, double* la) {
-        double ea[3] = {e0[0] + a * de[0], e0[1] + a * de[1], e0[2] + a * de[2]};
-        *la = hyp3(ea[0], ea[1], ea[2]);
-        return (2 * a * dot(e0, de) + a * a * dot(de, de)) / std::max(*la + l0, 1e-12);
+      // node m's step at step length k (steps, energy.wgsl:63-72): alpha d, plus on a detached piece the
+      // rotation curve of its rigid part (alpha being a power of two, alpha d is exact, so a node off
+      // every piece steps exactly as alpha times its direction)
+      const bool curves = !curveOn.empty();
+      auto stepAt = [&](int m, int k, double* o3) {
+        const double a = LINE_ALPHAS[k];
+        for (int q = 0; q < 3; ++q) o3[q] = pinned[m] ? 0.0 : a * d[3 * m + q];
+        if (curves && curveOn[m] && !pinned[m]) {
+          const double th[3] = {a * curveW[3 * m], a * curveW[3 * m + 1], a * curveW[3 * m + 2]};
+          double c[3];
+          rotationCurve(th, &curveR[3 * m], c);
+          for (int q = 0; q < 3; ++q) o3[q] += c[q];
+        }
       };
-      double dn[3], d0[3] = {dx[3 * n], dx[3 * n + 1], dx[3 * n + 2]};
-      dirOf(n, dn);
-      if (!pinned[n]) {
+      // |e0 + D| - |e0| without cancellation, and |e0 + D|
+      auto lenChange = [&](const double* e0, const double* D, double l0, double* la) {
+        double ea[3] = {e0[0] + D[0], e0[1] + D[1], e0[2] + D[2]};
+        *la = hyp3(ea[0], ea[1], ea[2]);
+        return (2 * dot(e0, D) + dot(D, D)) / std::max(*la + l0, 1e-12);
+      };
+      double sn[4][3];
+      for (int k = 0; k < NA; ++k) stepAt(n, k, sn[k]);
+      // a quadratic node term (gradient g, Hessian applied by Hs) over the steps
+      auto quadS = [&](const double* g, auto Hs) {
+        for (int k = 0; k < NA; ++k) {
+          double hs[3];
+          Hs(sn[k], hs);
+          const double lin = dot(g, sn[k]), q = 0.5 * dot(sn[k], hs);
+          o[k] += lin + q;
+          mg[k] += std::fabs(lin) + std::fabs(q);
+        }
+      };
+      double d0[3] = {dx[3 * n], dx[3 * n + 1], dx[3 * n + 2]};
+      const bool curved = curves && curveOn[n] && !pinned[n];
+      if (!pinned[n] && !curved) {
+        double dn[3];
+        dirOf(n, dn);
         double w = mass[n] / (h * h);
         double dp[3] = {d0[0] - pred[3 * n], d0[1] - pred[3 * n + 1], d0[2] - pred[3 * n + 2]};
         quad(w * dot(dn, dp), w * dot(dn, dn));
@@ -1272,6 +1339,33 @@ struct Solver {
         bool core;
         if (floorTerm(n, gf, Hf, &core)) quad(dot(gf, dn), Hf[0] * dn[0] * dn[0] + Hf[1] * dn[1] * dn[1] + Hf[2] * dn[2] * dn[2]);
       }
+      if (curved) {
+        // the same node terms along the curved steps
+        double w = mass[n] / (h * h);
+        double gi[3] = {w * (d0[0] - pred[3 * n]), w * (d0[1] - pred[3 * n + 1]), w * (d0[2] - pred[3 * n + 2])};
+        quadS(gi, [&](const double* v3, double* o3) { for (int q = 0; q < 3; ++q) o3[q] = w * v3[q]; });
+        double g[3] = {0, 0, 0};
+        double kg = gripTerm(n, g);
+        if (kg > 0) quadS(g, [&](const double* v3, double* o3) { for (int q = 0; q < 3; ++q) o3[q] = kg * v3[q]; });
+        if (contactOn && !extG.empty()) {
+          const double* eg = &extG[3 * n];
+          const double* eh = &extH[6 * n];
+          if (eg[0] != 0 || eg[1] != 0 || eg[2] != 0 || eh[0] != 0 || eh[3] != 0 || eh[5] != 0)
+            quadS(eg, [&](const double* v, double* o3) {
+              o3[0] = eh[0] * v[0] + eh[1] * v[1] + eh[2] * v[2];
+              o3[1] = eh[1] * v[0] + eh[3] * v[1] + eh[4] * v[2];
+              o3[2] = eh[2] * v[0] + eh[4] * v[1] + eh[5] * v[2];
+            });
+        }
+        double Dd[9], t1[3];
+        airDrag(n, Dd);
+        dragMul(Dd, d0, t1);
+        quadS(t1, [&](const double* v3, double* o3) { dragMul(Dd, v3, o3); });
+        double gf[3] = {0, 0, 0}, Hf[3];
+        bool core;
+        if (floorTerm(n, gf, Hf, &core))
+          quadS(gf, [&](const double* v3, double* o3) { for (int q = 0; q < 3; ++q) o3[q] = Hf[q] * v3[q]; });
+      }
       const Layer& mat = layer(n);
       for (int f = 0; f < 2; ++f) {
         const Yarn& y = mat.yarns[f];
@@ -1279,20 +1373,20 @@ struct Solver {
         int s = 2 * n + f;
         if (next >= 0 && segActive(s)) {
           double L = restLength[s];
-          double en[3], ec[3], db[3], de[3];
+          double en[3], ec[3];
           for (int q = 0; q < 3; ++q) {
             en[q] = x[3 * next + q] - x[3 * n + q];
             ec[q] = en[q] + dx[3 * next + q] - d0[q];
           }
-          dirOf(next, db);
-          for (int q = 0; q < 3; ++q) de[q] = db[q] - dn[q];
           double l0 = hyp3(ec[0], ec[1], ec[2]), ln = hyp3(en[0], en[1], en[2]);
           double T0, K0;
           response(s, l0 / L - 1, &T0, &K0);
           double c = y.axialViscosity / (L * h);
           for (int k = 0; k < NA; ++k) {
-            double la;
-            double dl = lenChange(ec, de, LINE_ALPHAS[k], l0, &la);
+            double la, sb[3], de[3];
+            stepAt(next, k, sb);
+            for (int q = 0; q < 3; ++q) de[q] = sb[q] - sn[k][q];
+            double dl = lenChange(ec, de, l0, &la);
             double Ta, Ka;
             response(s, la / L - 1, &Ta, &Ka);
             add(k, 0.5 * (T0 + Ta) * dl);
@@ -1304,21 +1398,21 @@ struct Solver {
           double cf[5];
           bendCoeffs(n, f, 2 * prev + f, s, cf);
           double kb = cf[0], kd = cf[1], ab = cf[2], wa = cf[3], wc = cf[4];
-          double rn[3], r0[3], dp[3], dq[3], dr[3];
+          double rn[3], r0[3];
           for (int q = 0; q < 3; ++q) {
             rn[q] = wa * x[3 * prev + q] - 2 * x[3 * n + q] + wc * x[3 * next + q];
             r0[q] = rn[q] + wa * dx[3 * prev + q] - 2 * d0[q] + wc * dx[3 * next + q];
           }
-          dirOf(prev, dp);
-          dirOf(next, dq);
-          for (int q = 0; q < 3; ++q) dr[q] = wa * dp[q] - 2 * dn[q] + wc * dq[q];
           double q0 = dot(r0, r0), l0 = std::sqrt(q0), lrn = hyp3(rn[0], rn[1], rn[2]);
           for (int k = 0; k < NA; ++k) {
-            double a = LINE_ALPHAS[k];
-            double dqa = 2 * a * dot(r0, dr) + a * a * dot(dr, dr);
+            double dp[3], dq[3], dr[3];
+            stepAt(prev, k, dp);
+            stepAt(next, k, dq);
+            for (int q = 0; q < 3; ++q) dr[q] = wa * dp[q] - 2 * sn[k][q] + wc * dq[q];
+            double dqa = 2 * dot(r0, dr) + dot(dr, dr);
             add(k, 0.5 * kb * bendPsiDelta(q0, q0 + dqa, dqa, ab));
             double la;
-            double dl = lenChange(r0, dr, a, l0, &la);
+            double dl = lenChange(r0, dr, l0, &la);
             add(k, 0.5 * kd * dl * (la + l0 - 2 * lrn));
           }
         }
@@ -1331,16 +1425,16 @@ struct Solver {
         for (auto& e : pq) {
           int p = e[0], q = e[1];
           if (!diagActive(n, e[2])) continue;
-          double ec[3], dq[3], dp[3], de[3];
+          double ec[3];
           for (int z = 0; z < 3; ++z) ec[z] = x[3 * q + z] + dx[3 * q + z] - x[3 * p + z] - dx[3 * p + z];
-          dirOf(q, dq);
-          dirOf(p, dp);
-          for (int z = 0; z < 3; ++z) de[z] = dq[z] - dp[z];
           double l0 = hyp3(ec[0], ec[1], ec[2]), sl0[3], sla[3];
           shearLaw(ks, Ld, l0, jam, sl0);
           for (int k = 0; k < NA; ++k) {
-            double la;
-            double dl = lenChange(ec, de, LINE_ALPHAS[k], l0, &la);
+            double la, dq[3], dp[3], de[3];
+            stepAt(q, k, dq);
+            stepAt(p, k, dp);
+            for (int z = 0; z < 3; ++z) de[z] = dq[z] - dp[z];
+            double dl = lenChange(ec, de, l0, &la);
             shearLaw(ks, Ld, la, jam, sla);
             add(k, 0.5 * (sl0[0] + sla[0]) * dl);
           }
@@ -1431,6 +1525,8 @@ struct Solver {
         pred[3 * n + q] = pinned[n] ? 0 : hv + h * h * prm.gravity[q];
         dx[3 * n + q] = hv;
       }
+    // detached pieces start from their rotation over the substep (encodePredict, solver.ts:698-704)
+    if (pieceCount > 0) spinStart();
     // contact detection at the predicted iterate (SelfContact.encodeDetect, solver.ts:743)
     if (contactOn) crossLayer ? crossDetect() : contactDetect();
     // projectStart (step.wgsl:90-95): the predicted start made feasible and bounded against the floor
@@ -1466,7 +1562,7 @@ struct Solver {
   }
 
   // multigrid
-  std::shared_ptr<StencilOperator> assembleFineOperator() const;
+  std::shared_ptr<StencilOperator> assembleFineOperator(std::vector<double>* kx = nullptr) const;
   void rhs(double* b) const;
   std::vector<MGLevel> buildHierarchy(std::shared_ptr<StencilOperator> fine) const;
   void vcycle(const std::vector<MGLevel>& levels, int k, double* x, const double* b) const;
@@ -1723,7 +1819,7 @@ const double I3[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
 
 // assembleFineOperator (newtonMultigrid.ts:169-274), plus the floor's diagonal Hessian and its hard
 // limit (assemble.wgsl:191-209, 318-322) when the floor is on.
-std::shared_ptr<StencilOperator> Solver::assembleFineOperator() const {
+std::shared_ptr<StencilOperator> Solver::assembleFineOperator(std::vector<double>* kx) const {
   std::vector<LatticeLayer> ll;
   for (auto& L : layers) ll.push_back({L.nx, L.ny, L.nodeOffset});
   auto Ap = std::make_shared<StencilOperator>(ll);
@@ -1819,6 +1915,20 @@ std::shared_ptr<StencilOperator> Solver::assembleFineOperator() const {
       scatterPair(A, p, q, H);
     }
   }
+  // the external block of each node of a detached piece (assemble.wgsl:172-190, 323-327): its
+  // inertia, grip and drag here, its contact and floor blocks and active bounds below
+  if (kx) {
+    kx->assign(9 * static_cast<size_t>(N), 0.0);
+    for (int n = 0; n < N; ++n) {
+      if (A.fixed[n] || !inPiece(n)) continue;
+      double* K = &(*kx)[9 * static_cast<size_t>(n)];
+      double gT[3] = {0, 0, 0};
+      const double w = mass[n] / (h * h) + gripTerm(n, gT);
+      double D[9];
+      airDrag(n, D);
+      for (int z = 0; z < 9; ++z) K[z] = D[z] + (z % 4 == 0 ? w : 0.0);
+    }
+  }
   // contact's diagonal blocks, the floor's, then the active bounds (contact and the floor's hard
   // limit) where the forces still press on, at ACTIVE_BOUND times the block's trace
   // (assemble.wgsl:142, 191-209, 304-322)
@@ -1828,10 +1938,13 @@ std::shared_ptr<StencilOperator> Solver::assembleFineOperator() const {
       double g[3], Hf[3];
       nodeGradient(n, g);
       double* Dn = &A.A[(static_cast<size_t>(n) * STENCIL + CENTER) * 9];
+      double* K = kx && inPiece(n) ? &(*kx)[9 * static_cast<size_t>(n)] : nullptr;
       if (contactOn && !extH.empty()) {
         const double* eh = &extH[6 * n];
         double B[9] = {eh[0], eh[1], eh[2], eh[1], eh[3], eh[4], eh[2], eh[4], eh[5]};
         for (int z = 0; z < 9; ++z) Dn[z] += B[z];
+        if (K)
+          for (int z = 0; z < 9; ++z) K[z] += B[z];
       }
       double gg[3] = {0, 0, 0};
       bool core = false;
@@ -1839,6 +1952,7 @@ std::shared_ptr<StencilOperator> Solver::assembleFineOperator() const {
         Dn[0] += Hf[0];
         Dn[4] += Hf[1];
         Dn[8] += Hf[2];
+        if (K) K[0] += Hf[0], K[4] += Hf[1], K[8] += Hf[2];
       }
       const double kAct = 100.0 * (Dn[0] + Dn[4] + Dn[8]);
       if (contactOn && !ctBound.empty())
@@ -1848,9 +1962,15 @@ std::shared_ptr<StencilOperator> Solver::assembleFineOperator() const {
           double app = -(dx[3 * n] * m[0] + dx[3 * n + 1] * m[1] + dx[3 * n + 2] * m[2]);
           if (app >= m[3] - 1e-3 * std::fabs(m[3]) && g[0] * m[0] + g[1] * m[1] + g[2] * m[2] > 0)
             for (int r = 0; r < 3; ++r)
-              for (int c = 0; c < 3; ++c) Dn[3 * r + c] += kAct * m[r] * m[c];
+              for (int c = 0; c < 3; ++c) {
+                Dn[3 * r + c] += kAct * m[r] * m[c];
+                if (K) K[3 * r + c] += kAct * m[r] * m[c];
+              }
         }
-      if (core && g[2] > 0) Dn[8] += kAct;
+      if (core && g[2] > 0) {
+        Dn[8] += kAct;
+        if (K) K[8] += kAct;
+      }
     }
   }
   return Ap;
@@ -1997,6 +2117,253 @@ void inv3(const double* a, double* out) {
   out[6] = c02 * id;
   out[7] = (a01 * a20 - a00 * a21) * id;
   out[8] = (a00 * a11 - a01 * a10) * id;
+}
+
+// rotationOfSpring (assemble.wgsl:20-26): a rigid rotation w moves the ends of a term's vector d by
+// w x d, which a spring block of transverse stiffness kPerp (or a scalar stencil k on d) resists with
+// kPerp (|d|^2 I - d d^T).
+static void addRotationOfSpring(double kPerp, const double* d, double* K) {
+  const double l2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) K[3 * r + c] += kPerp * ((r == c ? l2 : 0.0) - d[r] * d[c]);
+}
+
+// The stiffness the internal terms a node of a detached piece owns put on a rigid rotation
+// (assemble.wgsl:245, 255, 301): its span to the next node along each family (the span's transverse
+// stiffness, its tension over its length), the bending triple centred on it, and the two shear
+// diagonals it is the lower end of (of its own cell, and of the cell below, to that cell's +u corner).
+void Solver::rigidRotation(std::vector<double>& kr) const {
+  kr.assign(9 * static_cast<size_t>(N), 0.0);
+  const double h = prm.h;
+  auto pos = [&](int m, int z) { return x[3 * m + z] + dx[3 * m + z]; };
+  for (int n = 0; n < N; ++n) {
+    if (!inPiece(n) || pinned[n]) continue;
+    double* K = &kr[9 * static_cast<size_t>(n)];
+    for (int f = 0; f < 2; ++f) {
+      const int prev = nbr[4 * n + 2 * f], next = nbr[4 * n + 2 * f + 1];
+      const int s = 2 * n + f;
+      if (next >= 0 && segActive(s)) {
+        double e[3], l = 0;
+        for (int z = 0; z < 3; ++z) e[z] = pos(next, z) - pos(n, z), l += e[z] * e[z];
+        l = std::sqrt(l);
+        const double L = restLength[s];
+        double T, Kt;
+        response(s, l / L - 1, &T, &Kt);
+        const double fs = T + layer(n).yarns[f].axialViscosity / (L * h) * (l - segLength(s));
+        addRotationOfSpring(std::max(fs, 0.0) / l, e, K);
+      }
+      if (prev >= 0 && next >= 0 && segActive(2 * prev + f) && segActive(s)) {
+        double cf[5];
+        bendCoeffs(n, f, 2 * prev + f, s, cf);
+        const double kb = cf[0], fold = cf[2], wa = cf[3], wc = cf[4];
+        double r[3], q2 = 0;
+        for (int z = 0; z < 3; ++z) r[z] = wa * pos(prev, z) - 2 * pos(n, z) + wc * pos(next, z), q2 += r[z] * r[z];
+        double ps[3];
+        bendPsi(q2, fold, ps);
+        const double k = kb * (ps[1] + 2 * ps[2] * q2) + (kb * layer(n).yarns[f].bendViscosity) / h;
+        addRotationOfSpring(k, r, K);
+      }
+    }
+    // shear diagonal 0 of cell n (n to its +u+v corner) and diagonal 1 of the cell below (its +u
+    // corner to n)
+    const int below = nbr[4 * n + 2];
+    const int cells[2][2] = {{n, 0}, {below, 1}};
+    for (auto& cd : cells) {
+      const int c = cd[0];
+      if (c < 0) continue;
+      const int r = nbr[4 * c + 1], t = nbr[4 * c + 3];
+      if (r < 0 || t < 0 || !diagActive(c, cd[1])) continue;
+      const int other = cd[1] == 0 ? nbr[4 * r + 3] : r;
+      double ks, jam, sl[3], e[3], l = 0;
+      cellShear(c, &ks, &jam);
+      const double Ld = std::sqrt(restLength[2 * c] * restLength[2 * c] + restLength[2 * c + 1] * restLength[2 * c + 1]);
+      for (int z = 0; z < 3; ++z) e[z] = pos(other, z) - pos(n, z), l += e[z] * e[z];
+      l = std::sqrt(l);
+      shearLaw(ks, Ld, l, jam, sl);
+      addRotationOfSpring(std::max(sl[0], 0.0) / l, e, K);
+    }
+  }
+}
+
+// rigidFrame (rigid_frame.wgsl:56-161): per piece its mass centroid at the iterate and E = Z^T K Z
+// over its nodes' external blocks, plus their internal rotation stiffness on the rotation block; the
+// rotation block regularised relative to its scale, then E^-1 through a Cholesky factor (zero when E
+// is not positive definite).
+void Solver::rigidFrame(const std::vector<double>& kx) {
+  std::vector<double> kr;
+  rigidRotation(kr);
+  pieceFrame.assign(40 * static_cast<size_t>(pieceCount), 0.0);
+  auto tri = [](int i, int j) { return i * 6 - (i * (i + 1)) / 2 + j; };
+  for (int p = 0; p < pieceCount; ++p) {
+    const uint32_t a = pieceStart[p], b = pieceStart[p + 1];
+    double m[4] = {0, 0, 0, 0};
+    for (uint32_t k = a; k < b; ++k) {
+      const int n = static_cast<int>(pieceNodes[k]);
+      for (int z = 0; z < 3; ++z) m[z] += mass[n] * (x[3 * n + z] + dx[3 * n + z]);
+      m[3] += mass[n];
+    }
+    double c[3] = {0, 0, 0};
+    if (m[3] > 0)
+      for (int z = 0; z < 3; ++z) c[z] = m[z] / m[3];
+    double e[21] = {0};
+    for (uint32_t k = a; k < b; ++k) {
+      const int n = static_cast<int>(pieceNodes[k]);
+      const double* K = &kx[9 * static_cast<size_t>(n)];
+      double r[3];
+      for (int z = 0; z < 3; ++z) r[z] = x[3 * n + z] + dx[3 * n + z] - c[z];
+      double Z[6][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+      for (int i = 0; i < 3; ++i) cross3(Z[i], r, Z[3 + i]);
+      for (int i = 0; i < 6; ++i) {
+        double KZ[3];
+        for (int row = 0; row < 3; ++row) KZ[row] = K[3 * row] * Z[i][0] + K[3 * row + 1] * Z[i][1] + K[3 * row + 2] * Z[i][2];
+        for (int j = i; j < 6; ++j) e[tri(i, j)] += Z[j][0] * KZ[0] + Z[j][1] * KZ[1] + Z[j][2] * KZ[2];
+      }
+      const double* R = &kr[9 * static_cast<size_t>(n)];
+      for (int i = 0; i < 3; ++i)
+        for (int j = i; j < 3; ++j) e[tri(3 + i, 3 + j)] += R[3 * i + j];
+    }
+    double* F = &pieceFrame[40 * static_cast<size_t>(p)];
+    F[0] = c[0], F[1] = c[1], F[2] = c[2], F[3] = m[3] > 0 ? 1 : 0;
+    const double st = (e[tri(0, 0)] + e[tri(1, 1)] + e[tri(2, 2)]) / 3;
+    const double sr = (e[tri(3, 3)] + e[tri(4, 4)] + e[tri(5, 5)]) / 3;
+    const double eps = 1e-6 * std::max(sr, 1e-8 * st) + 1e-30;
+    double A6[6][6], Lc[6][6] = {{0}};
+    for (int i = 0; i < 6; ++i) {
+      for (int j = 0; j < 6; ++j) A6[i][j] = e[tri(std::min(i, j), std::max(i, j))];
+      if (i >= 3) A6[i][i] += eps;
+    }
+    bool ok = st > 0;
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j <= i; ++j) {
+        double sum = A6[i][j];
+        for (int k = 0; k < j; ++k) sum -= Lc[i][k] * Lc[j][k];
+        if (i == j) {
+          if (sum <= 0) ok = false, sum = 1;
+          Lc[i][i] = std::sqrt(sum);
+        } else {
+          Lc[i][j] = sum / Lc[j][j];
+        }
+      }
+    for (int col = 0; col < 6; ++col) {
+      double y[6], z6[6];
+      for (int i = 0; i < 6; ++i) {
+        double sum = i == col ? 1 : 0;
+        for (int k = 0; k < i; ++k) sum -= Lc[i][k] * y[k];
+        y[i] = sum / Lc[i][i];
+      }
+      for (int i = 5; i >= 0; --i) {
+        double sum = y[i];
+        for (int k = i + 1; k < 6; ++k) sum -= Lc[k][i] * z6[k];
+        z6[i] = sum / Lc[i][i];
+      }
+      for (int i = 0; i < 6; ++i) F[4 + 6 * i + col] = ok ? z6[i] : 0.0;
+    }
+  }
+}
+
+// rigidReduce / rigidApply (rigid_apply.wgsl:37-87): per piece the rhs force and torque about its
+// centroid and its rigid step (t, w) = E^-1 (force, torque); x0 = t + w x r on its nodes, zero elsewhere.
+void Solver::rigidStart(const double* b, double* x0) {
+  pieceStep.assign(6 * static_cast<size_t>(pieceCount), 0.0);
+  for (int p = 0; p < pieceCount; ++p) {
+    const double* F = &pieceFrame[40 * static_cast<size_t>(p)];
+    double g[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t k = pieceStart[p]; k < pieceStart[p + 1]; ++k) {
+      const int n = static_cast<int>(pieceNodes[k]);
+      double r[3], t[3];
+      for (int z = 0; z < 3; ++z) r[z] = x[3 * n + z] + dx[3 * n + z] - F[z], g[z] += b[3 * n + z];
+      cross3(r, &b[3 * n], t);
+      for (int z = 0; z < 3; ++z) g[3 + z] += t[z];
+    }
+    for (int i = 0; i < 6; ++i) {
+      double sum = 0;
+      for (int j = 0; j < 6; ++j) sum += F[4 + 6 * i + j] * g[j];
+      pieceStep[6 * p + i] = F[3] > 0.5 ? sum : 0.0;
+    }
+  }
+  for (int n = 0; n < N; ++n) {
+    if (!inPiece(n)) continue;
+    const int p = static_cast<int>(pieceOf[n]);
+    const double* F = &pieceFrame[40 * static_cast<size_t>(p)];
+    const double* q = &pieceStep[6 * p];
+    double r[3], wr[3];
+    for (int z = 0; z < 3; ++z) r[z] = x[3 * n + z] + dx[3 * n + z] - F[z];
+    cross3(q + 3, r, wr);
+    for (int z = 0; z < 3; ++z) x0[3 * n + z] = q[z] + wr[z];
+  }
+}
+
+// curveSet (rigid_spin.wgsl:138-154): per node of a piece with a valid frame, the rotation of the
+// direction's rigid start and the node's arm from the centroid at the iterate.
+void Solver::curveSet() {
+  curveOn.assign(N, 0);
+  curveW.assign(3 * static_cast<size_t>(N), 0.0);
+  curveR.assign(3 * static_cast<size_t>(N), 0.0);
+  for (int n = 0; n < N; ++n) {
+    if (!inPiece(n)) continue;
+    const int p = static_cast<int>(pieceOf[n]);
+    const double* F = &pieceFrame[40 * static_cast<size_t>(p)];
+    if (!(F[3] > 0.5)) continue;
+    curveOn[n] = 1;
+    for (int z = 0; z < 3; ++z) {
+      curveW[3 * n + z] = pieceStep[6 * p + 3 + z];
+      curveR[3 * n + z] = x[3 * n + z] + dx[3 * n + z] - F[z];
+    }
+  }
+}
+
+// spinReduce / spinApply (rigid_spin.wgsl:44-136): a piece's rotation over the last substep, from its
+// angular momentum about its centroid (w = I^-1 L, regularised as the rigid frame), continued over
+// this one: the start moves by (R + R^T - 2 I) r = -2 (1 - cos th) r_perp about the centroid.
+void Solver::spinStart() {
+  pieceStep.assign(6 * static_cast<size_t>(pieceCount), 0.0);
+  for (int p = 0; p < pieceCount; ++p) {
+    const uint32_t a = pieceStart[p], b = pieceStart[p + 1];
+    double M = 0, mx[3] = {0, 0, 0}, mv[3] = {0, 0, 0};
+    for (uint32_t k = a; k < b; ++k) {
+      const int n = static_cast<int>(pieceNodes[k]);
+      M += mass[n];
+      for (int z = 0; z < 3; ++z) mx[z] += mass[n] * x[3 * n + z], mv[z] += mass[n] * v[3 * n + z];
+    }
+    double c[3] = {0, 0, 0}, vc[3] = {0, 0, 0};
+    if (M > 0)
+      for (int z = 0; z < 3; ++z) c[z] = mx[z] / M, vc[z] = mv[z] / M;
+    double L[3] = {0, 0, 0}, I[6] = {0, 0, 0, 0, 0, 0};  // xx yy zz xy xz yz
+    for (uint32_t k = a; k < b; ++k) {
+      const int n = static_cast<int>(pieceNodes[k]);
+      const double m = mass[n];
+      double r[3], u[3], t[3];
+      for (int z = 0; z < 3; ++z) r[z] = x[3 * n + z] - c[z], u[z] = v[3 * n + z] - vc[z];
+      cross3(r, u, t);
+      for (int z = 0; z < 3; ++z) L[z] += m * t[z];
+      const double rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+      I[0] += m * (rr - r[0] * r[0]);
+      I[1] += m * (rr - r[1] * r[1]);
+      I[2] += m * (rr - r[2] * r[2]);
+      I[3] -= m * r[0] * r[1];
+      I[4] -= m * r[0] * r[2];
+      I[5] -= m * r[1] * r[2];
+    }
+    const double eps = 1e-6 * (I[0] + I[1] + I[2]) / 3 + 1e-30;
+    const double T[9] = {I[0] + eps, I[3], I[4], I[3], I[1] + eps, I[5], I[4], I[5], I[2] + eps};
+    double Ti[9], th[3];
+    inv3(T, Ti);
+    for (int z = 0; z < 3; ++z) th[z] = (Ti[3 * z] * L[0] + Ti[3 * z + 1] * L[1] + Ti[3 * z + 2] * L[2]) * prm.h;
+    if (!(M > 0) || !std::isfinite(th[0]) || !std::isfinite(th[1]) || !std::isfinite(th[2])) th[0] = th[1] = th[2] = 0;
+    for (int z = 0; z < 3; ++z) pieceStep[6 * p + z] = c[z], pieceStep[6 * p + 3 + z] = th[z];
+  }
+  for (int n = 0; n < N; ++n) {
+    if (!inPiece(n) || pinned[n]) continue;
+    const double* q = &pieceStep[6 * static_cast<size_t>(pieceOf[n])];
+    const double phi = hyp3(q[3], q[4], q[5]);
+    if (phi < 1e-9) continue;
+    const double k[3] = {q[3] / phi, q[4] / phi, q[5] / phi};
+    double r[3], kr[3], kkr[3];
+    for (int z = 0; z < 3; ++z) r[z] = x[3 * n + z] - q[z];
+    cross3(k, r, kr);
+    cross3(k, kr, kkr);
+    for (int z = 0; z < 3; ++z) dx[3 * n + z] += 2 * (1 - std::cos(phi)) * kkr[z];
+  }
 }
 void pivotInv3(const double* a, double* out, double shift) {
   double e = shift * std::max(std::max(std::fabs(a[0]), std::fabs(a[4])), std::fabs(a[8]));
@@ -2276,7 +2643,10 @@ double chooseStep(const double* e, const double* m) {
 // newtonStepPCG (newtonMultigrid.ts:610-645).
 double Solver::newtonStep(int* pcgDone, double* rel, double* alphaOut) {
   if (contactOn) crossLayer ? crossTerms() : contactTerms();
-  auto A = assembleFineOperator();
+  std::vector<double> kx;
+  auto A = assembleFineOperator(pieceCount > 0 ? &kx : nullptr);
+  // the detached pieces' rigid modes at this iterate (encodeAssemble, solver.ts:615-616)
+  if (pieceCount > 0) rigidFrame(kx);
   std::vector<double> b(3 * static_cast<size_t>(N));
   rhs(b.data());
   std::vector<MGLevel> levels;
@@ -2289,13 +2659,27 @@ double Solver::newtonStep(int* pcgDone, double* rel, double* alphaOut) {
   }
   stageLevels = levels;
   std::vector<double> d(3 * static_cast<size_t>(N), 0.0);
+  // PCG starts from each piece's rigid response (encodeRigidStart, solver.ts:651-657)
+  if (pieceCount > 0) rigidStart(b.data(), d.data());
   pcg(levels, b.data(), d.data(), prm.pcg_iterations, prm.pcg_rel_tol, pcgDone, rel);
+  // pieces step along the rotation of that start (encodeLineSearch, solver.ts:680-681)
+  if (pieceCount > 0) curveSet();
   double alpha = 1;
   if (prm.line_search) {
     double e[4], mag[4];
     energyChange(d.data(), e, mag);
     alpha = chooseStep(e, mag);
   }
+  // curveApply (energy.wgsl:293-302): delta bent so that alpha delta moves them along that path
+  if (pieceCount > 0 && alpha > 0)
+    for (int n = 0; n < N; ++n) {
+      if (pinned[n] || !curveOn[n]) continue;
+      const double th[3] = {alpha * curveW[3 * n], alpha * curveW[3 * n + 1], alpha * curveW[3 * n + 2]};
+      double c[3];
+      rotationCurve(th, &curveR[3 * n], c);
+      for (int z = 0; z < 3; ++z) d[3 * n + z] += c[z] / alpha;
+    }
+  curveOn.clear();
   double m = 0;
   for (size_t q = 0; q < d.size(); ++q) d[q] *= alpha;
   // newtonApply's contact and floor bounds (step.wgsl:97-112): the applied step is what is left of it
@@ -2510,6 +2894,31 @@ int ora_set_grip_goal(ora_solver* o, int32_t grip, const double* goal) {
   for (int q = 0; q < 3; ++q) o->s.grips[grip].goal[q] = goal[q];
   return 0;
 }
+int ora_set_pieces(ora_solver* o, const uint32_t* piece_of, const uint32_t* start, int32_t count, const uint32_t* nodes) {
+  Solver& S = o->s;
+  if (count < 0 || (count > 0 && (!piece_of || !start || !nodes))) {
+    g_err = "ora_set_pieces: bad arguments";
+    return -1;
+  }
+  // setPieces (solver.ts:664-677): pieces beyond MAX_PIECES go without the correction
+  const int kept = std::min(count, Solver::MAX_PIECES);
+  S.pieceCount = kept;
+  S.pieceOf.assign(S.N, Solver::NO_PIECE);
+  S.pieceStart.assign(start, start + (kept > 0 ? kept + 1 : 0));
+  S.pieceNodes.clear();
+  if (kept > 0) {
+    for (int n = 0; n < S.N; ++n) S.pieceOf[n] = piece_of[n] < static_cast<uint32_t>(kept) ? piece_of[n] : Solver::NO_PIECE;
+    S.pieceNodes.assign(nodes, nodes + start[kept]);
+    for (uint32_t k = 0; k < start[kept]; ++k)
+      if (nodes[k] >= static_cast<uint32_t>(S.N)) {
+        g_err = "ora_set_pieces: node out of range";
+        S.pieceCount = 0;
+        return -1;
+      }
+  }
+  return 0;
+}
+
 int ora_set_floor(ora_solver* o, int32_t enabled, double z, double bulge, double stiffness, double friction,
                   double friction_speed) {
   FloorParams& F = o->s.floor;

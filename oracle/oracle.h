@@ -67,6 +67,10 @@ int ora_add_grip(ora_solver* s, const int32_t* nodes, const double* w, const dou
                  const double* goal, double k);
 int ora_set_grip_goal(ora_solver* s, int32_t grip, const double* goal);
 /* Floor (GPU shader math, common.wgsl:251-270, restated; extension). */
+/* The detached pieces (GpuSolver.setPieces, solver.ts:664-677): per node its piece or 0xFFFFFFFF, piece p's
+   nodes nodes[start[p] .. start[p + 1]); count pieces (start has count + 1 entries), 0 removes them. Each
+   piece's rigid modes then start PCG, curve its line search and start its substeps (rigid_*.wgsl). */
+int ora_set_pieces(ora_solver* s, const uint32_t* piece_of, const uint32_t* start, int32_t count, const uint32_t* nodes);
 int ora_set_floor(ora_solver* s, int32_t enabled, double z, double bulge, double stiffness, double friction,
                   double friction_speed);
 
