@@ -3,7 +3,10 @@ restated in the oracle, pinned by the reference's own contracts for them (tests/
 piece thrown with a spin about its normal keeps its shape and its spin and falls (tumble, :139-192),
 and a piece cut out of a mounted sheet falls as freely as drag lets it at the shipped solver settings
 of two Newton and two PCG iterations (cutOut, :305-352) - which without the rigid-mode start of the
-Newton direction it does not (a few percent of its fall: the piece hovers).
+Newton direction it does not (a few percent of its fall: the piece hovers). Two more of its detached
+contracts: an intact span between two detached nodes pulled apart resists the extension
+(differential, :84-106), and bending viscosity does not resist a rigid rotation of a bent triple
+(bendViscosity, :246-304).
 
 The pieces come from the host topology analysis (topology.ts restated in btd_b200.topology) over the
 oracle's spans. The scenes are small (the product scene's node pitch, 3.42 x 3.48 mm) so the oracle
@@ -168,3 +171,82 @@ def test_setting_no_pieces_removes_the_correction():
     a.substep()
     b.substep()
     assert np.array_equal(a.x, b.x)
+
+
+def isolated(spans):
+    """A free 9 x 9 layer at zero gravity with only the given spans (owner, family) intact."""
+    m = btd.material_preset(0)
+    sc = btd.compile_scene([btd.layer_spec(m, 0.028, 0.028, bundle=(9, 6), z=0.08, seed=3)])
+    sc.pinned[:] = 0
+    o = Oracle(sc, **{**SHIPPED, "gravity": (0.0, 0.0, 0.0)})
+    seg = o.segments()
+    flags = seg["seg_flags"].copy()
+    keep = {2 * n + f for n, f in spans}
+    for q in range(2 * sc.N):
+        if q not in keep:
+            flags[q] |= SEG_BROKEN
+    o.set_segments(seg_flags=flags)
+    return sc, o, seg["rest_length"]
+
+
+def test_an_intact_span_pulled_apart_by_its_nodes_resists_the_extension():
+    """differential (detached.ts:84-106): two detached nodes joined by one intact span, moving apart
+    along it at 0.2 m/s at zero gravity: over 0.25 s the span stays within 1 % of its rest length and
+    intact."""
+    sc, o, rest = isolated([(40, 0)])
+    a, b = 40, 41
+    L = rest[2 * a]
+    x = o.x.copy()
+    x[a] = x[b] = (0.0, 0.0, 0.08)
+    x[a, 0], x[b, 0] = -L / 2, L / 2
+    v = np.zeros_like(x)
+    v[a, 0], v[b, 0] = -0.1, 0.1
+    o.set_state(x, v)
+    o.set_pieces(*pieces_of(o, sc)[:3])
+    worst = 0.0
+    for _ in range(30):
+        o.substep()
+        worst = max(worst, abs(np.linalg.norm(o.x[b] - o.x[a]) / L - 1))
+    flags = o.segments()["seg_flags"][2 * a]
+    assert worst < 0.01 and flags == 1, (worst, flags)
+
+
+def test_bending_viscosity_does_not_resist_a_rigid_rotation():
+    """bendViscosity (detached.ts:246-304): a triple bent by 0.3 rad, both spans at rest length. Its
+    viscous gradient (the gradient less that of the same scene without bending viscosity) vanishes for
+    a rigid rotation step (30 degrees about the vertical, then about the first span's axis) and is not
+    zero for a step that bends it further (the far node turned by another 0.1 rad)."""
+    m = btd.material_preset(0)
+    a = 40
+    out = {}
+    for visc in (True, False):
+        mat = btd.material_preset(0)
+        if not visc:
+            for f in range(2):
+                mat.yarns[f].bend_viscosity = 0.0
+        sc = btd.compile_scene([btd.layer_spec(mat, 0.028, 0.028, bundle=(9, 6), z=0.08, seed=3)])
+        sc.pinned[:] = 0
+        o = Oracle(sc, **{**SHIPPED, "gravity": (0.0, 0.0, 0.0)})
+        seg = o.segments()
+        flags = seg["seg_flags"].copy()
+        for q in range(2 * sc.N):
+            if q not in (2 * a, 2 * (a + 1)):
+                flags[q] |= SEG_BROKEN
+        o.set_segments(seg_flags=flags)
+        La, Lc = seg["rest_length"][2 * a], seg["rest_length"][2 * (a + 1)]
+        th = 0.3
+        p = np.array([[-La, 0, 0], [0, 0, 0], [Lc * np.cos(th), Lc * np.sin(th), 0]])
+        rz = lambda q, t: np.array([q[0] * np.cos(t) - q[1] * np.sin(t), q[0] * np.sin(t) + q[1] * np.cos(t), q[2]])  # noqa: E731
+        rx = lambda q, t: np.array([q[0], q[1] * np.cos(t) - q[2] * np.sin(t), q[1] * np.sin(t) + q[2] * np.cos(t)])  # noqa: E731
+        x = o.x.copy()
+        x[a:a + 3] = p
+        o.set_state(x, np.zeros_like(x))
+        for name, move in (("rigid", lambda q, k: rx(rz(q, np.pi / 6), np.pi / 6)), ("bend", lambda q, k: rz(q, 0.1) if k == 2 else q)):
+            dx = np.zeros_like(x)
+            for k in range(3):
+                dx[a + k] = move(p[k], k) - p[k]
+            o.set_dx(dx, np.zeros_like(x))
+            out[name, visc] = o.node_gradient(a + 1)
+    rigid = np.linalg.norm(out["rigid", True] - out["rigid", False])
+    bend = np.linalg.norm(out["bend", True] - out["bend", False])
+    assert bend > 0 and rigid < 1e-4 * bend, (rigid, bend)
