@@ -47,6 +47,16 @@ WORKLOADS[BATCH] = dict(n=None, size=None, h=1 / 60, newton=4, rel=1e-6,
                              "the config-0 pitch, stiffness factors U(0.5, 2), central yarn regions of 0-30 % with lognormal "
                              "break strains, one edge grip each pulled at 0.05-0.2 m/s, all seeded; dt 1/60, 4 projected-Newton, "
                              "MG-PCG to rel-res 1e-6; sharded across GPUs by estimated bytes")
+PRODUCT = "product-21k"
+WORKLOADS[PRODUCT] = dict(n=None, size=None, h=1 / 120, newton=2, rel=0.0, pcg=2, contact=True, product=True,
+                          desc="the product scene: the default 182 x 115 denim panel (20,930 nodes, scene.ts defaults), "
+                               "settled by the drape schedule (settle.ts), then hanging at the shipped solver settings "
+                               "(GPU_DEFAULTS: h 1/120, 2 Newton x 2 PCG iterations - fixed counts, no residual stop - "
+                               "self-contact on)")
+METRIC_PRODUCT = "Newton steps/s of the product scene's substep at the shipped settings (2 Newton x 2 PCG, self-contact)"
+# the reference's published substep times on this scene (Apple M5, WebGPU): 2 Newton x 2 PCG 6.9 ms plus
+# 0.6 ms of self-contact (docs/decisions/2026-10-10-feedback-round2.md:11-14)
+PRODUCT_PUBLISHED_MS = 6.9 + 0.6
 DEFAULT_WORKLOAD = "hanging-256"
 HIST_EDGES = [0, 5, 10, 15, 20, 25, 30, 40, 60, 100, 500]
 MG = dict(max_coarsest_nodes=400, coarse_sweeps=2, line_colors=3, lag_coarse=True, line_search=True)
@@ -63,13 +73,30 @@ def package():
 
 
 def build_scene(btd, w):
+    if w.get("product"):
+        return btd.compile_scene(btd.default_spec())
     if w.get("contact"):
         return btd.configs.config2()
     return btd.configs.hanging_patch(w["n"], w["size"], seed=1)
 
 
 def solver_params(btd, w):
+    if w.get("product"):
+        return btd.default_params()
     return btd.configs.solver_params(w["h"], w["newton"], w["rel"], self_contact=1 if w.get("contact") else 0)
+
+
+def workload_oracle(btd, w, threads=0):
+    """The oracle configured as the workload's solve (PCG to the relative residual, or the fixed count)."""
+    sys.path.insert(0, ROOT)
+    from oracle import Oracle
+
+    sc = build_scene(btd, w)
+    o = Oracle(sc, h=w["h"], newton_iterations=w["newton"], pcg_iterations=w.get("pcg", 500), pcg_rel_tol=w["rel"],
+               threads=threads, self_contact=bool(w.get("contact")), **MG)
+    if w.get("contact") and not w.get("product"):
+        o.set_floor(btd.configs.CONFIG2["floor"])
+    return o
 
 
 def peaks():
@@ -126,18 +153,12 @@ class ClockSampler:
 
 def cpu_sample(btd, w, substeps, threads=0):
     """The oracle (the reference's CPU solver restated, FP64, OpenMP) on `substeps` substeps."""
-    sys.path.insert(0, ROOT)
-    from oracle import Oracle
-
-    sc = build_scene(btd, w)
-    o = Oracle(sc, h=w["h"], newton_iterations=w["newton"], pcg_iterations=500, pcg_rel_tol=w["rel"], threads=threads,
-               self_contact=bool(w.get("contact")), **MG)
+    o = workload_oracle(btd, w, threads)
     cores = threads if threads > 0 else (os.cpu_count() or 1)
-    if w.get("contact"):
+    if w.get("contact") and not w.get("product"):
         # bounded sample: one Newton iteration with the contacts engaged - the first substep's second
         # (its prediction and first iteration, untimed, converge in ~50 PCG iterations; the later
         # ones, ~30 s each on 8 host cores, are the representative work)
-        o.set_floor(btd.configs.CONFIG2["floor"])
         o.predict()
         o.newton_step()
         t = time.perf_counter()
@@ -166,11 +187,7 @@ def across_ranks(dist, values, op="max", device="cuda"):
 def cpu_sample_single_core(btd, w):
     """The oracle on one host thread, bounded: the first substep's prediction and first Newton
     iteration of the workload (a whole substep takes tens of seconds on one core at 256 x 256)."""
-    sys.path.insert(0, ROOT)
-    from oracle import Oracle
-
-    sc = build_scene(btd, w)
-    o = Oracle(sc, h=w["h"], newton_iterations=w["newton"], pcg_iterations=500, pcg_rel_tol=w["rel"], threads=1, **MG)
+    o = workload_oracle(btd, w, threads=1)
     t = time.perf_counter()
     o.predict()
     o.newton_step()
@@ -400,7 +417,9 @@ def main():
     sc = build_scene(btd, w)
     params = solver_params(btd, w)
     gpu = btd.GpuSolver(sc, params)
-    if w.get("contact"):
+    if w.get("product"):
+        gpu.settle_drape()  # the product starts from its settled drape (drape.bin / settleDrape)
+    elif w.get("contact"):
         gpu.set_floor(btd.configs.CONFIG2["floor"])
     if args.eager:
         gpu.set_graph_mode(False)
@@ -479,7 +498,8 @@ def main():
             dist.destroy_process_group()
         return
     line = {
-        "metric": METRIC, "value": value, "unit": "Newton steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "metric": METRIC_PRODUCT if w.get("product") else METRIC, "value": value, "unit": "Newton steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": args.workload, "description": w["desc"], "nodes": N, "levels": gpu.level_count(),
@@ -496,13 +516,19 @@ def main():
                      "matvec_gbs": mv_gbs, "matvec_ms": ms_mv},
         "clocks": clocks.summary(),
     }
+    if w.get("product"):
+        line["config"]["ms_per_substep"] = ms_step
+        line["config"]["reference_published"] = {
+            "ms_per_substep": PRODUCT_PUBLISHED_MS, "hardware": "Apple M5, WebGPU",
+            "source": "docs/decisions/2026-10-10-feedback-round2.md:11-14 (2 Newton x 2 PCG 6.9 ms + self-contact 0.6 ms)",
+            "substep_time_ratio": PRODUCT_PUBLISHED_MS / ms_step}
     if world == 1 and not args.no_cpu_baseline:
         v_cpu, dt_cpu, cores = cpu_sample(btd, w, 1)
-        what = ("the first substep's second Newton iteration (contacts engaged)" if w.get("contact")
+        what = ("the first substep's second Newton iteration (contacts engaged)" if w.get("contact") and not w.get("product")
                 else f"1 substep ({w['newton']} Newton) of the workload from its initial state")
         line["cpu_baseline"] = {"value": v_cpu, "unit": "Newton steps/s", "cores": cores, "kind": "port",
                                 "sample": f"{what}, {dt_cpu:.1f} s"}
-        if not w.get("contact"):
+        if not w.get("contact") or w.get("product"):
             v1, dt1 = cpu_sample_single_core(btd, w)
             line["cpu_baseline_single_core"] = {"value": v1, "unit": "Newton steps/s", "cores": 1, "kind": "port",
                                                 "sample": f"the first substep's prediction and first Newton iteration, {dt1:.1f} s"}
