@@ -58,3 +58,23 @@ def test_layer_spec_coupon_extent():
     sc = btd.compile_scene(btd.layer_spec(d, 10 * d.pitch_u, 8 * d.pitch_v, angle=0.3, collar_rows=2, seed=3))
     assert sc.N == sc.nx * sc.ny
     assert sc.pinned.reshape(sc.ny, sc.nx)[2:-2, 2:-2].sum() == 0
+
+
+def test_scene_compile_rejects_bad_specs():
+    """No layer, a bundle wider than the 32-bit cut masks, and a layer too small for two nodes a family
+    are BTD_E_INVALID with a message, not a crash or an empty scene."""
+    import ctypes as C
+
+    from btd_b200 import _abi
+
+    m = btd.material_preset(0)
+    p = C.POINTER(_abi.SceneC)()
+    rc = _abi.lib().btd_scene_compile(None, 0, C.byref(p))
+    assert rc == -1 and "layer" in _abi.last_error(), (rc, _abi.last_error())
+    for spec in (btd.layer_spec(m, 0.05, 0.05, bundle=(33, 1), seed=3), btd.layer_spec(m, 1e-4, 0.05, bundle=(9, 6), seed=3)):
+        try:
+            btd.compile_scene([spec])
+        except _abi.BtdError as e:
+            assert e.rc == -1, e
+        else:
+            raise AssertionError("compile_scene accepted a bad spec")
