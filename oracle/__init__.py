@@ -76,6 +76,17 @@ def lib():
             "ora_field_share_factor": ([vp, C.c_int32, vp] + [C.c_int32] * 4 + [C.c_double], C.c_double),
             "ora_field_share_cap": ([C.c_int32] + [C.c_double] * 5, C.c_double),
             "ora_field_constants": ([vp], None),
+            "ora_learned_size": ([], C.c_int32),
+            "ora_learned_dims": ([vp], C.c_int32),
+            "ora_learned_set": ([vp, vp, C.c_int32, C.c_int32, C.c_double], C.c_int),
+            "ora_learned_log": ([vp, C.c_int32, C.c_int64], C.c_int),
+            "ora_learned_ops": ([vp], C.c_int32),
+            "ora_learned_op_nodes": ([vp, C.c_int32], C.c_int32),
+            "ora_learned_op": ([vp, C.c_int32, vp, vp], C.c_int),
+            "ora_learned_calls": ([vp], C.c_int32),
+            "ora_learned_call": ([vp, C.c_int32, vp, vp, vp], C.c_int),
+            "ora_learned_stats": ([vp, vp], C.c_int),
+            "ora_learned_forward": ([vp, vp, C.c_int64, vp], C.c_int),
         }
         for name, (a, r) in sig.items():
             getattr(h, name).argtypes = a
@@ -351,6 +362,59 @@ class Oracle:
         done, rel = C.c_int32(), C.c_double()
         _call("ora_pcg", C.c_void_p(self._h), _ptr(b), _ptr(x), iterations, C.c_double(rel_tol), C.byref(done), C.byref(rel))
         return x.reshape(-1, 3), done.value, rel.value
+
+    # ---- learned coarse correction (extension; no counterpart in the reference)
+    def set_learned(self, weights=None, on=True, guard=0.9):
+        """Add the learned coarse space of `weights` (flat, ora_learned_size() values) on the coarsest level
+        of every V-cycle; on=False returns to the plain method."""
+        w = None if weights is None else np.ascontiguousarray(weights, np.float64).reshape(-1)
+        _call("ora_learned_set", C.c_void_p(self._h), _ptr(w), 0 if w is None else len(w), int(on), C.c_double(guard))
+
+    def learned_log(self, on=True, capacity=1 << 20):
+        """Start (clearing) or stop logging the coarsest level's training material, at most `capacity` calls."""
+        _call("ora_learned_log", C.c_void_p(self._h), int(on), capacity)
+
+    def learned_samples(self):
+        """The logged material: ops, a list of (At, X) - the whitened coarsest operator over its free
+        unknowns (3n, 3n) and its node inputs (n, 20) - and calls, a list of (op, r, d) - the whitened
+        residual and exact correction (3n each) of one coarsest-level call."""
+        h = C.c_void_p(self._h)
+        ops = []
+        for k in range(lib().ora_learned_ops(h)):
+            n = _call("ora_learned_op_nodes", h, k)
+            At, X = np.zeros((3 * n, 3 * n)), np.zeros((n, learned_dims()[0]))
+            _call("ora_learned_op", h, k, _ptr(At), _ptr(X))
+            ops.append((At, X))
+        calls = []
+        for q in range(lib().ora_learned_calls(h)):
+            op = C.c_int32()
+            _call("ora_learned_call", h, q, C.byref(op), None, None)
+            n3 = 3 * len(ops[op.value][1])
+            r, d = np.zeros(n3), np.zeros(n3)
+            _call("ora_learned_call", h, q, C.byref(op), _ptr(r), _ptr(d))
+            calls.append((op.value, r, d))
+        return ops, calls
+
+    def learned_stats(self):
+        """dict(applied, fallbacks, solves) since creation."""
+        out = np.zeros(3, np.int64)
+        _call("ora_learned_stats", C.c_void_p(self._h), _ptr(out))
+        return dict(zip(("applied", "fallbacks", "solves"), (int(v) for v in out)))
+
+
+def learned_dims():
+    """(inputs, hidden, basis vectors) of the coarsest-level network."""
+    out = np.zeros(3, np.int32)
+    lib().ora_learned_dims(_ptr(out))
+    return tuple(int(v) for v in out)
+
+
+def learned_forward(weights, X):
+    """The network on node inputs X (rows, 20) as the oracle's V-cycle evaluates it: (rows, 24)."""
+    X = np.ascontiguousarray(X, np.float64)
+    out = np.zeros((len(X), 3 * learned_dims()[2]))
+    _call("ora_learned_forward", _ptr(np.ascontiguousarray(weights, np.float64)), _ptr(X), len(X), _ptr(out))
+    return out
 
 
 class laws:

@@ -273,6 +273,85 @@ struct MGLevel {
   std::shared_ptr<Prolongation> P;
 };
 
+// ---------------------------------------------------------------------------- learned coarse correction
+// Extension with no counterpart in the reference (the reference's coarsest level is two alternating
+// line sweeps, newtonMultigrid.ts:495-502): a learned coarse space on the coarsest level. A per-node MLP
+// maps features of each coarsest node to LC_K basis values per coordinate; with the node's diagonal
+// block D_i = L_i L_i^T the basis is Phi_i = L_i^-T Psi_i (Psi_i the network's 3 x LC_K output). Half-way
+// through the coarsest sweeps the V-cycle adds the Galerkin correction on that basis,
+//   x += Phi (Phi^T A Phi)^-1 Phi^T (b - A x),
+// an A-orthogonal projection; the sweeps around it are mirror images, so the V-cycle stays symmetric
+// and PCG keeps its plain form. Inputs per node (LC_IN = 20), none of them depending on the residual:
+//   10  lattice position u = i / (nx - 1), v = j / (ny - 1), sin/cos(pi u), sin/cos(pi v),
+//       sin/cos(2 pi u), sin/cos(2 pi v);
+//    6  D_i / tr(D_i): entries 00, 11, 22, 01, 02, 12;
+//    1  log(tr(D_i) / mean tr(D));
+//    1  fraction of the 8 window neighbours that are fixed or outside the lattice;
+//    2  damage flag (a span at the node exists but is broken or not fully intact), contact flag (contact
+//       terms on the node), each the maximum over the fine nodes its prolongation weights reach.
+// The basis is built once per PCG solve. A solve whose mean contraction per iteration
+// (||r_k|| / ||r_0||)^(1/k) exceeds the guard after three iterations restarts from its iterate with the
+// plain V-cycle (the fallback). Logging records the training material: per coarsest operator the
+// whitened operator L^-1 A L^-T over its free unknowns and the node inputs, and per call the whitened
+// residual L^-1 r and exact correction L^T A^-1 r (dense Cholesky of the coarsest level).
+// Network: tanh(x W1 + b1) -> tanh(. W2 + b2) -> . W3 + b3; W row-major [in][out]; output 3 k + c is
+// coordinate c of basis vector k.
+constexpr int LC_IN = 20, LC_HID = 64, LC_K = 8, LC_OUT = 3 * LC_K;
+constexpr int LC_WEIGHTS = LC_IN * LC_HID + LC_HID + LC_HID * LC_HID + LC_HID + LC_HID * LC_OUT + LC_OUT;
+
+void lcForward(const double* w, const double* in, double* out) {
+  const double *W1 = w, *b1 = W1 + LC_IN * LC_HID, *W2 = b1 + LC_HID, *b2 = W2 + LC_HID * LC_HID, *W3 = b2 + LC_HID,
+               *b3 = W3 + LC_HID * LC_OUT;
+  double h1[LC_HID], h2[LC_HID];
+  for (int h = 0; h < LC_HID; ++h) {
+    double s = b1[h];
+    for (int i = 0; i < LC_IN; ++i) s += in[i] * W1[i * LC_HID + h];
+    h1[h] = std::tanh(s);
+  }
+  for (int h = 0; h < LC_HID; ++h) {
+    double s = b2[h];
+    for (int i = 0; i < LC_HID; ++i) s += h1[i] * W2[i * LC_HID + h];
+    h2[h] = std::tanh(s);
+  }
+  for (int o = 0; o < LC_OUT; ++o) {
+    double s = b3[o];
+    for (int i = 0; i < LC_HID; ++i) s += h2[i] * W3[i * LC_OUT + o];
+    out[o] = s;
+  }
+}
+
+struct LearnedOp {  // one logged coarsest operator
+  int nodes = 0;              // free unknowns / 3
+  std::vector<double> At, X;  // whitened operator (3 nodes)^2, inputs nodes x LC_IN
+};
+struct LearnedCall {
+  int op = 0;
+  std::vector<double> r, d;  // whitened residual and exact correction, 3 nodes each
+};
+
+struct LearnedCoarse {
+  bool on = false;       // add the learned coarse space on the coarsest level of every V-cycle
+  bool active = false;   // this solve: on and not fallen back
+  double guard = 0.9;    // mean contraction per PCG iteration above which a solve falls back
+  std::vector<double> w; // LC_WEIGHTS
+  std::vector<float> flags;  // 2 per coarsest node, set at the start of each PCG solve
+  // the basis of the current solve: Phi (3 N x K), the Cholesky factor of Phi^T A Phi, dropped columns
+  const StencilOperator* basisOp = nullptr;
+  std::vector<double> phi, G;
+  std::vector<uint8_t> dead;
+  // logging
+  bool log = false;
+  size_t logCap = 0;  // calls
+  std::vector<LearnedOp> ops;
+  std::vector<LearnedCall> calls;
+  std::shared_ptr<const StencilOperator> denseOp;  // coarsest operator whose dense factor is cached
+  std::vector<double> denseL, nodeL;
+  std::vector<int> denseFree;
+  size_t denseDim = 0;
+  bool denseOk = false;
+  long long applied = 0, fallbacks = 0, solves = 0;
+};
+
 constexpr double LINK_MIN_INTACT = 0.02;
 constexpr double PIVOT_SHIFT = 2e-6;
 const double LINE_ALPHAS[4] = {1, 0.5, 0.25, 0.125};
@@ -1569,6 +1648,14 @@ struct Solver {
   void pcg(const std::vector<MGLevel>& levels, const double* b, double* x, int iterations, double tol, int* done,
            double* rel) const;
   double newtonStep(int* pcgDone, double* rel, double* alphaOut);
+
+  // learned coarse correction (extension; no counterpart in the reference)
+  mutable LearnedCoarse lc;
+  void learnedFlags(const std::vector<MGLevel>& levels) const;
+  bool learnedInputs(const StencilOperator& A, std::vector<double>& L, std::vector<uint8_t>& ok,
+                     std::vector<double>& X) const;
+  void learnedBasis(const std::vector<MGLevel>& levels) const;
+  void learnedCorrection(const std::vector<MGLevel>& levels, int k, double* x, const double* b) const;
 };
 
 // updateField (yarnField.ts:338-410).
@@ -2523,6 +2610,14 @@ void Solver::vcycle(const std::vector<MGLevel>& levels, int k, double* x, const 
   const StencilOperator& A = *levels[k].A;
   int colors = prm.line_colors;
   if (!levels[k].P) {
+    if (lc.active || lc.log) {
+      // the learned coarse space (extension) half-way through the sweeps, which mirror around it
+      const int half = prm.coarse_sweeps / 2;
+      for (int s = 0; s < half; ++s) smoothLines(A, x, b, (s & 1) == 1, colors);
+      learnedCorrection(levels, k, x, b);
+      for (int s = half; s < prm.coarse_sweeps; ++s) smoothLines(A, x, b, (s & 1) == 1, colors);
+      return;
+    }
     for (int s = 0; s < prm.coarse_sweeps; ++s) smoothLines(A, x, b, (s & 1) == 1, colors);
     return;
   }
@@ -2555,6 +2650,326 @@ void Solver::vcycle(const std::vector<MGLevel>& levels, int k, double* x, const 
     }
   }
   smoothLines(A, x, b, true, colors);
+}
+
+// Lower Cholesky factor of a symmetric 3 x 3 block; false unless positive definite.
+static bool chol3(const double* D, double* L) {
+  double a = D[0];
+  if (!(a > 0)) return false;
+  L[0] = std::sqrt(a);
+  L[1] = L[2] = L[5] = 0;
+  L[3] = D[3] / L[0];
+  L[6] = D[6] / L[0];
+  double c = D[4] - L[3] * L[3];
+  if (!(c > 0)) return false;
+  L[4] = std::sqrt(c);
+  L[7] = (D[7] - L[6] * L[3]) / L[4];
+  double e = D[8] - L[6] * L[6] - L[7] * L[7];
+  if (!(e > 0)) return false;
+  L[8] = std::sqrt(e);
+  return true;
+}
+
+// Damage and contact flags of the coarsest nodes: on the fine lattice a node is damaged when a span at it
+// exists but is broken or not fully intact, in contact when contact terms act on it; a coarse node takes
+// the maximum over the fine nodes its prolongation weights reach.
+void Solver::learnedFlags(const std::vector<MGLevel>& levels) const {
+  const int F = levels[0].A->N;
+  std::vector<float> f(2 * static_cast<size_t>(F), 0.f);
+  if (F == N) {
+    bool ct = contactOn && extH.size() == 6 * static_cast<size_t>(N);
+    for (int n = 0; n < N; ++n) {
+      for (int fam = 0; fam < 2; ++fam)
+        for (int dir = -1; dir <= 1; dir += 2) {
+          int s = seg(n, fam, dir);
+          if (s >= 0 && (segFlags[s] & SEG_EXISTS) && ((segFlags[s] & SEG_BROKEN) || intact[s] < 1)) f[2 * n] = 1;
+        }
+      if (ct)
+        for (int z = 0; z < 6; ++z)
+          if (extH[6 * n + z] != 0) f[2 * n + 1] = 1;
+    }
+  }
+  for (size_t k = 0; k + 1 < levels.size(); ++k) {
+    const Prolongation& P = *levels[k].P;
+    const int Fk = levels[k].A->N, Ck = levels[k + 1].A->N;
+    std::vector<float> c(2 * static_cast<size_t>(Ck), 0.f);
+    for (int n = 0; n < Fk; ++n)
+      for (int q = 0; q < 4; ++q) {
+        int m = P.idx[4 * n + q];
+        if (m < 0 || !(P.w[4 * n + q] > 0)) continue;
+        c[2 * m] = std::max(c[2 * m], f[2 * n]);
+        c[2 * m + 1] = std::max(c[2 * m + 1], f[2 * n + 1]);
+      }
+    f.swap(c);
+  }
+  lc.flags.swap(f);
+}
+
+// The network inputs of every coarsest node (see LearnedCoarse) with the Cholesky factors of the
+// diagonal blocks; ok marks the free nodes whose block is positive definite.
+bool Solver::learnedInputs(const StencilOperator& A, std::vector<double>& L, std::vector<uint8_t>& ok,
+                           std::vector<double>& X) const {
+  const int M = A.N;
+  L.assign(9 * static_cast<size_t>(M), 0.0);
+  ok.assign(M, 0);
+  X.assign(static_cast<size_t>(M) * LC_IN, 0.0);
+  std::vector<double> tr(M, 0.0);
+  double trSum = 0;
+  int nOk = 0;
+  for (int n = 0; n < M; ++n) {
+    if (A.fixed[n]) continue;
+    const double* D = &A.A[(static_cast<size_t>(n) * STENCIL + CENTER) * 9];
+    if (!chol3(D, &L[9 * static_cast<size_t>(n)])) continue;
+    ok[n] = 1;
+    tr[n] = D[0] + D[4] + D[8];
+    trSum += tr[n];
+    nOk++;
+  }
+  if (!nOk) return false;
+  const double trMean = trSum / nOk, PI = 3.14159265358979323846;
+  const bool haveFlags = lc.flags.size() == 2 * static_cast<size_t>(M);
+  for (int n = 0; n < M; ++n) {
+    if (!ok[n]) continue;
+    double* in = &X[static_cast<size_t>(n) * LC_IN];
+    const LatticeLayer& Ly = A.layers[A.ij[3 * n + 2]];
+    double u = Ly.nx > 1 ? static_cast<double>(A.ij[3 * n]) / (Ly.nx - 1) : 0.0;
+    double v = Ly.ny > 1 ? static_cast<double>(A.ij[3 * n + 1]) / (Ly.ny - 1) : 0.0;
+    int q = 0;
+    in[q++] = u;
+    in[q++] = v;
+    for (int f = 1; f <= 2; ++f) {
+      in[q++] = std::sin(f * PI * u);
+      in[q++] = std::cos(f * PI * u);
+      in[q++] = std::sin(f * PI * v);
+      in[q++] = std::cos(f * PI * v);
+    }
+    const double* D = &A.A[(static_cast<size_t>(n) * STENCIL + CENTER) * 9];
+    in[q++] = D[0] / tr[n];
+    in[q++] = D[4] / tr[n];
+    in[q++] = D[8] / tr[n];
+    in[q++] = D[1] / tr[n];
+    in[q++] = D[2] / tr[n];
+    in[q++] = D[5] / tr[n];
+    in[q++] = std::log(tr[n] / trMean);
+    int held = 0;
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int di = -1; di <= 1; ++di) {
+        if (!di && !dj) continue;
+        int m = A.nbr(n, di, dj);
+        if (m < 0 || A.fixed[m]) held++;
+      }
+    in[q++] = held / 8.0;
+    in[q++] = haveFlags ? lc.flags[2 * n] : 0.0;
+    in[q++] = haveFlags ? lc.flags[2 * n + 1] : 0.0;
+  }
+  return true;
+}
+
+// The basis of this solve on the coarsest level: Phi = L^-T Psi from the network, A Phi, and the
+// Cholesky factor of G = Phi^T A Phi; a column whose pivot falls below 1e-10 of the largest diagonal
+// entry (dependent on the others) is dropped.
+void Solver::learnedBasis(const std::vector<MGLevel>& levels) const {
+  lc.basisOp = nullptr;
+  const StencilOperator& A = *levels.back().A;
+  const int M = A.N;
+  std::vector<double> L, X;
+  std::vector<uint8_t> ok;
+  if (!learnedInputs(A, L, ok, X)) return;
+  const size_t n3 = 3 * static_cast<size_t>(M);
+  lc.phi.assign(n3 * LC_K, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int n = 0; n < M; ++n) {
+    if (!ok[n]) continue;
+    double o[LC_OUT];
+    lcForward(lc.w.data(), &X[static_cast<size_t>(n) * LC_IN], o);
+    const double* Ln = &L[9 * static_cast<size_t>(n)];
+    for (int k = 0; k < LC_K; ++k) {  // L^T phi = psi
+      double p2 = o[3 * k + 2] / Ln[8];
+      double p1 = (o[3 * k + 1] - Ln[7] * p2) / Ln[4];
+      double p0 = (o[3 * k] - Ln[3] * p1 - Ln[6] * p2) / Ln[0];
+      lc.phi[(3 * static_cast<size_t>(n)) * LC_K + k] = p0;
+      lc.phi[(3 * static_cast<size_t>(n) + 1) * LC_K + k] = p1;
+      lc.phi[(3 * static_cast<size_t>(n) + 2) * LC_K + k] = p2;
+    }
+  }
+  std::vector<double> col(n3), Acol(n3), G(LC_K * LC_K, 0.0);
+  std::vector<std::vector<double>> AP(LC_K);
+  for (int k = 0; k < LC_K; ++k) {
+    for (size_t q = 0; q < n3; ++q) col[q] = lc.phi[q * LC_K + k];
+    A.apply(col.data(), Acol.data());
+    for (int n = 0; n < M; ++n)
+      if (A.fixed[n]) Acol[3 * n] = Acol[3 * n + 1] = Acol[3 * n + 2] = 0;
+    AP[k] = Acol;
+  }
+  for (int a = 0; a < LC_K; ++a)
+    for (int c = 0; c < LC_K; ++c) {
+      double s = 0;
+      for (size_t q = 0; q < n3; ++q) s += lc.phi[q * LC_K + a] * AP[c][q];
+      G[a * LC_K + c] = s;
+    }
+  for (int a = 0; a < LC_K; ++a)  // symmetrise
+    for (int c = 0; c < a; ++c) G[a * LC_K + c] = G[c * LC_K + a] = 0.5 * (G[a * LC_K + c] + G[c * LC_K + a]);
+  double gmax = 0;
+  for (int a = 0; a < LC_K; ++a) gmax = std::max(gmax, G[a * LC_K + a]);
+  if (!(gmax > 0) || !std::isfinite(gmax)) return;
+  lc.dead.assign(LC_K, 0);
+  for (int j = 0; j < LC_K; ++j) {
+    double d = G[j * LC_K + j];
+    for (int q = 0; q < j; ++q) d -= G[j * LC_K + q] * G[j * LC_K + q];
+    if (!(d > 1e-10 * gmax)) {
+      lc.dead[j] = 1;
+      for (int i = j; i < LC_K; ++i) G[i * LC_K + j] = 0;
+      G[j * LC_K + j] = 1;
+      continue;
+    }
+    d = std::sqrt(d);
+    G[j * LC_K + j] = d;
+    for (int i = j + 1; i < LC_K; ++i) {
+      double v = G[i * LC_K + j];
+      for (int q = 0; q < j; ++q) v -= G[i * LC_K + q] * G[j * LC_K + q];
+      G[i * LC_K + j] = v / d;
+    }
+  }
+  lc.G = G;
+  lc.basisOp = &A;
+}
+
+// The learned coarse space on the coarsest level k, half-way through its sweeps (see LearnedCoarse):
+// logs the training material when logging, adds the Galerkin correction on the basis when active.
+void Solver::learnedCorrection(const std::vector<MGLevel>& levels, int k, double* x, const double* b) const {
+  const StencilOperator& A = *levels[k].A;
+  const int M = A.N;
+  const size_t n3 = 3 * static_cast<size_t>(M);
+  std::vector<double> r(n3);
+  A.apply(x, r.data());
+  for (int n = 0; n < M; ++n)
+    for (int q = 0; q < 3; ++q) r[3 * n + q] = A.fixed[n] ? 0.0 : b[3 * n + q] - r[3 * n + q];
+
+  if (lc.log && lc.calls.size() < lc.logCap) {
+    if (lc.denseOp.get() != &A) {  // a new coarsest operator: dense whitened copy and its factor
+      lc.denseOp = levels[k].A;
+      std::vector<double> X;
+      std::vector<uint8_t> ok;
+      lc.denseOk = learnedInputs(A, lc.nodeL, ok, X);
+      lc.denseFree.assign(M, -1);
+      int nf = 0;
+      for (int n = 0; n < M; ++n) {
+        if (A.fixed[n]) continue;
+        if (!ok[n]) lc.denseOk = false;
+        lc.denseFree[n] = nf++;
+      }
+      const size_t D3 = 3 * static_cast<size_t>(nf);
+      lc.denseDim = D3;
+      lc.denseOk = lc.denseOk && nf > 0 && D3 <= 6000;
+      lc.denseL.assign(lc.denseOk ? D3 * D3 : 0, 0.0);
+      if (lc.denseOk) {
+        double* Dm = lc.denseL.data();
+        const double* NL = lc.nodeL.data();
+        // whitened blocks L_n^-1 B L_m^-T
+        for (int n = 0; n < M; ++n) {
+          int a = lc.denseFree[n];
+          if (a < 0) continue;
+          for (int dj = -2; dj <= 2; ++dj)
+            for (int di = -2; di <= 2; ++di) {
+              int m = A.nbr(n, di, dj);
+              if (m < 0 || lc.denseFree[m] < 0) continue;
+              const double* B = &A.A[(static_cast<size_t>(n) * STENCIL + offsetIndex(di, dj)) * 9];
+              const double *Ln = &NL[9 * static_cast<size_t>(n)], *Lm = &NL[9 * static_cast<size_t>(m)];
+              double T[9], W[9];
+              for (int c = 0; c < 3; ++c) {  // T = L_n^-1 B, column c
+                T[c] = B[c] / Ln[0];
+                T[3 + c] = (B[3 + c] - Ln[3] * T[c]) / Ln[4];
+                T[6 + c] = (B[6 + c] - Ln[6] * T[c] - Ln[7] * T[3 + c]) / Ln[8];
+              }
+              for (int rr = 0; rr < 3; ++rr) {  // W = T L_m^-T: row rr solves L_m w = T[rr]
+                W[3 * rr] = T[3 * rr] / Lm[0];
+                W[3 * rr + 1] = (T[3 * rr + 1] - Lm[3] * W[3 * rr]) / Lm[4];
+                W[3 * rr + 2] = (T[3 * rr + 2] - Lm[6] * W[3 * rr] - Lm[7] * W[3 * rr + 1]) / Lm[8];
+              }
+              for (int rr = 0; rr < 3; ++rr)
+                for (int cc = 0; cc < 3; ++cc) Dm[(3 * a + rr) * D3 + 3 * lc.denseFree[m] + cc] = W[3 * rr + cc];
+            }
+        }
+        LearnedOp op;
+        op.nodes = nf;
+        op.At.assign(Dm, Dm + D3 * D3);
+        for (int n = 0; n < M; ++n)
+          if (lc.denseFree[n] >= 0) op.X.insert(op.X.end(), &X[static_cast<size_t>(n) * LC_IN], &X[static_cast<size_t>(n + 1) * LC_IN]);
+        lc.ops.push_back(std::move(op));
+        for (size_t j = 0; j < D3 && lc.denseOk; ++j) {  // in-place lower Cholesky of the whitened operator
+          double d = Dm[j * D3 + j];
+          for (size_t q = 0; q < j; ++q) d -= Dm[j * D3 + q] * Dm[j * D3 + q];
+          if (!(d > 0)) {
+            lc.denseOk = false;
+            lc.ops.pop_back();
+            break;
+          }
+          d = std::sqrt(d);
+          Dm[j * D3 + j] = d;
+#pragma omp parallel for schedule(static)
+          for (size_t i = j + 1; i < D3; ++i) {
+            double v = Dm[i * D3 + j];
+            for (size_t q = 0; q < j; ++q) v -= Dm[i * D3 + q] * Dm[j * D3 + q];
+            Dm[i * D3 + j] = v / d;
+          }
+        }
+      }
+    }
+    if (lc.denseOk) {
+      const size_t D3 = lc.denseDim;
+      const double* Dm = lc.denseL.data();
+      LearnedCall call;
+      call.op = static_cast<int>(lc.ops.size()) - 1;
+      call.r.assign(D3, 0.0);
+      for (int n = 0; n < M; ++n) {
+        int a = lc.denseFree[n];
+        if (a < 0) continue;
+        const double* Ln = &lc.nodeL[9 * static_cast<size_t>(n)];
+        const double* rn = &r[3 * n];
+        double* g = &call.r[3 * a];
+        g[0] = rn[0] / Ln[0];
+        g[1] = (rn[1] - Ln[3] * g[0]) / Ln[4];
+        g[2] = (rn[2] - Ln[6] * g[0] - Ln[7] * g[1]) / Ln[8];
+      }
+      std::vector<double> d(call.r);
+      for (size_t i = 0; i < D3; ++i) {
+        double v = d[i];
+        for (size_t q = 0; q < i; ++q) v -= Dm[i * D3 + q] * d[q];
+        d[i] = v / Dm[i * D3 + i];
+      }
+      for (size_t i = D3; i-- > 0;) {
+        double v = d[i];
+        for (size_t q = i + 1; q < D3; ++q) v -= Dm[q * D3 + i] * d[q];
+        d[i] = v / Dm[i * D3 + i];
+      }
+      call.d = std::move(d);
+      lc.calls.push_back(std::move(call));
+    }
+  }
+  if (!lc.active || lc.basisOp != &A) return;
+
+  double u[LC_K], c[LC_K];
+  for (int a = 0; a < LC_K; ++a) {
+    double s = 0;
+    for (size_t q = 0; q < n3; ++q) s += lc.phi[q * LC_K + a] * r[q];
+    u[a] = lc.dead[a] ? 0.0 : s;
+  }
+  for (int i = 0; i < LC_K; ++i) {  // G c = u with G = R R^T (R lower)
+    double v = u[i];
+    for (int q = 0; q < i; ++q) v -= lc.G[i * LC_K + q] * c[q];
+    c[i] = lc.dead[i] ? 0.0 : v / lc.G[i * LC_K + i];
+  }
+  for (int i = LC_K; i-- > 0;) {
+    double v = c[i];
+    for (int q = i + 1; q < LC_K; ++q) v -= lc.G[q * LC_K + i] * c[q];
+    c[i] = lc.dead[i] ? 0.0 : v / lc.G[i * LC_K + i];
+  }
+  for (size_t q = 0; q < n3; ++q) {
+    double s = 0;
+    for (int a = 0; a < LC_K; ++a) s += lc.phi[q * LC_K + a] * c[a];
+    x[q] += s;
+  }
+  lc.applied++;
 }
 
 // Deterministic dot product: fixed 64 chunks summed in order, independent of the thread count.
@@ -2591,6 +3006,13 @@ void Solver::pcg(const std::vector<MGLevel>& levels, const double* b, double* x,
     if (relOut) *relOut = 0;
     return;
   }
+  // learned coarse correction (extension): on for this solve until the guard trips
+  lc.active = lc.on && lc.w.size() == static_cast<size_t>(LC_WEIGHTS);
+  if (lc.active || lc.log) learnedFlags(levels);
+  if (lc.active) {
+    lc.solves++;
+    learnedBasis(levels);
+  }
   vcycle(levels, 0, z.data(), r.data());
   p = z;
   double rz = dotv(r.data(), z.data(), n);
@@ -2616,13 +3038,25 @@ void Solver::pcg(const std::vector<MGLevel>& levels, const double* b, double* x,
       it++;
       break;
     }
+    // guard: mean contraction per iteration above lc.guard after three iterations -> plain V-cycle,
+    // PCG restarted from the current iterate
+    bool restart = false;
+    if (lc.active && it + 1 >= 3) {
+      double relNow = tol > 0 ? rel : std::sqrt(dotv(r.data(), r.data(), n)) / r0;
+      if (!(std::pow(relNow, 1.0 / (it + 1)) <= lc.guard)) {
+        lc.active = false;
+        lc.fallbacks++;
+        restart = true;
+      }
+    }
     std::fill(z.begin(), z.end(), 0.0);
     vcycle(levels, 0, z.data(), r.data());
     double rz2 = dotv(r.data(), z.data(), n);
-    double beta = rz2 / rz;
+    double beta = restart ? 0.0 : rz2 / rz;
     rz = rz2;
     for (size_t q = 0; q < n; ++q) p[q] = z[q] + beta * p[q];
   }
+  lc.active = false;
   if (tol <= 0 && r0 > 0) rel = std::sqrt(dotv(r.data(), r.data(), n)) / r0;
   if (done) *done = it;
   if (relOut) *relOut = rel;
@@ -3141,5 +3575,73 @@ double ora_field_share_cap(int32_t reach, double mu, double n0, double wrap, dou
 }
 // SHARE_FRACTION, DAMAGE_CUT, DAMAGE_PULLED
 void ora_field_constants(double* out3) { out3[0] = SHARE_FRACTION, out3[1] = DAMAGE_CUT, out3[2] = DAMAGE_PULLED; }
+
+// Learned coarse correction (extension; no counterpart in the reference).
+int32_t ora_learned_size(void) { return LC_WEIGHTS; }
+int32_t ora_learned_dims(int32_t* in_hidden_basis) {
+  in_hidden_basis[0] = LC_IN, in_hidden_basis[1] = LC_HID, in_hidden_basis[2] = LC_K;
+  return 0;
+}
+int ora_learned_set(ora_solver* o, const double* w, int32_t count, int32_t on, double guard) {
+  if (!o || (on && (!w || count != LC_WEIGHTS))) {
+    g_err = "ora_learned_set: weights must hold ora_learned_size() values";
+    return -1;
+  }
+  if (w && count == LC_WEIGHTS) o->s.lc.w.assign(w, w + LC_WEIGHTS);
+  o->s.lc.on = on != 0;
+  o->s.lc.guard = guard;
+  return 0;
+}
+int ora_learned_log(ora_solver* o, int32_t on, int64_t capacity) {
+  auto& lc = o->s.lc;
+  lc.log = on != 0;
+  lc.logCap = capacity > 0 ? static_cast<size_t>(capacity) : 0;
+  lc.ops.clear();
+  lc.calls.clear();
+  lc.denseOp.reset();
+  lc.denseL.clear();
+  return 0;
+}
+int32_t ora_learned_ops(ora_solver* o) { return static_cast<int32_t>(o->s.lc.ops.size()); }
+int32_t ora_learned_op_nodes(ora_solver* o, int32_t k) {
+  if (k < 0 || k >= static_cast<int32_t>(o->s.lc.ops.size())) {
+    g_err = "ora_learned_op_nodes: operator out of range";
+    return -1;
+  }
+  return o->s.lc.ops[k].nodes;
+}
+int ora_learned_op(ora_solver* o, int32_t k, double* At, double* X) {
+  if (k < 0 || k >= static_cast<int32_t>(o->s.lc.ops.size())) {
+    g_err = "ora_learned_op: operator out of range";
+    return -1;
+  }
+  const LearnedOp& op = o->s.lc.ops[k];
+  std::copy(op.At.begin(), op.At.end(), At);
+  std::copy(op.X.begin(), op.X.end(), X);
+  return 0;
+}
+int32_t ora_learned_calls(ora_solver* o) { return static_cast<int32_t>(o->s.lc.calls.size()); }
+int ora_learned_call(ora_solver* o, int32_t q, int32_t* op, double* r, double* d) {
+  if (q < 0 || q >= static_cast<int32_t>(o->s.lc.calls.size())) {
+    g_err = "ora_learned_call: call out of range";
+    return -1;
+  }
+  const LearnedCall& c = o->s.lc.calls[q];
+  *op = c.op;  // r and d may be null to ask for the operator (and so the size) first
+  if (r) std::copy(c.r.begin(), c.r.end(), r);
+  if (d) std::copy(c.d.begin(), c.d.end(), d);
+  return 0;
+}
+int ora_learned_stats(ora_solver* o, int64_t* applied_fallbacks_solves) {
+  applied_fallbacks_solves[0] = o->s.lc.applied;
+  applied_fallbacks_solves[1] = o->s.lc.fallbacks;
+  applied_fallbacks_solves[2] = o->s.lc.solves;
+  return 0;
+}
+int ora_learned_forward(const double* w, const double* X, int64_t rows, double* out) {
+#pragma omp parallel for schedule(static)
+  for (int64_t q = 0; q < rows; ++q) lcForward(w, X + q * LC_IN, out + q * LC_OUT);
+  return 0;
+}
 
 }  // extern "C"

@@ -103,6 +103,27 @@ int ora_vcycle(ora_solver* s, const double* b, double* z);
 int ora_pcg(ora_solver* s, const double* b, double* x, int32_t iterations, double rel_tol, int32_t* done,
             double* rel_residual);
 
+/* Learned coarse correction (extension; no counterpart in the reference): a learned coarse space on the
+   coarsest V-cycle level. A 20-64-64-24 tanh MLP maps each coarsest node's inputs (lattice position with
+   sin/cos features, its normalised diagonal block, fixed-neighbour fraction, damage and contact flags)
+   to 8 basis values per coordinate; half-way through the coarsest sweeps the V-cycle adds the Galerkin
+   correction on that basis. A solve whose mean contraction per iteration exceeds `guard` after three
+   iterations restarts from its iterate with the plain V-cycle. Weights W1[20][64], b1, W2[64][64], b2,
+   W3[64][24], b3, row-major [in][out]. Logging keeps, per coarsest operator, its whitened dense form
+   over the free unknowns and the node inputs, and per call the whitened residual and exact correction
+   (the training material). */
+int32_t ora_learned_size(void);
+int32_t ora_learned_dims(int32_t* in_hidden_basis);
+int ora_learned_set(ora_solver* s, const double* weights, int32_t count, int32_t on, double guard);
+int ora_learned_log(ora_solver* s, int32_t on, int64_t capacity_calls);
+int32_t ora_learned_ops(ora_solver* s);
+int32_t ora_learned_op_nodes(ora_solver* s, int32_t k);
+int ora_learned_op(ora_solver* s, int32_t k, double* At, double* X);
+int32_t ora_learned_calls(ora_solver* s);
+int ora_learned_call(ora_solver* s, int32_t q, int32_t* op, double* r, double* d);
+int ora_learned_stats(ora_solver* s, int64_t* applied_fallbacks_solves);
+int ora_learned_forward(const double* weights, const double* X, int64_t rows, double* out);
+
 /* Block pentadiagonal solve (newtonMultigrid.ts:435-473). */
 int ora_solve_penta(int32_t n, const double* D, const double* E, const double* F, const double* r, double* x,
                     double shift);
