@@ -122,7 +122,29 @@ def config1(seed=11):
     1000 % strain); inside, each yarn segment at a crossing breaks at a strain drawn from
     lognormal(ln 0.08, 0.25), its field strength the tension T(eps) = EA eps of the linear law.
     Returns the scene and the two grips: the edge columns i = 0, 1 and i = n - 2, n - 1."""
-    c = CONFIG1
+    return _yarn_region_patch(CONFIG1, seed)
+
+
+# Learned coarse correction: the tearing patch - CONFIG1's yarn lattice at 256 x 256 over 0.6 m (the
+# same pitch), a central 64 x 64-cell region of lognormal break strains, self-contact on, the two
+# edge grips pulled apart at 0.5 m/s; the network (3 layers, hidden 64) guarded at a mean contraction
+# of 0.9 per PCG iteration.
+CONFIG4 = dict(CONFIG1, n=256, size=0.6, region=64, grip_speed=0.5, self_contact=True, hidden=64, guard=0.9)
+
+
+def config4(seed=41, n=None, region=None):
+    """CONFIG4's scene and grips as config1 returns them; n and region scale it down at the same pitch
+    (a 64 x 64 patch with a 16 x 16-cell region keeps its proportions)."""
+    c = dict(CONFIG4)
+    if n is not None:
+        c["size"] = c["size"] / (c["n"] - 1) * (n - 1)
+        c["n"] = n
+    if region is not None:
+        c["region"] = region
+    return _yarn_region_patch(c, seed)
+
+
+def _yarn_region_patch(c, seed):
     n, bu, bv = c["n"], c["bundle"][0], c["bundle"][1]
     pitch = c["size"] / (n - 1)
     m = yarn_material(pitch / bu, c["yarn_ea"], c["yarn_bending"], c["crossing_friction"])

@@ -10,8 +10,11 @@ off or only logging; what the trained network gains over the method without it o
 and the guard that falls back to plain Galerkin MG-PCG when a solve does not contract.
 
 Scenes: the plain configuration's 64 x 64 hanging patch (0.3 m, dt 1/60, 4 projected-Newton
-iterations, lagged 3-level hierarchy, rel-res 1e-6), seeded jitter; training on seed 1, evaluation on
-seed 2."""
+iterations, lagged 3-level hierarchy, rel-res 1e-6), seeded jitter, training on seed 1 and evaluation
+on seed 2, also with the hierarchy rebuilt every Newton iteration; and configuration 4's tearing patch
+scaled down to 64 x 64 at its pitch (16 x 16-cell yarn region of lognormal break strains, self-contact,
+edge grips pulled apart at 0.5 m/s), training on seed 41 together with the hanging patch's material,
+evaluation on seed 42."""
 import numpy as np
 import pytest
 
@@ -49,6 +52,48 @@ def trained(logged):
     ops, calls = logged
     w, hist = L.train(ops, calls, steps=500)
     return w, hist
+
+
+C4 = configs.CONFIG4
+
+
+def tearing(seed, substeps, weights=None, log=False):
+    """Configuration 4 scaled to 64 x 64 on the oracle: the two edge grips move apart at its speed."""
+    sc, left, right = configs.config4(seed, n=64, region=16)
+    o = Oracle(sc, h=C4["h"], newton_iterations=4, pcg_iterations=500, pcg_rel_tol=1e-6, max_coarsest_nodes=400,
+               coarse_sweeps=2, line_colors=3, lag_coarse=True, line_search=True, self_contact=True)
+    if weights is not None:
+        o.set_learned(weights, on=True, guard=C4["guard"])
+    if log:
+        o.learned_log(True, 4000)
+    x0 = o.x
+    grips = [(int(nodes[len(nodes) // 2]), sign) for nodes, sign in ((left, -1.0), (right, 1.0))]
+    for (picked, _), nodes in zip(grips, (left, right)):
+        o.add_grip(nodes, np.ones(len(nodes)), (x0[nodes] - x0[picked]).reshape(-1), x0[picked], C4["grip_stiffness"])
+    its, rel = [], []
+    for s in range(1, substeps + 1):
+        for g, (picked, sign) in enumerate(grips):
+            o.set_grip_goal(g, x0[picked] + np.array([sign * 0.5 * C4["grip_speed"] * s * C4["h"], 0, 0]))
+        o.predict()
+        for _ in range(4):
+            r = o.newton_step()
+            its.append(r["pcg_iterations"])
+            rel.append(r["rel_residual"])
+        o.finalize()
+        o.update_damage()
+    return o, np.array(its), np.array(rel)
+
+
+@pytest.fixture(scope="module")
+def trained_mix(logged):
+    """Trained on the hanging patch's material and a tearing patch's (seed 41)."""
+    o, _, _ = tearing(41, 8, log=True)
+    ops4, calls4 = o.learned_samples()
+    ops0, calls0 = logged
+    ops = ops0 + ops4
+    calls = calls0 + [(op + len(ops0), r, d) for op, r, d in calls4]
+    w, _ = L.train(ops, calls, steps=800)
+    return w
 
 
 def test_dimensions():
@@ -138,3 +183,28 @@ def test_guard_falls_back_to_plain_mg_pcg(trained):
     s = o.learned_stats()
     assert s["fallbacks"] == s["solves"] == len(its)
     assert rel.max() <= 1e-6
+
+
+def test_trained_network_gains_with_a_fresh_hierarchy(trained):
+    """Trained on the lagged hierarchy's material, used with the hierarchy rebuilt every Newton iteration."""
+    w, _ = trained
+    sc = configs.hanging_patch(64, 0.3, seed=2)
+    p = dict(P, lag_coarse=False)
+    plain, learn = Oracle(sc, **p), Oracle(sc, **p)
+    learn.set_learned(w, on=True, guard=0.9)
+    ip, _ = run(plain, 3)
+    il, rl = run(learn, 3)
+    print(f"fresh hierarchy: plain {ip.mean():.2f}, learned {il.mean():.2f} PCG iterations per Newton step")
+    assert il.mean() <= 0.8 * ip.mean()
+    assert rl.max() <= 1e-6
+
+
+def test_tearing_patch_gains_on_a_held_out_seed(trained_mix):
+    o_p, ip, rp = tearing(42, 8)
+    o_l, il, rl = tearing(42, 8, weights=trained_mix)
+    broken_p, broken_l = o_p.counts()[0], o_l.counts()[0]
+    print(f"tearing patch: plain {ip.mean():.2f}, learned {il.mean():.2f} PCG iterations per Newton step; "
+          f"{o_l.learned_stats()}; spans broken {broken_p} / {broken_l}")
+    assert broken_p > 0  # the patch tears within these substeps
+    assert il.mean() <= 0.95 * ip.mean()
+    assert rp.max() <= 1e-6 and rl.max() <= 1e-6
