@@ -560,6 +560,9 @@ def main():
     }
     if variants is not None:
         line["config"]["mg_variants"] = variants
+    # the metric's learned arm: the learned coarse space runs in the FP64 oracle only (its CUDA kernels
+    # are not built), so this line measures the plain MG-PCG path
+    line["config"]["learned_arm"] = "not on the CUDA path: this value is plain MG-PCG"
     if w.get("product"):
         line["config"]["ms_per_substep"] = ms_step
         line["config"]["reference_published"] = {
