@@ -208,3 +208,18 @@ def test_tearing_patch_gains_on_a_held_out_seed(trained_mix):
     assert broken_p > 0  # the patch tears within these substeps
     assert il.mean() <= 0.95 * ip.mean()
     assert rp.max() <= 1e-6 and rl.max() <= 1e-6
+
+
+def test_headline_size_with_a_fresh_hierarchy(trained):
+    """The 256 x 256 hanging patch (0.6 m, 5 levels, coarsest 17 x 17), hierarchy rebuilt every Newton
+    iteration, with the network trained on the 64 x 64 patch's material."""
+    w, _ = trained
+    sc = configs.hanging_patch(256, 0.6, seed=1)
+    p = dict(P, lag_coarse=False)
+    plain, learn = Oracle(sc, **p), Oracle(sc, **p)
+    learn.set_learned(w, on=True, guard=0.9)
+    ip, _ = run(plain, 2)
+    il, rl = run(learn, 2)
+    print(f"256 x 256, fresh hierarchy: plain {ip.mean():.2f}, learned {il.mean():.2f} PCG iterations per Newton step")
+    assert il.mean() <= 0.8 * ip.mean()
+    assert rl.max() <= 1e-6
