@@ -106,8 +106,9 @@ def loss_grad(w, ops, calls):
     return total / m, g
 
 
-def train(ops, calls, steps=600, batch_ops=4, lr=3e-3, seed=0, w=None):
-    """Adam over minibatches of logged operators (all calls of each); returns (weights, loss every 50 steps)."""
+def train(ops, calls, steps=600, batch_ops=4, lr=3e-3, seed=0, w=None, op_weights=None):
+    """Adam over minibatches of logged operators (all calls of each), drawn uniformly or in proportion to
+    op_weights (one per operator); returns (weights, loss every 50 steps)."""
     rng = np.random.default_rng(seed)
     w = init(seed) if w is None else w.copy()
     m, v = np.zeros_like(w), np.zeros_like(w)
@@ -118,7 +119,11 @@ def train(ops, calls, steps=600, batch_ops=4, lr=3e-3, seed=0, w=None):
     keys = sorted(by_op)
     hist = []
     for t in range(1, steps + 1):
-        pick = rng.choice(len(keys), min(batch_ops, len(keys)), replace=False)
+        prob = None
+        if op_weights is not None:
+            prob = np.array([op_weights[k] for k in keys], np.float64)
+            prob /= prob.sum()
+        pick = rng.choice(len(keys), min(batch_ops, len(keys)), replace=False, p=prob)
         batch = [c for k in pick for c in by_op[keys[k]]]
         loss, g = loss_grad(w, ops, batch)
         m = b1 * m + (1 - b1) * g

@@ -223,3 +223,26 @@ def test_headline_size_with_a_fresh_hierarchy(trained):
     print(f"256 x 256, fresh hierarchy: plain {ip.mean():.2f}, learned {il.mean():.2f} PCG iterations per Newton step")
     assert il.mean() <= 0.8 * ip.mean()
     assert rl.max() <= 1e-6
+
+
+def test_committed_weights_gain_without_costing():
+    """The network trained by oracle/train_learned.py on 1.7 M node pairs logged by the plain solver on
+    configurations 0, 1, 3 and 4 (tests/golden/learned_coarse.npy): fewer PCG iterations per Newton step
+    on the held-out hanging patch, lagged or rebuilt hierarchy, and none more on the held-out tearing
+    patch."""
+    import os
+    w = np.load(os.path.join(os.path.dirname(__file__), "golden", "learned_coarse.npy")).astype(np.float64)
+    assert w.shape == (L.SIZE,)
+    for lag, bound in ((True, 0.8), (False, 0.7)):
+        p = dict(P, lag_coarse=lag)
+        sc = configs.hanging_patch(64, 0.3, seed=2)
+        plain, learn = Oracle(sc, **p), Oracle(sc, **p)
+        learn.set_learned(w, on=True, guard=0.9)
+        ip, _ = run(plain, 2)
+        il, rl = run(learn, 2)
+        print(f"committed weights, hanging patch, lagged={lag}: plain {ip.mean():.2f}, learned {il.mean():.2f}")
+        assert il.mean() <= bound * ip.mean() and rl.max() <= 1e-6
+    _, ip, _ = tearing(42, 4)
+    o, il, rl = tearing(42, 4, weights=w)
+    print(f"committed weights, tearing patch: plain {ip.mean():.2f}, learned {il.mean():.2f}")
+    assert il.mean() <= 1.02 * ip.mean() and rl.max() <= 1e-6
