@@ -2598,6 +2598,18 @@ std::vector<MGLevel> Solver::buildHierarchy(std::shared_ptr<StencilOperator> fin
     std::vector<LatticeLayer> coarse;
     auto P = buildProlongation(*cur, &coarse);
     auto C = galerkin(*cur, coarse, *P);
+    if (prm.coarse_bf16)  // precision study: the coarse rows as BF16 storage would hold them
+      for (size_t q = 0; q < C->A.size(); ++q) {
+        // 2: the 24 coupling blocks only, the diagonal block kept
+        if (prm.coarse_bf16 == 2 && (q / 9) % STENCIL == CENTER) continue;
+        double& v = C->A[q];
+        float f = static_cast<float>(v);
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+        std::memcpy(&f, &u, 4);
+        v = f;
+      }
     levels.back().P = P;
     levels.push_back({C, nullptr});
     cur = C;

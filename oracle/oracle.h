@@ -40,6 +40,9 @@ typedef struct ora_params {
   int32_t cross_layer;       /* with contact on, a scene of several layers gets the cross-layer node contact of
                                 contact.wgsl in place of self-contact, as the reference does (solver.ts:364);
                                 0 keeps self-contact on every scene */
+  int32_t coarse_bf16;       /* extension (precision study): every coarse level's operator rounded to BF16
+                                (nearest, ties to even) as it is built, the next level built from the rounded one;
+                                1 all 25 blocks, 2 the 24 coupling blocks (the diagonal block kept) */
 } ora_params;
 
 typedef struct ora_solver ora_solver;
