@@ -10,7 +10,9 @@
  * reference ships no golden vectors for the solve.
  *
  * Extensions flagged as not in the reference: a PCG relative-residual stop, several grips, the
- * floor contact of the GPU shaders restated on the CPU.
+ * floor contact of the GPU shaders restated on the CPU, the learned coarse space on the coarsest
+ * V-cycle level (with its training material logging), and BF16 storage of the coarse levels as a
+ * precision study.
  */
 #ifndef BTD_ORACLE_H
 #define BTD_ORACLE_H
