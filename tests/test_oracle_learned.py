@@ -246,3 +246,27 @@ def test_committed_weights_gain_without_costing():
     o, il, rl = tearing(42, 4, weights=w)
     print(f"committed weights, tearing patch: plain {ip.mean():.2f}, learned {il.mean():.2f}")
     assert il.mean() <= 1.02 * ip.mean() and rl.max() <= 1e-6
+
+
+def test_config4_scene():
+    """Configuration 4's tearing patch at full size: 256 x 256 over 0.6 m bundled [2, 2], the central
+    64 x 64 cells' crossings with lognormal(ln 0.08, 0.25) break strains (as tensions EA eps), the rest
+    holding to 10 EA, no pins, grips on the two edge column pairs; scaled, the same pitch."""
+    c = configs.CONFIG4
+    sc, left, right = configs.config4()
+    assert (sc.nx, sc.ny) == (256, 256) and not sc.pinned.any()
+    pos = sc.position.reshape(-1, 3)
+    assert np.isclose(pos[1, 0] - pos[0, 0], 0.6 / 255, rtol=1e-4)
+    L = sc.layers[0]
+    s = sc.field_strength.reshape(L.field_m, L.field_k, 2)
+    lo = (256 - 64) // 2
+    inner = s[2 * lo:2 * (lo + 64), 2 * lo:2 * (lo + 64)]
+    eps = inner / c["yarn_ea"]
+    assert abs(np.median(np.log(eps)) - np.log(0.08)) < 0.01 and abs(np.log(eps).std() - 0.25) < 0.01
+    mask = np.ones(s.shape[:2], bool)
+    mask[2 * lo:2 * (lo + 64), 2 * lo:2 * (lo + 64)] = False
+    assert np.allclose(s[mask], 10 * c["yarn_ea"])
+    assert len(left) == len(right) == 2 * 256
+    small, _, _ = configs.config4(n=64, region=16)
+    p = small.position.reshape(-1, 3)
+    assert (small.nx, small.ny) == (64, 64) and np.isclose(p[1, 0] - p[0, 0], 0.6 / 255, rtol=1e-4)
