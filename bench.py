@@ -41,6 +41,12 @@ WORKLOADS["config2-256"] = dict(n=256, size=0.6, h=1 / 60, newton=4, rel=1e-6, c
                                 desc="configuration 2: a free 256x256-vertex sheet (0.6 m, config-0 material) folded about 1-3 seeded "
                                      "parallel lines, dropped from 0.3 m onto the floor with self-contact on (SELF_CONTACT law); "
                                      "dt 1/60, 4 projected-Newton, MG-PCG to rel-res 1e-6; timed from the drop")
+TEARING = "config4-256"
+WORKLOADS[TEARING] = dict(n=256, size=0.6, h=1 / 120, newton=4, rel=1e-6, contact=True, tearing=True,
+                          desc="configuration 4's tearing patch: the 256x256 yarn lattice (0.6 m, yarn EA 2e3 N, bending "
+                               "1e-7 N m^2, crossing friction 0.3, bundled [2, 2]) with a central 64x64-cell region of "
+                               "lognormal(ln 0.08, 0.25) break strains, self-contact on, two edge grips (columns 0-1 and "
+                               "n-2..n-1) pulled apart at 0.5 m/s; dt 1/120, 4 projected-Newton, MG-PCG to rel-res 1e-6")
 BATCH = "batch-512"
 WORKLOADS[BATCH] = dict(n=None, size=None, h=1 / 60, newton=4, rel=1e-6,
                         desc="512 independent hanging patches (the batched configuration): sides uniform in [16, 128] nodes at "
@@ -57,7 +63,7 @@ METRIC_PRODUCT = "Newton steps/s of the product scene's substep at the shipped s
 # the reference's published substep times on this scene (Apple M5, WebGPU): 2 Newton x 2 PCG 6.9 ms plus
 # 0.6 ms of self-contact (docs/decisions/2026-10-10-feedback-round2.md:11-14)
 PRODUCT_PUBLISHED_MS = 6.9 + 0.6
-DEFAULT_WORKLOAD = "hanging-256"
+DEFAULT_WORKLOAD = TEARING
 HIST_EDGES = [0, 5, 10, 15, 20, 25, 30, 40, 60, 100, 500]
 MG = dict(max_coarsest_nodes=400, coarse_sweeps=2, line_colors=3, lag_coarse=True, line_search=True)
 
@@ -72,64 +78,153 @@ def package():
     return mod
 
 
-def build_scene(btd, w):
+class Patch:
+    """The workload's scene and its grips: (nodes, sign) per grip, the grip moving along x by
+    sign * speed / 2 per second (the two edges of the tearing patch separate at `speed`)."""
+
+    def __init__(self, sc, grips=(), speed=0.0, stiffness=0.0):
+        self.sc, self.grips, self.speed, self.stiffness = sc, list(grips), speed, stiffness
+
+    @classmethod
+    def build(cls, btd, w):
+        if w.get("product"):
+            return cls(btd.compile_scene(btd.default_spec()))
+        if w.get("tearing"):
+            c = btd.configs.CONFIG4
+            sc, left, right = btd.configs.config4()
+            return cls(sc, [(left, -1.0), (right, 1.0)], c["grip_speed"], c["grip_stiffness"])
+        if w.get("contact"):
+            return cls(btd.configs.config2())
+        return cls(btd.configs.hanging_patch(w["n"], w["size"], seed=1))
+
+    def anchors(self, x0):
+        """(picked node, anchor) per grip: the middle node of its patch at its float32 position."""
+        out = []
+        for nodes, _ in self.grips:
+            picked = int(nodes[len(nodes) // 2])
+            out.append((picked, np.asarray(x0, np.float64)[picked].astype(np.float32).astype(np.float64)))
+        return out
+
+    def goals(self, anchors, s, h):
+        """Grip targets before substep s (1-based)."""
+        return [a + np.array([sign * 0.5 * self.speed * s * h, 0.0, 0.0]) for (_, a), (_, sign) in zip(anchors, self.grips)]
+
+    # the reference arm builds its scene in a child process (the scene compiler lives in the product
+    # library, which the reference arm must not map) and loads it from a file
+    def save(self, path):
+        sc = self.sc
+        arrays = {name: getattr(sc, name) for name in sc.__dict__ if isinstance(getattr(sc, name), np.ndarray)}
+        layers = np.frombuffer(b"".join(bytes(L) for L in sc.layers), np.uint8)
+        grips = {f"grip{k}": np.asarray(nodes, np.int32) for k, (nodes, _) in enumerate(self.grips)}
+        np.savez(path, _layers=layers, _meta=np.array([sc.N, sc.C, len(sc.layers), len(self.grips)], np.int64),
+                 _signs=np.array([g[1] for g in self.grips] + [0.0]), _grip=np.array([self.speed, self.stiffness]),
+                 **arrays, **grips)
+
+    @classmethod
+    def load(cls, btd, path):
+        import ctypes
+
+        d = np.load(path)
+        N, C, nl, ng = (int(v) for v in d["_meta"])
+        size = ctypes.sizeof(btd._abi.LayerInfo)
+        raw = d["_layers"].tobytes()
+        layers = [btd._abi.LayerInfo.from_buffer_copy(raw[k * size:(k + 1) * size]) for k in range(nl)]
+        arrays = {k: d[k].copy() for k in d.files if not k.startswith("_") and not k.startswith("grip")}
+        sc = btd.Scene(layers, N, C, arrays)
+        grips = [(d[f"grip{k}"], float(d["_signs"][k])) for k in range(ng)]
+        return cls(sc, grips, float(d["_grip"][0]), float(d["_grip"][1]))
+
+
+def solver_params(btd, w, settings=None):
     if w.get("product"):
-        return btd.compile_scene(btd.default_spec())
-    if w.get("contact"):
-        return btd.configs.config2()
-    return btd.configs.hanging_patch(w["n"], w["size"], seed=1)
-
-
-def solver_params(btd, w):
-    if w.get("product"):
-        return btd.default_params()
-    return btd.configs.solver_params(w["h"], w["newton"], w["rel"], self_contact=1 if w.get("contact") else 0)
-
-
-# Multigrid settings measured beside the default one: the Galerkin hierarchy rebuilt at every Newton
-# iteration instead of lagged from the first (the reference lags it, newtonMultigrid.ts:579, for its
-# fixed two PCG iterations), and that coarsened down to at most 30 nodes instead of 400. On the oracle
-# they take the PCG iterations per Newton step of the 256 x 256 hanging patch from 37 to 20 and 13,
-# and of the folded drop with self-contact at 64 x 64 from 94 to 59 and 41; each extra level costs
-# its launches in every V-cycle, so the device decides between them.
-MG_VARIANTS = (dict(lag_coarse=0), dict(lag_coarse=0, max_coarsest_nodes=30))
-
-
-def measure_variant(btd, w, sc, steps, warmup, settings):
-    """The workload's substeps with other multigrid settings: Newton steps/s from the device-timed
-    substep graph (L2 flushed before each, as the default's), PCG iterations per Newton step and the
-    level count."""
-    p = solver_params(btd, w)
-    for k, v in settings.items():
+        p = btd.default_params()
+    else:
+        p = btd.configs.solver_params(w["h"], w["newton"], w["rel"], self_contact=1 if w.get("contact") else 0)
+    for k, v in (settings or {}).items():
         setattr(p, k, v)
-    g = btd.GpuSolver(sc, p)
-    if w.get("contact"):
+    return p
+
+
+def gpu_arm(btd, w, patch, settings=None):
+    """A GpuSolver set up as the workload (floor, drape, grips) and its per-substep driver."""
+    g = btd.GpuSolver(patch.sc, solver_params(btd, w, settings))
+    if w.get("product"):
+        g.settle_drape()  # the product starts from its settled drape (drape.bin / settleDrape)
+    elif w.get("contact") and not w.get("tearing"):
         g.set_floor(btd.configs.CONFIG2["floor"])
+    anchors = patch.anchors(g.x)
+    for slot, ((nodes, _), (picked, a)) in enumerate(zip(patch.grips, anchors)):
+        g.attach_patch(slot, picked, nodes, np.ones(len(nodes)), a.astype(np.float32), patch.stiffness, max_lead=1.0)
+
+    def drive(s):
+        for slot, goal in enumerate(patch.goals(anchors, s, w["h"])):
+            g.set_target(goal.astype(np.float32), slot=slot)
+
+    return g, drive
+
+
+def timed_substeps(g, drive, first, count):
+    """Device time (ms) of `count` substeps from substep `first`, L2 flushed before each (outside the
+    CUDA events on the solver's stream); the grip targets are set before each."""
+    total = 0.0
+    for s in range(first, first + count):
+        drive(s)
+        total += g.profile_stage("substep", reps=1, flush=True)
+    return total
+
+
+# Multigrid settings measured beside the reference's schedule (hierarchy lagged from a substep's first
+# Newton iteration, newtonMultigrid.ts:579; coarsest level at most 400 nodes, solver.ts:70): the
+# Galerkin hierarchy rebuilt at every Newton iteration, and that coarsened down to at most 30 nodes.
+# On the oracle they take the PCG iterations per Newton step of the 256 x 256 hanging patch from 37 to
+# 20 and 13; each extra level costs its launches in every V-cycle, so the device decides.
+MG_VARIANTS = {"rebuilt": dict(lag_coarse=0), "rebuilt_deep": dict(lag_coarse=0, max_coarsest_nodes=30)}
+
+
+def measure_arm(btd, w, patch, steps, warmup, settings=None):
+    """The workload's substeps W + 1 .. W + K on a fresh solver with `settings`: Newton steps/s from the
+    device-timed substeps, PCG iterations per Newton step, levels and kernel launches."""
+    g, drive = gpu_arm(btd, w, patch, settings)
     try:
-        for _ in range(warmup):
+        for s in range(1, warmup + 1):
+            drive(s)
             g.substep()
         g.synchronize()
         g.clear_counters()
-        ms = g.profile_stage("substep", reps=steps, flush=True)
+        ms = timed_substeps(g, drive, warmup + 1, steps)
+        g.synchronize()
         c = g.counter_dict()
-        return {"settings": dict(settings), "levels": g.level_count(),
-                "value": c["newton"] / (ms * steps / 1e3), "unit": "Newton steps/s", "ms_per_step": ms,
-                "pcg_iterations_per_newton": c["pcg_total"] / max(1, c["newton"])}
+        return {"settings": dict(settings or {}), "levels": g.level_count(), "value": c["newton"] / (ms / 1e3),
+                "unit": "Newton steps/s", "ms_per_step": ms / steps,
+                "pcg_iterations_per_newton": c["pcg_total"] / max(1, c["newton"]),
+                "gpu_launches": int(g.launch_count(steps, c["newton"], c["pcg_total"]))}
     finally:
         g.close()
 
 
-def workload_oracle(btd, w, threads=0):
-    """The oracle configured as the workload's solve (PCG to the relative residual, or the fixed count)."""
+def workload_oracle(w, patch, threads=0):
+    """The oracle configured as the workload's solve (PCG to the relative residual, or the fixed count),
+    with the workload's floor and grips; returns it and its per-substep driver."""
     sys.path.insert(0, ROOT)
     from oracle import Oracle
 
-    sc = build_scene(btd, w)
-    o = Oracle(sc, h=w["h"], newton_iterations=w["newton"], pcg_iterations=w.get("pcg", 500), pcg_rel_tol=w["rel"],
+    o = Oracle(patch.sc, h=w["h"], newton_iterations=w["newton"], pcg_iterations=w.get("pcg", 500), pcg_rel_tol=w["rel"],
                threads=threads, self_contact=bool(w.get("contact")), **MG)
-    if w.get("contact") and not w.get("product"):
-        o.set_floor(btd.configs.CONFIG2["floor"])
-    return o
+    if w.get("contact") and not w.get("product") and not w.get("tearing"):
+        o.set_floor(CONFIG2_FLOOR)
+    x0 = o.x.astype(np.float32).astype(np.float64)
+    anchors = patch.anchors(x0)
+    for (nodes, _), (picked, a) in zip(patch.grips, anchors):
+        o.add_grip(nodes, np.ones(len(nodes)), (x0[nodes] - x0[picked]).reshape(-1), a, patch.stiffness)
+
+    def drive(s):
+        for slot, goal in enumerate(patch.goals(anchors, s, w["h"])):
+            o.set_grip_goal(slot, goal.astype(np.float32).astype(np.float64))
+
+    return o, drive
+
+
+CONFIG2_FLOOR = 0.0  # the folded drop's floor height (configs.CONFIG2["floor"])
 
 
 def peaks():
@@ -184,11 +279,12 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def cpu_sample(btd, w, substeps, threads=0):
-    """The oracle (the reference's CPU solver restated, FP64, OpenMP) on `substeps` substeps."""
-    o = workload_oracle(btd, w, threads)
+def cpu_sample(w, patch, substeps, threads=0, warmup=0):
+    """The oracle (the reference's CPU solver restated, FP64, OpenMP) on substeps warmup + 1 ..
+    warmup + substeps of the workload (the warm-up ones untimed); returns Newton steps/s, seconds, cores."""
+    o, drive = workload_oracle(w, patch, threads)
     cores = threads if threads > 0 else (os.cpu_count() or 1)
-    if w.get("contact") and not w.get("product"):
+    if w.get("contact") and not w.get("product") and not w.get("tearing"):
         # bounded sample: one Newton iteration with the contacts engaged - the first substep's second
         # (its prediction and first iteration, untimed, converge in ~50 PCG iterations; the later
         # ones, ~30 s each on 8 host cores, are the representative work)
@@ -198,8 +294,12 @@ def cpu_sample(btd, w, substeps, threads=0):
         o.newton_step()
         dt = time.perf_counter() - t
         return 1.0 / dt, dt, cores
+    for s in range(1, warmup + 1):
+        drive(s)
+        o.substep()
     t = time.perf_counter()
-    for _ in range(substeps):
+    for s in range(warmup + 1, warmup + substeps + 1):
+        drive(s)
         o.substep()
     dt = time.perf_counter() - t
     return substeps * w["newton"] / dt, dt, cores
@@ -217,10 +317,11 @@ def across_ranks(dist, values, op="max", device="cuda"):
     return [float(v) for v in t.tolist()]
 
 
-def cpu_sample_single_core(btd, w):
+def cpu_sample_single_core(w, patch):
     """The oracle on one host thread, bounded: the first substep's prediction and first Newton
     iteration of the workload (a whole substep takes tens of seconds on one core at 256 x 256)."""
-    o = workload_oracle(btd, w, threads=1)
+    o, drive = workload_oracle(w, patch, threads=1)
+    drive(1)
     t = time.perf_counter()
     o.predict()
     o.newton_step()
@@ -228,52 +329,94 @@ def cpu_sample_single_core(btd, w):
     return 1.0 / dt, dt
 
 
-def batch_cpu_sample(btd, patches=2):
-    """The oracle on the first `patches` patches of the batch, one substep each, grips held."""
+def batch_patches(btd, count):
+    """The first `count` patches of the batch with their grips, as Patch objects whose single grip moves
+    with the patch's velocity (the Patch's goals are replaced by the velocity's)."""
+    out = []
+    for sc, g in btd.configs.config3(only=list(range(count))):
+        p = Patch(sc, [(np.asarray(g["nodes"], np.int32), 0.0)], 0.0, float(g["stiffness"]))
+        p.picked, p.weights, p.velocity = int(g["picked"]), np.asarray(g["weights"], np.float64), np.asarray(g["velocity"])
+        out.append(p)
+    return out
+
+
+def batch_cpu_sample(w, patches, steps, warmup=0):
+    """The oracle on the given batch patches: substeps warmup + 1 .. warmup + steps of each (the warm-up
+    ones untimed), its grip held and moved with the patch's velocity."""
     sys.path.insert(0, ROOT)
     from oracle import Oracle
 
-    c = btd.configs.CONFIG3
-    dt = 0.0
-    newton = 0
-    for sc, g in btd.configs.config3(only=list(range(patches))):
-        o = Oracle(sc, h=c["h"], newton_iterations=c["newton_iterations"], pcg_iterations=500, pcg_rel_tol=c["pcg_rel_tol"], **MG)
+    dt, newton = 0.0, 0
+    for p in patches:
+        o = Oracle(p.sc, h=w["h"], newton_iterations=w["newton"], pcg_iterations=500, pcg_rel_tol=w["rel"], **MG)
         x = o.x
-        nodes = np.asarray(g["nodes"])
-        anchor = x[g["picked"]].copy()
-        o.add_grip(nodes, np.asarray(g["weights"], np.float64), (x[nodes] - x[g["picked"]]).reshape(-1), anchor, g["stiffness"])
-        o.set_grip_goal(0, anchor + c["h"] * g["velocity"])
-        t = time.perf_counter()
-        o.substep()
-        dt += time.perf_counter() - t
-        newton += c["newton_iterations"]
+        nodes = np.asarray(p.grips[0][0])
+        anchor = x[p.picked].copy()
+        o.add_grip(nodes, p.weights, (x[nodes] - x[p.picked]).reshape(-1), anchor, p.stiffness)
+        for s in range(1, warmup + steps + 1):
+            o.set_grip_goal(0, anchor + s * w["h"] * p.velocity)
+            t = time.perf_counter()
+            o.substep()
+            if s > warmup:
+                dt += time.perf_counter() - t
+                newton += w["newton"]
     return newton / dt, dt, os.cpu_count() or 1
 
 
+def dump_patches(args, path):
+    """Child process of the reference arm: writes the workload's patches (scene, grips) to files."""
+    btd = package()
+    w = WORKLOADS[args.workload]
+    if args.workload == BATCH:
+        for k, p in enumerate(batch_patches(btd, 2)):
+            p.save(f"{path}.{k}.npz")
+            np.savez(f"{path}.{k}.grip.npz", picked=p.picked, weights=p.weights, velocity=p.velocity)
+    else:
+        Patch.build(btd, w).save(f"{path}.0.npz")
+
+
+def load_patches(btd, args, path):
+    if args.workload != BATCH:
+        return [Patch.load(btd, f"{path}.0.npz")]
+    out = []
+    for k in range(2):
+        p = Patch.load(btd, f"{path}.{k}.npz")
+        g = np.load(f"{path}.{k}.grip.npz")
+        p.picked, p.weights, p.velocity = int(g["picked"]), g["weights"], g["velocity"]
+        out.append(p)
+    return out
+
+
 def run_reference(args, w, rank):
+    """The reference arm: the reference's CPU solver (its FP64 restatement, the oracle) on the host
+    cores, on the same workload, metric and substep window (W warm-up substeps untimed, then K timed).
+    The scenes are compiled in a child process and read from files, so that this process maps no
+    library of the product."""
     if rank != 0:
         return
+    import tempfile
+
     btd = package()
-    if args.workload == BATCH:
-        value, dt, cores = batch_cpu_sample(btd, max(1, args.steps))
-        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Newton steps/s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(1, args.steps), "higher_is_better": True,
-                "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": args.workload, "description": w["desc"]},
-                "cpu_baseline": {"value": value, "unit": "Newton steps/s", "cores": cores, "kind": "port",
-                                 "sample": f"one substep of each of the first {max(1, args.steps)} patches"},
-                "e2e": {"value": value, "unit": "Newton steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return
-    for _ in range(args.warmup):
-        pass  # the CPU solver has no warm-up state worth timing; warm-up steps run inside the sample below
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "patch")
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--workload", args.workload, "--dump-patches", path],
+                       check=True)
+        patches = load_patches(btd, args, path)
     steps = max(1, args.steps)
-    value, dt, cores = cpu_sample(btd, w, steps)
+    if args.workload == BATCH:
+        value, dt, cores = batch_cpu_sample(w, patches, steps, args.warmup)
+        sample = f"substeps {args.warmup + 1}..{args.warmup + steps} of the first {len(patches)} patches (warm-up untimed)"
+        scaling = "strong"
+    else:
+        value, dt, cores = cpu_sample(w, patches[0], steps, warmup=args.warmup)
+        sample = f"substeps {args.warmup + 1}..{args.warmup + steps} x {w['newton']} Newton of the workload (warm-up untimed)"
+        scaling = "weak"
+        if w.get("contact") and not w.get("tearing"):
+            sample = "the first substep's second Newton iteration (contacts engaged)"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Newton steps/s", "n_gpus": args.gpus, "steps": steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": scaling, "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "config": {"workload": args.workload, "description": w["desc"]},
-            "cpu_baseline": {"value": value, "unit": "Newton steps/s", "cores": cores, "kind": "port",
-                             "sample": f"{steps} substeps x {w['newton']} Newton of the workload from its initial state"},
+            "cpu_baseline": {"value": value, "unit": "Newton steps/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "Newton steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -400,7 +543,7 @@ def run_batch(args, w, rank, world, local, dist):
         "clocks": clocks.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
-        v_cpu, dt_cpu, cores = batch_cpu_sample(btd)
+        v_cpu, dt_cpu, cores = batch_cpu_sample(w, batch_patches(btd, 2), 1)
         line["cpu_baseline"] = {"value": v_cpu, "unit": "Newton steps/s", "cores": cores, "kind": "port",
                                 "sample": f"one substep of each of the first 2 patches, {dt_cpu:.1f} s"}
     print(json.dumps(line), flush=True)
@@ -422,7 +565,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--eager", action="store_true", help="launch kernel by kernel (for per-kernel profilers)")
     ap.add_argument("--patches", type=int, default=512, help="patches of the batch workload")
+    ap.add_argument("--dump-patches", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.dump_patches:
+        dump_patches(args, args.dump_patches)
+        return
     args.warmup = max(3, args.warmup)
     w = WORKLOADS[args.workload]
     rank = int(os.environ.get("RANK", "0"))
@@ -447,13 +594,9 @@ def main():
         run_batch(args, w, rank, world, local, dist)
         return
     btd = package()
-    sc = build_scene(btd, w)
-    params = solver_params(btd, w)
-    gpu = btd.GpuSolver(sc, params)
-    if w.get("product"):
-        gpu.settle_drape()  # the product starts from its settled drape (drape.bin / settleDrape)
-    elif w.get("contact"):
-        gpu.set_floor(btd.configs.CONFIG2["floor"])
+    patch = Patch.build(btd, w)
+    sc = patch.sc
+    gpu, drive = gpu_arm(btd, w, patch)
     if args.eager:
         gpu.set_graph_mode(False)
 
@@ -463,55 +606,37 @@ def main():
         torch.cuda.synchronize()
         gpu.synchronize()
 
-    # warm-up (captures the substep graph, fills caches)
-    for _ in range(args.warmup):
+    # warm-up: substeps 1..W (captures the substep graph, fills caches)
+    for s in range(1, args.warmup + 1):
+        drive(s)
         gpu.substep()
     gpu.synchronize()
     gpu.clear_counters()
 
-    # ---- device-timed region: K substeps, cold L2 before each (flush outside the events)
+    # ---- device-timed region: substeps W + 1 .. W + K, cold L2 before each (flush outside the events)
     barrier()
     idx = local
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     if vis:
         idx = vis.split(",")[local]
     with ClockSampler(idx) as clocks:
-        ms_step = gpu.profile_stage("substep", reps=args.steps, flush=True)
+        ms_total = timed_substeps(gpu, drive, args.warmup + 1, args.steps)
         barrier()
+    ms_step = ms_total / args.steps
     c = gpu.counter_dict()
     newton_total = c["newton"]
     pcg_total = c["pcg_total"]
-    t_dev = ms_step * args.steps / 1e3
+    t_dev = ms_total / 1e3
     if dist is not None:
         t_dev = across_ranks(dist, [t_dev], "max")[0]
     value = world * newton_total / t_dev
     launches = gpu.launch_count(args.steps, newton_total, pcg_total)
+    levels = gpu.level_count()
 
-    # ---- end to end through the C ABI from pinned host buffers: state in, substep, state out
-    N = sc.N
-    xh = torch.empty((N, 4), dtype=torch.float32, pin_memory=True)
-    vh = torch.empty((N, 4), dtype=torch.float32, pin_memory=True)
-    lib = btd._abi.lib()
-    h = gpu._h
-    btd._abi.check("btd_get_state", h, xh.data_ptr(), vh.data_ptr())
-    gpu.clear_counters()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        btd._abi.check("btd_set_state", h, xh.data_ptr(), vh.data_ptr())
-        btd._abi.check("btd_substep", h, 0, 0)
-        btd._abi.check("btd_get_state", h, xh.data_ptr(), vh.data_ptr())
-    barrier()
-    t_e2e = time.perf_counter() - t0
-    cd_e2e = gpu.counter_dict()
-    newton_e2e = cd_e2e["newton"]
-    pcg_e2e = cd_e2e["pcg_total"] / max(1, cd_e2e["newton"])
-    if dist is not None:
-        t_e2e = across_ranks(dist, [t_e2e], "max")[0]
-    e2e = world * newton_e2e / t_e2e
-
-    # ---- roofline of the dominant kernel (fine-level smoother sweep), live, cold L2 per launch
+    # ---- roofline of the dominant kernel (fine-level smoother sweep), live, cold L2 per launch, on the
+    # system of the last timed substep
     peak, peak_kind = peaks()
+    N = sc.N
     R0 = 232.0  # fine row algorithmic bytes
     ms_sweep = gpu.profile_stage("smooth", reps=10, flush=True)
     bytes_sweep = 2.0 * N * (R0 + 36.0)
@@ -525,15 +650,46 @@ def main():
             traffic = json.load(open(tpath)).get(args.workload, {}).get("smooth_sweep_dram_bytes")
         except Exception:
             traffic = None
+    gpu.close()
 
+    # ---- end to end through the C ABI from pinned host buffers: the state in (the previous step's
+    # output), the grip targets, one substep, the state out; substeps W + 1 .. W + K of a fresh solver
+    g2, drive2 = gpu_arm(btd, w, patch)
+    for s in range(1, args.warmup + 1):
+        drive2(s)
+        g2.substep()
+    xh = torch.empty((N, 4), dtype=torch.float32, pin_memory=True)
+    vh = torch.empty((N, 4), dtype=torch.float32, pin_memory=True)
+    h = g2._h
+    btd._abi.check("btd_get_state", h, xh.data_ptr(), vh.data_ptr())
+    g2.synchronize()
+    g2.clear_counters()
+    barrier()
+    t0 = time.perf_counter()
+    for s in range(args.warmup + 1, args.warmup + args.steps + 1):
+        btd._abi.check("btd_set_state", h, xh.data_ptr(), vh.data_ptr())
+        drive2(s)
+        btd._abi.check("btd_substep", h, 0, 0)
+        btd._abi.check("btd_get_state", h, xh.data_ptr(), vh.data_ptr())
+    barrier()
+    t_e2e = time.perf_counter() - t0
+    cd_e2e = g2.counter_dict()
+    g2.close()
+    newton_e2e = cd_e2e["newton"]
+    pcg_e2e = cd_e2e["pcg_total"] / max(1, cd_e2e["newton"])
+    if dist is not None:
+        t_e2e = across_ranks(dist, [t_e2e], "max")[0]
+    e2e = world * newton_e2e / t_e2e
+
+    # ---- other multigrid settings on the same substep window (one GPU only)
     variants = None
     if world == 1 and not w.get("product"):
-        variants = []
-        for settings in MG_VARIANTS:
+        variants = {}
+        for name, settings in MG_VARIANTS.items():
             try:
-                variants.append(measure_variant(btd, w, sc, args.steps, args.warmup, settings))
+                variants[name] = measure_arm(btd, w, patch, args.steps, args.warmup, settings)
             except Exception as e:  # reported, never fatal to the default measurement
-                variants.append({"settings": dict(settings), "error": f"{type(e).__name__}: {e}"})
+                variants[name] = {"settings": dict(settings), "error": f"{type(e).__name__}: {e}"}
 
     if rank != 0:
         if dist is not None:
@@ -544,13 +700,15 @@ def main():
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": args.workload, "description": w["desc"], "nodes": N, "levels": gpu.level_count(),
+        "config": {"workload": args.workload, "description": w["desc"], "nodes": N, "levels": None,
                    "newton_per_step": w["newton"], "pcg_iterations_per_newton": pcg_total / max(1, newton_total),
+                   "substeps_timed": [args.warmup + 1, args.warmup + args.steps],
                    "l2": "flushed before every timed step (256 MiB rewrite outside the events)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e, "unit": "Newton steps/s", "h2d_bytes_per_step": 2 * 16 * N, "d2h_bytes_per_step": 2 * 16 * N,
                 "pcg_iterations_per_newton": pcg_e2e,
-                "loop": "each step: the state in from pinned host memory (the previous step's output), one substep, the state out"},
+                "loop": "each step: the state in from pinned host memory (the previous step's output), the grip targets, "
+                        "one substep, the state out"},
         "gpu_launches": int(launches),
         "roofline": {"kernel": "k_smooth<FineRows> (fine yarn-line sweep, 6 colour launches)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
@@ -558,10 +716,9 @@ def main():
                      "matvec_gbs": mv_gbs, "matvec_ms": ms_mv},
         "clocks": clocks.summary(),
     }
+    line["config"]["levels"] = levels
     if variants is not None:
         line["config"]["mg_variants"] = variants
-    # the metric's learned arm: the learned coarse space runs in the FP64 oracle only (its CUDA kernels
-    # are not built), so this line measures the plain MG-PCG path
     line["config"]["learned_arm"] = "not on the CUDA path: this value is plain MG-PCG"
     if w.get("product"):
         line["config"]["ms_per_substep"] = ms_step
@@ -570,13 +727,13 @@ def main():
             "source": "docs/decisions/2026-10-10-feedback-round2.md:11-14 (2 Newton x 2 PCG 6.9 ms + self-contact 0.6 ms)",
             "substep_time_ratio": PRODUCT_PUBLISHED_MS / ms_step}
     if world == 1 and not args.no_cpu_baseline:
-        v_cpu, dt_cpu, cores = cpu_sample(btd, w, 1)
+        v_cpu, dt_cpu, cores = cpu_sample(w, patch, 1)
         what = ("the first substep's second Newton iteration (contacts engaged)" if w.get("contact") and not w.get("product")
-                else f"1 substep ({w['newton']} Newton) of the workload from its initial state")
+                and not w.get("tearing") else f"substep 1 ({w['newton']} Newton) of the workload from its initial state")
         line["cpu_baseline"] = {"value": v_cpu, "unit": "Newton steps/s", "cores": cores, "kind": "port",
                                 "sample": f"{what}, {dt_cpu:.1f} s"}
-        if not w.get("contact") or w.get("product"):
-            v1, dt1 = cpu_sample_single_core(btd, w)
+        if not w.get("contact") or w.get("product") or w.get("tearing"):
+            v1, dt1 = cpu_sample_single_core(w, patch)
             line["cpu_baseline_single_core"] = {"value": v1, "unit": "Newton steps/s", "cores": 1, "kind": "port",
                                                 "sample": f"the first substep's prediction and first Newton iteration, {dt1:.1f} s"}
     print(json.dumps(line), flush=True)

@@ -208,6 +208,7 @@ SIGNATURES = {
     "btd_set_grip_hold": ([C.c_void_p, C.c_int32, C.c_float], C.c_int),
     "btd_release_grip": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_read_grip": ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, _p(C.c_int32)], C.c_int),
+    "btd_set_wait_bound": ([C.c_int32], C.c_int),
     "btd_last_error": ([C.c_char_p, C.c_size_t], C.c_int),
 }
 

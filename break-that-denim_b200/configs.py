@@ -63,13 +63,15 @@ def shell_material(pitch, stretch=(8e3, 4e3), shear=200.0, bending=1e-5, areal_d
 
 
 def hanging_patch(n, size=0.3, seed=1, jitter=1e-4, **mat):
-    """An n x n shell patch, top row (j = n - 1) pinned, flat plus N(0, jitter) on free coordinates."""
-    pitch = size / (n - 1)
+    """An n x n shell patch (n = (nx, ny): nx x ny at the pitch size / (nx - 1)), top row (j = ny - 1)
+    pinned, flat plus N(0, jitter) on free coordinates."""
+    nx, ny = (n, n) if np.isscalar(n) else (int(n[0]), int(n[1]))
+    pitch = size / (nx - 1)
     m = shell_material(pitch, **mat)
-    sc = compile_scene(layer_spec(m, (n - 0.5) * pitch, (n - 0.5) * pitch, collar_rows=0, seed=seed))
-    assert sc.nx == n and sc.ny == n, (sc.nx, sc.ny)
-    pinned = np.zeros((n, n), np.uint8)
-    pinned[n - 1, :] = 1
+    sc = compile_scene(layer_spec(m, (nx - 0.5) * pitch, (ny - 0.5) * pitch, collar_rows=0, seed=seed))
+    assert sc.nx == nx and sc.ny == ny, (sc.nx, sc.ny)
+    pinned = np.zeros((ny, nx), np.uint8)
+    pinned[ny - 1, :] = 1
     sc.pinned[:] = pinned.reshape(-1)
     free = sc.pinned == 0
     pos = sc.position.reshape(-1, 3)

@@ -141,13 +141,20 @@ __device__ __forceinline__ bool mbarTryWait(uint64_t* bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for phase `parity` of an mbarrier (each try suspends the thread for a while). If it
-// runs out, the error flag is raised and the wait is given a second bound, so the CTA does not exit
-// with its copies in flight; either way the kernel goes on (with garbage, flagged) instead of hanging.
+// Bounded wait for phase `parity` of an mbarrier (each try suspends the thread for a while). If the
+// first bound runs out, the error flag is raised and the wait gets a second bound of its own, so that
+// copies still in flight land before the CTA goes on and exits; either way the kernel goes on (with
+// garbage, flagged) instead of hanging. The copies waited on are this CTA's own bulk copies from
+// global memory (tens of KB, microseconds), so the second bound (2^20 tries, seconds) runs out only
+// when the expected transaction bytes exceed the bytes issued - a bug, with no copy left in flight.
+// The first bound is a device variable so that a test can make it run out (btd_set_wait_bound): with
+// zero tries the flag is raised at once and the copies land under the second bound.
 constexpr int MBAR_TRIES = 1 << 20;
 constexpr uint32_t ERR_COPY_TIMEOUT = 1u;
+__device__ int g_mbarFirstTries = MBAR_TRIES;
 __device__ __forceinline__ void mbarWaitBounded(uint64_t* bar, unsigned parity, uint32_t* err) {
-  for (int i = 0; i < MBAR_TRIES; ++i)
+  const int first = g_mbarFirstTries;
+  for (int i = 0; i < first; ++i)
     if (mbarTryWait(bar, parity)) return;
   if (err) atomicOr(err, ERR_COPY_TIMEOUT);
   for (int i = 0; i < MBAR_TRIES; ++i)

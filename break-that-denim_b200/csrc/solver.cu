@@ -1560,6 +1560,13 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
   });
 }
 
+int btd_set_wait_bound(int32_t first_tries) {
+  GUARD({
+    const int v = first_tries < 0 ? MBAR_TRIES : std::min<int>(first_tries, MBAR_TRIES);
+    CK(cudaMemcpyToSymbol(g_mbarFirstTries, &v, sizeof v));
+  });
+}
+
 int btd_level_count(btd_solver* s, int32_t* out) {
   GUARD({
     checkSolver(s);

@@ -331,10 +331,19 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton_iterations,
  * running while a stream is being captured). Its reduction scratch is a static device array of
  * 131,328 bytes that every GPU loading the library holds until exit; lattices of more than
  * 524,288 nodes are rejected with BTD_E_INVALID. The first call on each device looks the array's
- * address up (cudaGetSymbolAddress) and should come before any stream capture. All calls share the
- * array: calls that overlap on the GPU race and must be serialised by the caller. */
+ * address up (cudaGetSymbolAddress) and should come before any stream capture; that address is kept
+ * for the life of the process, so this entry point must not be used after a cudaDeviceReset of the
+ * device it ran on. All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
 int btd_matvec_noalloc(int32_t nx, int32_t ny, const void* op, const void* fixed, const void* x, void* y, double* xy,
                        void* stream);
+
+/* Test hook for the bounded device-side waits (no counterpart in the reference): the first bound of
+ * the smoother's wait for its staging copies, in tries (negative: the default, 2^20). With 0 the
+ * wait's error flag is raised at once while the copies still land under its second bound, so results
+ * stay correct and the next btd_synchronize returns BTD_E_TIMEOUT once. Process-wide (every solver on
+ * the current device). */
+int btd_set_wait_bound(int32_t first_tries);
 
 /* Last error message of the calling thread (always NUL-terminated when n > 0). */
 int btd_last_error(char* buf, size_t n);

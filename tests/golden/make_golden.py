@@ -1,4 +1,6 @@
-"""Regenerates the committed golden fixtures from the reference checkout (run where it is mounted).
+"""Regenerates the committed golden fixtures from a checkout of the reference.
+
+Usage: python tests/golden/make_golden.py <reference checkout>  (or set BTD_REFERENCE to its path).
 
 drape_header.json: the header of the reference's precomputed drape (public/drape.bin:
 [magic, version, node count, sceneHash], src/simulation/gpu/settle.ts:4-22) for its default scene.
@@ -14,7 +16,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BTD_REFERENCE")
+if not REF:
+    sys.exit("usage: make_golden.py <reference checkout> (or set BTD_REFERENCE)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 data = open(os.path.join(REF, "public", "drape.bin"), "rb").read()

@@ -63,3 +63,22 @@ def kink_rows(oracle):
         if abs(l / seg["rest_length"][s] - 1) < 1e-6:
             rows.update((a, b))
     return rows
+
+
+def operator_apply(A, nx, ny, d, fixed=None):
+    """y = A d in FP64 with a single-layer level operator read back in the reference's 25-offset
+    layout (offset o: di = o % 5 - 2, dj = o // 5 - 2; newtonMultigrid.ts:38-48), rows of fixed nodes
+    zero when `fixed` is given (StencilOperator.apply, newtonMultigrid.ts:96-125)."""
+    d = np.asarray(d, np.float64).reshape(-1, 3)
+    y = np.zeros_like(d)
+    i, j = np.meshgrid(np.arange(nx), np.arange(ny))
+    i, j = i.reshape(-1), j.reshape(-1)
+    for o in range(25):
+        di, dj = o % 5 - 2, o // 5 - 2
+        ok = (i + di >= 0) & (i + di < nx) & (j + dj >= 0) & (j + dj < ny)
+        n = np.nonzero(ok)[0]
+        m = (j[ok] + dj) * nx + (i[ok] + di)
+        y[n] += np.einsum("nab,nb->na", A[n, o], d[m])
+    if fixed is not None:
+        y[np.asarray(fixed).reshape(-1) != 0] = 0.0
+    return y

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import btd_b200 as btd
-from helpers import MG, copy_state, correctness_coupon, kink_rows, max_abs_rel_to_scale, reference_params
+from helpers import MG, copy_state, correctness_coupon, kink_rows, max_abs_rel_to_scale, operator_apply, reference_params
 from oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -106,21 +106,6 @@ def test_pcg_relative_residual_stop(staged):
     assert max_abs_rel_to_scale(dg, dc) < 1e-3
 
 
-def operator_apply(A, nx, ny, d):
-    """y = A d with a level operator in the reference's 25-offset layout (offset o: di = o % 5 - 2,
-    dj = o // 5 - 2), in FP64."""
-    y = np.zeros_like(d)
-    i, j = np.meshgrid(np.arange(nx), np.arange(ny))
-    i, j = i.reshape(-1), j.reshape(-1)
-    for o in range(25):
-        di, dj = o % 5 - 2, o // 5 - 2
-        ok = (i + di >= 0) & (i + di < nx) & (j + dj >= 0) & (j + dj < ny)
-        n = np.nonzero(ok)[0]
-        m = (j[ok] + dj) * nx + (i[ok] + di)
-        y[n] += np.einsum("nab,nb->na", A[n, o], d[m])
-    return y
-
-
 def test_pcg_stops_on_the_fp64_true_residual(staged):
     """At rel-res 1e-6 the stop is decided by the outer residual b - A delta computed in FP64 from
     the fp32 operator and the iterate accumulated in FP64 (an fp32 iterate alone bottoms out near
@@ -213,6 +198,40 @@ def test_config0_free_trajectory():
     cfg, sc, cpu, gpu = config0_pair()
     err, moved = dynamics(cpu, gpu, cfg["steps"])
     assert err < 0.03 * moved, (err, moved)
+
+
+def test_config0_rebuilt_deep_hierarchy():
+    """The multigrid variant the bench measures beside the reference's schedule: the Galerkin hierarchy
+    rebuilt at every Newton iteration and coarsened down to at most 30 nodes (5 levels at 64 x 64
+    instead of 3). From shared states, each of 20 steps of config 0 lands near the oracle's positions
+    run with the same settings (median 1e-5 relative, as the default schedule), with PCG iteration
+    counts per Newton step within a quarter of the oracle's, and fewer than the lagged schedule's."""
+    cfg = btd.configs.CONFIG0
+    sc = btd.configs.config0()
+    mg = dict(MG, lag_coarse=False, max_coarsest_nodes=30)
+    cpu = Oracle(sc, h=cfg["h"], newton_iterations=cfg["newton_iterations"], pcg_iterations=500,
+                 pcg_rel_tol=cfg["pcg_rel_tol"], **mg)
+    gpu = btd.GpuSolver(sc, btd.configs.solver_params(cfg["h"], cfg["newton_iterations"], cfg["pcg_rel_tol"], lag_coarse=0,
+                                                      max_coarsest_nodes=30))
+    errs, its_c, its_g, newton = [], 0, 0, 0
+    for _ in range(20):
+        copy_state(cpu, gpu)
+        gpu.clear_counters()
+        cpu.predict()
+        for _ in range(cfg["newton_iterations"]):
+            its_c += cpu.newton_step()["pcg_iterations"]
+        cpu.finalize()
+        gpu.substep()
+        c = gpu.counter_dict()
+        its_g += c["pcg_total"]
+        newton += c["newton"]
+        xc = cpu.x
+        errs.append(np.abs(gpu.x.astype(np.float64) - xc).max() / np.abs(xc).max())
+    assert gpu.level_count() == cpu.level_count() == 5
+    assert np.median(errs) < 1e-5, np.median(errs)
+    assert max(errs) < 3e-4, max(errs)
+    assert abs(its_g - its_c) <= 0.25 * its_c, (its_g, its_c)
+    assert its_g / newton < 25, its_g / newton
 
 
 def test_substep_is_deterministic():
