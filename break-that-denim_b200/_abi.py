@@ -209,6 +209,21 @@ SIGNATURES = {
     "btd_release_grip": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_read_grip": ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, _p(C.c_int32)], C.c_int),
     "btd_set_wait_bound": ([C.c_int32], C.c_int),
+    "btd_set_gradient_precision": ([C.c_void_p, C.c_int32], C.c_int),
+    "btd_set_learned": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_double], C.c_int),
+    "btd_learned_stats": ([C.c_void_p, C.c_void_p], C.c_int),
+    "btd_learned_basis": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "btd_learned_log": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32], C.c_int),
+    "btd_trainer_create": ([C.c_void_p], C.c_int),
+    "btd_trainer_destroy": ([C.c_void_p], C.c_int),
+    "btd_trainer_add_op": ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32], C.c_int),
+    "btd_trainer_add_log": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
+    "btd_trainer_counts": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "btd_trainer_read_op": ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                             C.c_void_p], C.c_int),
+    "btd_trainer_loss_grad": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p], C.c_int),
+    "btd_trainer_train": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_uint64, C.c_void_p, C.c_int32,
+                           C.c_void_p], C.c_int),
     "btd_last_error": ([C.c_char_p, C.c_size_t], C.c_int),
 }
 

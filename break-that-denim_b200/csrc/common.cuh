@@ -68,7 +68,8 @@ struct SimParams {
   int lineSearch;
   double pcgTol;
   float newtonTol;
-  int pad0, pad1, pad2;
+  int gradFp64;  // the nonlinear residual (the Newton right-hand side) evaluated in FP64
+  int pad1, pad2;
 };
 
 // Device-side scalars of one Newton iteration (FP64 dots, alpha/beta, convergence state).
@@ -376,6 +377,24 @@ __device__ __forceinline__ Sym coarseBlock(const float4* __restrict__ op, int N,
 
 __device__ __forceinline__ void storeSymAt(float* row, int f, Sym s) {
   row[f] = s.xx, row[f + 1] = s.xy, row[f + 2] = s.xz, row[f + 3] = s.yy, row[f + 4] = s.yz, row[f + 5] = s.zz;
+}
+
+// Lower Cholesky factor of a symmetric 3 x 3 block (6 entries xx xy xz yy yz zz) in FP64: L00, L10, L11,
+// L20, L21, L22; false unless positive definite.
+__device__ __forceinline__ bool chol3d(const Sym& D, double (&L)[6]) {
+  const double a = D.xx;
+  if (!(a > 0.0)) return false;
+  L[0] = sqrt(a);
+  L[1] = D.xy / L[0];
+  L[3] = D.xz / L[0];
+  const double c = D.yy - L[1] * L[1];
+  if (!(c > 0.0)) return false;
+  L[2] = sqrt(c);
+  L[4] = (D.yz - L[3] * L[1]) / L[2];
+  const double e = D.zz - L[3] * L[3] - L[4] * L[4];
+  if (!(e > 0.0)) return false;
+  L[5] = sqrt(e);
+  return true;
 }
 
 // Level geometry passed by value to kernels.

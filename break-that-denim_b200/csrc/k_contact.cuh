@@ -51,6 +51,7 @@ struct ContactArgs {
   float4* cmeta;    // 2 per node: own bound, reciprocal bound (unit normal, largest approach)
   int* acc;         // CT_ACC per node
   float4* ext;      // 3 per node
+  uint8_t* flag;    // per node: contact terms act on it (the learned correction's input), or null
   ContactLaw law;
 };
 
@@ -507,6 +508,7 @@ __global__ void k_ct_gather(ContactArgs a) {
   a.ext[3 * n] = make_float4(v[0], v[1], v[2], 0.f);
   a.ext[3 * n + 1] = make_float4(v[3], v[4], v[5], v[6]);
   a.ext[3 * n + 2] = make_float4(v[7], v[8], 0.f, 0.f);
+  if (a.flag) a.flag[n] = (v[3] != 0.f || v[4] != 0.f || v[5] != 0.f || v[6] != 0.f || v[7] != 0.f || v[8] != 0.f) ? 1 : 0;
 }
 
 }  // namespace btd

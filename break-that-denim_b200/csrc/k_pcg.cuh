@@ -9,6 +9,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "k_learned.cuh"
 #include "k_mg.cuh"
 #include "k_step.cuh"
 
@@ -84,6 +85,7 @@ struct PcgArgs {
   Reduce red;
   cudaGraphConditionalHandle cond;  // PCG while-node condition
   int useCond;
+  LcState* lc;  // the learned coarse correction's state (null: not enabled)
 };
 
 __device__ __forceinline__ double safeDiv(double a, double b) {
@@ -248,6 +250,17 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_update_xr(PcgArgs a) {
     if (stop && s.converged == 0) s.converged = 1;
     s.check = !stop && met ? 1 : 0;
     if (stop) pcgStop(a, s);
+    // guard of the learned coarse correction: a solve whose mean contraction per iteration
+    // (||r_k|| / ||r_0||)^(1/k) exceeds the guard after three iterations goes on with the plain
+    // V-cycle, PCG restarted from its iterate (the next direction starts afresh)
+    if (a.lc && a.lc->active && !stop && !met && s.pcgIt >= 3) {
+      const double rel = P.pcgTol > 0.0 ? s.rel : sqrt(out[0]) / s.r0;
+      if (!(pow(rel, 1.0 / s.pcgIt) <= (double)a.lc->guard)) {
+        a.lc->active = 0;
+        a.lc->fallbacks += 1;
+        s.restart = 1;
+      }
+    }
     if (a.useCond) cudaGraphSetConditional(a.cond, stop ? 0u : 1u);
   }
 }

@@ -147,6 +147,135 @@ __device__ __forceinline__ Sym airDragBlock(const StepArgs& A, int n, const DLay
   return symId(k);
 }
 
+// ------------------------------------------------------------------ the gradient in FP64
+// The Newton right-hand side -grad(Phi) sums large elastic terms (span tensions of whole rows of the
+// sheet) to a small net force. In FP32 the strain of a span is only known to ~6e-8 (l / L - 1 rounded),
+// i.e. EA x 6e-8 of tension - a few per cent of a node's weight in the hanging patch - and that floor
+// stays in the Newton iterate however far PCG converges. This evaluates the same terms in FP64 from the
+// FP32 state (differences of positions formed before any rounding), so each Newton iteration is an
+// iterative-refinement step: FP64 residual, FP32 correction (the operator and the solve stay FP32).
+struct Dv {
+  double x, y, z;
+};
+__device__ __forceinline__ Dv dv(float4 a) { return {a.x, a.y, a.z}; }
+__device__ __forceinline__ Dv operator+(Dv a, Dv b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ Dv operator-(Dv a, Dv b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ Dv operator*(double s, Dv a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ double dotD(Dv a, Dv b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ double lenD(Dv a) { return sqrt(dotD(a, a)); }
+__device__ __forceinline__ Dv symVecD(const Sym& A, Dv v) {
+  return {A.xx * v.x + A.xy * v.y + A.xz * v.z, A.xy * v.x + A.yy * v.y + A.yz * v.z, A.xz * v.x + A.yz * v.y + A.zz * v.z};
+}
+__device__ __forceinline__ double axialTensionD(const DYarn& y, double eps) {
+  if (eps <= 0.0) return (double)y.eaCompress * eps;
+  const double ec = y.crimpStrain, lo = y.eaLow, hi = y.eaHigh, dk = hi - lo;
+  if (eps <= ec) return lo * eps + dk * eps * eps / (2.0 * ec);
+  return lo * ec + dk * ec * 0.5 + hi * (eps - ec);
+}
+__device__ __forceinline__ double bendPsiSlopeD(double q, double a) {
+  const double s = q / a, s0 = BEND_S0;
+  if (s < s0) {
+    const double d = 1.0 - s;
+    return 1.0 / (d * d);
+  }
+  const double d0 = 1.0 - s0;
+  return 1.0 / (d0 * d0) + 2.0 / (a * d0 * d0 * d0) * (q - s0 * a);
+}
+__device__ __forceinline__ double shearForceD(double ks, double jam, double Ld, double l) {
+  double f = ks * (l - Ld);
+  const double c = (Ld - l) / Ld - jam, ramp = SHEAR_RAMP;
+  if (c > 0.0) {
+    const double extra = ks * ((double)SHEAR_LOCK - 1.0);
+    f -= c < ramp ? extra * Ld * c * c / (2.0 * ramp) : extra * Ld * (c - 0.5 * ramp);
+  }
+  return f;
+}
+// Axial force vector of the span owned by a toward b (fs e / l), FP64.
+__device__ __forceinline__ Dv segForceD(const StepArgs& A, int a, int b, int f, const DLayer& mat, double h) {
+  const Dv en = dv(A.x[b]) - dv(A.x[a]);
+  const Dv e = en + (dv(A.dx[b]) - dv(A.dx[a]));
+  const double l = lenD(e), ln = lenD(en);
+  const Seg s = A.segs[2 * a + f];
+  const DYarn& y = mat.yarn[f];
+  const double L = s.rest;
+  const double T = (double)s.intact * axialTensionD(y, l / L - 1.0);
+  const double c = (double)y.axialVisc / (L * h);
+  return ((T + c * (l - ln)) / l) * e;
+}
+// Bending gradient vector of the triple (a, b, c) centred at b, FP64 (tripleGrad).
+__device__ __forceinline__ Dv tripleGradD(const StepArgs& A, int a, int b, int c, int f, const DLayer& mat, double h) {
+  const Seg sa = A.segs[2 * a + f], sb = A.segs[2 * b + f];
+  const double La = sa.rest, Lc = sb.rest, sum = La + Lc, lh = 2.0 * La * Lc / sum;
+  const double wa = 2.0 * Lc / sum, wc = 2.0 * La / sum, gz = 1.0 / (lh * lh * 0.5 * sum), fold = 4.0 * lh * lh;
+  const DYarn& y = mat.yarn[f];
+  const double kb = (double)y.bendRigidity * bendScale(sa.intact, sb.intact, sa.cutMask, sb.cutMask, (uint32_t)y.yarnsPerSpan) * gz;
+  const double kd = kb * (double)y.bendVisc / h;
+  const Dv xb = dv(A.x[b]);
+  const Dv rn = wa * (dv(A.x[a]) - xb) + wc * (dv(A.x[c]) - xb) + (wa + wc - 2.0) * xb;
+  const Dv r = rn + wa * dv(A.dx[a]) - 2.0 * dv(A.dx[b]) + wc * dv(A.dx[c]);
+  const double q = dotD(r, r), lr = sqrt(q);
+  const double ke = kb * bendPsiSlopeD(q, fold);
+  return (ke + kd * (lr - lenD(rn)) / fmax(lr, 1e-12)) * r;
+}
+
+// The gradient of node n in FP64: the same terms as k_assemble's FP32 g (inertia, drag, external,
+// floor, axial, bending, shear).
+__device__ Dv gradientD(const StepArgs& A, int n, const SimParams& P, const NodeStatic& st, const DLayer& L, int i, int j,
+                        const Sym& Dd) {
+  const double h = P.h, w = (double)st.mass / (h * h);
+  const Dv dxn = dv(A.dx[n]);
+  Dv g = w * (dxn - dv(A.pred[n]));
+  g = g + symVecD(Dd, dxn);
+  g = g + dv(A.ext[3 * n]);
+  if (P.floorOn) {
+    const double half = 0.5 * (double)L.thickness, delta = half + (double)P.floorBulge;
+    const double zc = (double)A.x[n].z + dxn.z, s = delta - (zc - (double)P.floorZ);
+    if (s > 0.0) {
+      const double kc = P.floorStiffness, lam = kc * s * s / delta;
+      const double kf = (double)P.floorFriction * lam / fmax(sqrt(dxn.x * dxn.x + dxn.y * dxn.y), (double)P.floorFrictionSpeed * h);
+      g = g + Dv{kf * dxn.x, kf * dxn.y, -lam};
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < 2; ++f) {
+    const int du = f == 0 ? 1 : 0, dv_ = f == 1 ? 1 : 0;
+    const int prev = nodeAt(L, i - du, j - dv_), next = nodeAt(L, i + du, j + dv_);
+    const int prev2 = nodeAt(L, i - 2 * du, j - 2 * dv_), next2 = nodeAt(L, i + 2 * du, j + 2 * dv_);
+    const bool actPrev = activeSpan(A.segs, prev, f);
+    const bool actNext = activeSpan(A.segs, n, f) && next >= 0;
+    if (actPrev) g = g + segForceD(A, prev, n, f, L, h);
+    if (actNext) g = g - segForceD(A, n, next, f, L, h);
+    if (actPrev && actNext) g = g - 2.0 * tripleGradD(A, prev, n, next, f, L, h);
+    if (actNext && activeSpan(A.segs, next, f) && next2 >= 0) {
+      const Seg s0 = A.segs[2 * n + f], s1 = A.segs[2 * next + f];
+      const double wa = 2.0 * (double)s1.rest / ((double)s0.rest + s1.rest);
+      g = g + wa * tripleGradD(A, n, next, next2, f, L, h);
+    }
+    if (actPrev && activeSpan(A.segs, prev2, f)) {
+      const Seg s0 = A.segs[2 * prev2 + f], s1 = A.segs[2 * prev + f];
+      const double wc = 2.0 * (double)s0.rest / ((double)s0.rest + s1.rest);
+      g = g + wc * tripleGradD(A, prev2, prev, n, f, L, h);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    int ci = i, cj = j, pi = i + 1, pj = j + 1;
+    if (c == 1) ci = i - 1, cj = j - 1, pi = i - 1, pj = j - 1;
+    if (c == 2) ci = i - 1, cj = j, pi = i - 1, pj = j + 1;
+    if (c == 3) ci = i, cj = j - 1, pi = i + 1, pj = j - 1;
+    const int p = nodeAt(L, pi, pj);
+    if (p < 0 || !diagActive(A.segs, L, ci, cj, c < 2 ? 0 : 1)) continue;
+    const Dv d = (dv(A.x[p]) - dv(A.x[n])) + (dv(A.dx[p]) - dxn);
+    const double len = lenD(d);
+    const float2 cs = cellShear(A, L, ci, cj);
+    const int cn = nodeAt(L, ci, cj);
+    const double r0 = A.segs[2 * cn].rest, r1 = A.segs[2 * cn + 1].rest;
+    const double fsh = shearForceD(cs.x, cs.y, sqrt(r0 * r0 + r1 * r1), len);
+    g = g - (fsh / len) * d;
+  }
+  return g;
+}
+
 // Normal stiffness of an active contact bound relative to the node's own diagonal (assemble.wgsl:142).
 constexpr float ACTIVE_BOUND = 100.f;
 
@@ -289,6 +418,11 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
   row[54] = C2[0], row[55] = C2[1], row[56] = C2[2], row[57] = C2[3];
 #pragma unroll
   for (int p = 0; p < FINE_PLANES; ++p) op[(size_t)p * N + n] = make_float4(row[4 * p], row[4 * p + 1], row[4 * p + 2], row[4 * p + 3]);
+  if (P.gradFp64) {
+    const Dv gd = gradientD(A, n, P, st, L, i, j, Dd);
+    rhs[n] = make_float4((float)-gd.x, (float)-gd.y, (float)-gd.z, 0.f);
+    return;
+  }
   rhs[n] = make_float4(-g.x, -g.y, -g.z, 0.f);
 }
 

@@ -24,6 +24,7 @@
 #include "common.cuh"
 #include "k_contact.cuh"
 #include "k_grip.cuh"
+#include "k_learned.cuh"
 #include "k_history.cuh"
 #include "k_mg.cuh"
 #include "k_pcg.cuh"
@@ -201,8 +202,20 @@ struct btd_solver {
     a.ext = ext;
     // SELF_CONTACT (selfcontact.ts:7-33)
     a.law = ContactLaw{12e-3f, 3e-3f, 1.0e-3f, 500.f, 0.45f, 0.002f, 0.45f, (1u << CT_TABLE_BITS) - 1u};
+    a.flag = lcOn() ? lcCtFlag : nullptr;
     return a;
   }
+  // learned coarse correction (extension): network, state, basis, flags per level, training log
+  LcState* dLc = nullptr;
+  MlpPacked* dNet = nullptr;
+  float* dLcW = nullptr;       // the flat FP32 weights as given (packed into dNet)
+  float* lcPhi = nullptr;      // 3 M x LC_K
+  uint8_t* lcCtFlag = nullptr; // per fine node
+  std::vector<uint8_t*> lcFlags;  // per level
+  LcLog lcLog{};
+  bool lcEnabled = false;
+  bool lcOn() const { return lcEnabled; }
+  LcArgs lcArgs() const { return LcArgs{dLc, dNet, lcPhi, lcLog}; }
   GripSlot* dGripSlots = nullptr;
   GripEntry* dGripEntries = nullptr;
   float4* dGripGoal = nullptr;
@@ -274,6 +287,7 @@ struct btd_solver {
     a.red = reduce();
     a.cond = h;
     a.useCond = useCond;
+    a.lc = lcOn() ? dLc : nullptr;
     return a;
   }
   HistArgs histArgs() const {
@@ -348,6 +362,19 @@ struct btd_solver {
       }
       encFactor(s, (int)k + 1);
     }
+    if (lcOn()) k_lc_bump<<<1, 1, 0, s>>>(dLc);
+  }
+
+  // The learned coarse space of this PCG solve: damage and contact flags restricted to the coarsest
+  // level, then the basis (once per solve; the correction itself runs inside every V-cycle).
+  void encLearnedBasis(cudaStream_t s) {
+    if (!lcOn()) return;
+    k_lc_flags_fine<<<blocksFor(N, 128), 128, 0, s>>>(N, dNodes, dLayers, segs, contactOn() ? lcCtFlag : nullptr, lcFlags[0]);
+    for (size_t k = 0; k + 1 < levels.size(); ++k)
+      k_lc_flags_restrict<<<blocksFor(levels[k + 1].N, 128), 128, 0, s>>>(levels[k].dev(), levels[k + 1].dev(), lcFlags[k],
+                                                                          lcFlags[k + 1]);
+    const Level& C = levels.back();
+    k_lc_basis<<<1, LC_THREADS, lcBasisSmem(C.N), s>>>(C.dev(), lcFlags.back(), lcArgs());
   }
 
   void encAssemble(cudaStream_t s, bool coarse) {
@@ -411,6 +438,14 @@ struct btd_solver {
   void encVCycle(cudaStream_t s, int k) {
     int last = (int)levels.size() - 1;
     if (k == last) {
+      if (lcOn()) {
+        // the learned coarse space half-way through the coarsest sweeps, which mirror around it
+        const int half = params.coarse_sweeps / 2;
+        for (int sw = 0; sw < half; ++sw) encSmooth(s, k, (sw & 1) == 1);
+        launch(k_lc_correct, 1, LC_THREADS, 0, s, levels[k].dev(), lcArgs());
+        for (int sw = half; sw < params.coarse_sweeps; ++sw) encSmooth(s, k, (sw & 1) == 1);
+        return;
+      }
       for (int sw = 0; sw < params.coarse_sweeps; ++sw) encSmooth(s, k, (sw & 1) == 1);
       return;
     }
@@ -450,6 +485,7 @@ struct btd_solver {
     cudaGraphConditionalHandle h;
     CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
     PcgArgs a = pcgArgs(h, 1);
+    encLearnedBasis(s);
     k_pcg_init<<<redBlocks, RED_THREADS, 0, s>>>(a);
     encVCycle(s, 0);
     launch(k_pcg_dot_rz, redBlocks, RED_THREADS, 0, s, a, 1);
@@ -475,6 +511,7 @@ struct btd_solver {
   // The same PCG launched kernel by kernel, the stop read back after every iteration.
   void runPCGEager(cudaStream_t s) {
     PcgArgs a = pcgArgs(0, 0);
+    encLearnedBasis(s);
     k_pcg_init<<<redBlocks, RED_THREADS, 0, s>>>(a);
     encVCycle(s, 0);
     launch(k_pcg_dot_rz, redBlocks, RED_THREADS, 0, s, a, 1);
@@ -966,6 +1003,7 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
     P.lineSearch = prm->line_search;
     P.pcgTol = prm->pcg_rel_tol;
     P.newtonTol = (float)prm->newton_tolerance;
+    P.gradFp64 = 1;
     s->pushParams();
 
     // ---- initial state (resetState)
@@ -1186,6 +1224,15 @@ int btd_set_graph_mode(btd_solver* s, int32_t use_graphs) {
   });
 }
 
+int btd_set_gradient_precision(btd_solver* s, int32_t fp64) {
+  GUARD({
+    checkSolver(s);
+    s->hostP.gradFp64 = fp64 ? 1 : 0;
+    s->pushParams();
+    s->sync();
+  });
+}
+
 int btd_set_pcg(btd_solver* s, int32_t max_iterations, double rel_tol) {
   GUARD({
     checkSolver(s);
@@ -1355,6 +1402,8 @@ int btd_stage_damage(btd_solver* s) {
 // ---------------------------------------------------------------- grips (interaction.ts:223-318)
 
 static_assert(GRIPS == BTD_GRIPS && GRIP_ENTRIES == BTD_GRIP_ENTRIES, "grip limits differ from btd.h");
+static_assert(LC_WEIGHTS == BTD_LEARNED_WEIGHTS && LC_K == BTD_LEARNED_K && LC_MAX_NODES == BTD_LEARNED_MAX_NODES,
+              "learned correction sizes differ from btd.h");
 static_assert(sizeof(GripEntry) == 32 && sizeof(GripSlot) == 64, "grip layout");
 
 static void checkSlot(btd_solver* s, int32_t slot) {
@@ -1560,7 +1609,174 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
   });
 }
 
-int btd_set_wait_bound(int32_t first_tries) {
+// ---------------------------------------------------------------- learned coarse correction (extension)
+
+// Drops the captured graphs (they are captured again with the current settings on their next use).
+static void resetGraphs(btd_solver* s) {
+  s->sync();
+  for (auto& kv : s->substepExec) cudaGraphExecDestroy(kv.second);
+  s->substepExec.clear();
+  if (s->pcgExec) cudaGraphExecDestroy(s->pcgExec);
+  s->pcgExec = s->capture([&](cudaStream_t q) { s->encPCG(q); });
+}
+
+static void learnedAlloc(btd_solver* s) {
+  if (s->dLc) return;
+  const Level& C = s->levels.back();
+  if (C.layers.size() != 1) throw std::invalid_argument("the learned coarse correction needs a single-layer lattice");
+  if (C.N > LC_MAX_NODES)
+    throw std::invalid_argument("the coarsest level has " + std::to_string(C.N) + " nodes; the learned coarse correction holds at most " +
+                                std::to_string(LC_MAX_NODES) + " (lower max_coarsest_nodes)");
+  static std::once_flag once;
+  static cudaError_t err = cudaSuccess;
+  std::call_once(once, [] {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void*)k_lc_basis);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_lc_basis, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    err = e;
+  });
+  CK(err);
+  s->dLc = s->alloc<LcState>(1);
+  s->dNet = s->alloc<MlpPacked>(1);
+  s->dLcW = s->alloc<float>(LC_WEIGHTS);
+  s->lcPhi = s->alloc<float>((size_t)3 * C.N * LC_K);
+  s->lcCtFlag = s->alloc<uint8_t>(s->N);
+  for (const Level& L : s->levels) s->lcFlags.push_back(s->alloc<uint8_t>(L.N));
+}
+
+extern "C" int btd_set_learned(btd_solver* s, const float* weights, int32_t count, int32_t on, double guard) {
+  GUARD({
+    checkSolver(s);
+    if (on && (!weights || count != LC_WEIGHTS))
+      throw std::invalid_argument("btd_set_learned: the network needs " + std::to_string(LC_WEIGHTS) + " weights");
+    if (weights) {
+      if (count != LC_WEIGHTS) throw std::invalid_argument("btd_set_learned: the network needs " + std::to_string(LC_WEIGHTS) + " weights");
+      for (int q = 0; q < count; ++q)
+        if (!std::isfinite(weights[q])) throw std::invalid_argument("btd_set_learned: non-finite weight");
+    }
+    if (!(guard > 0.0)) throw std::invalid_argument("btd_set_learned: guard must be positive");
+    const bool wasOn = s->lcEnabled;
+    if (on || weights) learnedAlloc(s);
+    if (weights) {
+      CK(cudaMemcpyAsync(s->dLcW, weights, sizeof(float) * LC_WEIGHTS, cudaMemcpyHostToDevice, s->stream));
+      k_mlp_pack<<<1, 256, 0, s->stream>>>(s->dLcW, s->dNet);
+      CK(cudaGetLastError());
+    }
+    if (s->dLc) {
+      LcState st;
+      CK(cudaMemcpyAsync(&st, s->dLc, sizeof st, cudaMemcpyDeviceToHost, s->stream));
+      s->sync();
+      st.on = on ? 1 : 0;
+      st.guard = (float)guard;
+      CK(cudaMemcpyAsync(s->dLc, &st, sizeof st, cudaMemcpyHostToDevice, s->stream));
+    }
+    // the kernels stay in the graphs while logging, so a solver that only logs keeps them too
+    s->lcEnabled = on != 0 || (s->dLc && s->lcLog.R);
+    if (s->lcEnabled != wasOn) resetGraphs(s);
+    s->sync();
+  });
+}
+
+extern "C" int btd_learned_stats(btd_solver* s, int64_t* out) {
+  GUARD({
+    checkSolver(s);
+    if (!out) throw std::invalid_argument("null output");
+    LcState st{};
+    if (s->dLc) {
+      CK(cudaMemcpyAsync(&st, s->dLc, sizeof st, cudaMemcpyDeviceToHost, s->stream));
+      s->sync();
+    }
+    out[0] = st.solves, out[1] = st.applied, out[2] = st.fallbacks, out[3] = st.nOps, out[4] = st.nCalls;
+  });
+}
+
+extern "C" int btd_learned_basis(btd_solver* s, float* phi, double* G, int32_t* dead, uint8_t* flags, int32_t* nodes) {
+  GUARD({
+    checkSolver(s);
+    if (!s->dLc) throw std::invalid_argument("btd_learned_basis: the learned correction was never set");
+    const Level& C = s->levels.back();
+    if (nodes) *nodes = C.N;
+    LcState st;
+    CK(cudaMemcpyAsync(&st, s->dLc, sizeof st, cudaMemcpyDeviceToHost, s->stream));
+    if (phi) CK(cudaMemcpyAsync(phi, s->lcPhi, sizeof(float) * 3 * (size_t)C.N * LC_K, cudaMemcpyDeviceToHost, s->stream));
+    if (flags) CK(cudaMemcpyAsync(flags, s->lcFlags.back(), C.N, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+    if (G) std::memcpy(G, st.G, sizeof st.G);
+    if (dead)
+      for (int k = 0; k < LC_K; ++k) dead[k] = st.basisOk ? st.dead[k] : -1;
+  });
+}
+
+extern "C" int btd_learned_log(btd_solver* s, int32_t on, int32_t cap_ops, int32_t cap_calls) {
+  GUARD({
+    checkSolver(s);
+    if (on && (cap_ops < 1 || cap_calls < 1)) throw std::invalid_argument("btd_learned_log: capacities must be >= 1");
+    learnedAlloc(s);
+    const int M = s->levels.back().N;
+    const bool wasOn = s->lcEnabled;
+    LcState st;
+    CK(cudaMemcpyAsync(&st, s->dLc, sizeof st, cudaMemcpyDeviceToHost, s->stream));
+    s->sync();
+    if (on) {
+      auto fits = [](int cap, size_t each) { return (size_t)cap * each <= (size_t(8) << 30); };
+      if (!fits(cap_ops, sizeof(float4) * COARSE_PLANES * M) || !fits(cap_calls, sizeof(float) * 3 * M))
+        throw std::invalid_argument("btd_learned_log: capacities above 8 GiB of log");
+      if (s->lcLog.R) {  // a new log replaces the old one
+        for (void* q : {(void*)s->lcLog.rows, (void*)s->lcLog.fixed, (void*)s->lcLog.X, (void*)s->lcLog.R, (void*)s->lcLog.opOf}) {
+          s->allocs.erase(std::remove(s->allocs.begin(), s->allocs.end(), q), s->allocs.end());
+          cudaFree(q);
+        }
+        s->lcLog = LcLog{};
+      }
+      s->lcLog.rows = s->alloc<float4>((size_t)cap_ops * COARSE_PLANES * M);
+      s->lcLog.fixed = s->alloc<uint32_t>((size_t)cap_ops * M);
+      s->lcLog.X = s->alloc<float>((size_t)cap_ops * M * LC_IN);
+      s->lcLog.R = s->alloc<float>((size_t)cap_calls * 3 * M);
+      s->lcLog.opOf = s->alloc<int>(cap_calls);
+      st.nOps = st.nCalls = 0;
+      st.capOps = cap_ops;
+      st.capCalls = cap_calls;
+      st.loggedGen = st.gen - 1;
+      st.curOp = -1;
+    }
+    st.log = on ? 1 : 0;
+    CK(cudaMemcpyAsync(s->dLc, &st, sizeof st, cudaMemcpyHostToDevice, s->stream));
+    s->lcEnabled = st.on != 0 || on != 0;
+    resetGraphs(s);  // the log's buffers are kernel arguments of the graphs
+    (void)wasOn;
+    s->sync();
+  });
+}
+
+extern "C++" {
+namespace btd {
+// The solver's learned log as device pointers and counts, for the trainer (trainer.cu).
+struct LearnedLogView {
+  const float4* rows;
+  const uint32_t* fixed;
+  const float* X;
+  const float* R;
+  const int* opOf;
+  int M, nx, ny, ops, calls;
+  cudaStream_t stream;
+};
+int learnedLogView(btd_solver* s, LearnedLogView* v) {
+  if (!s || !s->dLc || !s->lcLog.R) return -1;
+  LcState st;
+  if (cudaMemcpyAsync(&st, s->dLc, sizeof st, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess) return -1;
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return -1;
+  const Level& C = s->levels.back();
+  *v = LearnedLogView{s->lcLog.rows, s->lcLog.fixed, s->lcLog.X, s->lcLog.R, s->lcLog.opOf, C.N, C.layers[0].nx, C.layers[0].ny,
+                      st.nOps, std::min(st.nCalls, st.capCalls), s->stream};
+  return 0;
+}
+}  // namespace btd
+}  // extern "C++"
+
+extern "C" int btd_set_wait_bound(int32_t first_tries) {
   GUARD({
     const int v = first_tries < 0 ? MBAR_TRIES : std::min<int>(first_tries, MBAR_TRIES);
     CK(cudaMemcpyToSymbol(g_mbarFirstTries, &v, sizeof v));

@@ -142,6 +142,10 @@ class GpuSolver:
         """True: one captured graph per substep; False: kernel by kernel (for per-kernel profilers)."""
         check("btd_set_graph_mode", self._h, int(bool(use_graphs)))
 
+    def set_gradient_precision(self, fp64=True):
+        """The Newton right-hand side in FP64 (default) or FP32 (the reference shader's precision)."""
+        check("btd_set_gradient_precision", self._h, int(bool(fp64)))
+
     def set_pcg(self, max_iterations, rel_tol=0.0):
         check("btd_set_pcg", self._h, int(max_iterations), float(rel_tol))
 
@@ -239,6 +243,40 @@ class GpuSolver:
         return nodes[:n].copy(), w[:n].copy(), g[0], g[1], g[2]
 
     STAGES = {"matvec": 0, "smooth": 1, "assemble": 2, "vcycle": 3, "hierarchy": 4, "substep": 5}
+
+    # ---- learned coarse correction (extension; no counterpart in the reference)
+    LEARNED_WEIGHTS = 7064  # W1[20][64] b1[64] W2[64][64] b2[64] W3[64][24] b3[24], row-major [in][out]
+
+    def set_learned(self, weights=None, on=True, guard=0.9):
+        """Add the learned coarse space of `weights` (flat FP32, LEARNED_WEIGHTS values; rounded to BF16 on
+        the device) on the coarsest level of every V-cycle; a PCG solve whose mean contraction per
+        iteration exceeds `guard` after three iterations falls back to the plain V-cycle."""
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32).reshape(-1)
+        check("btd_set_learned", self._h, None if w is None else w.ctypes.data_as(C.c_void_p), 0 if w is None else w.size,
+              int(bool(on)), C.c_double(guard))
+
+    def learned_stats(self):
+        """dict(solves, applied, fallbacks, logged_ops, logged_calls) since the correction was set."""
+        out = np.zeros(5, np.int64)
+        check("btd_learned_stats", self._h, out.ctypes.data_as(C.c_void_p))
+        return dict(zip(("solves", "applied", "fallbacks", "logged_ops", "logged_calls"), (int(v) for v in out)))
+
+    def learned_basis(self):
+        """The last PCG solve's learned basis: (Phi (3 M, 8), G factor (8, 8), dead (8,) or -1 when no basis
+        was built, coarsest flags (M,): bit 0 damage, bit 1 contact)."""
+        M = C.c_int32()
+        check("btd_learned_basis", self._h, None, None, None, None, C.byref(M))
+        m = M.value
+        phi, G = np.zeros((3 * m, 8), np.float32), np.zeros((8, 8))
+        dead, flags = np.zeros(8, np.int32), np.zeros(m, np.uint8)
+        check("btd_learned_basis", self._h, phi.ctypes.data_as(C.c_void_p), G.ctypes.data_as(C.c_void_p),
+              dead.ctypes.data_as(C.c_void_p), flags.ctypes.data_as(C.c_void_p), C.byref(M))
+        return phi, G, dead, flags
+
+    def learned_log(self, on=True, capacity_ops=64, capacity_calls=8192):
+        """Log training material on the device: each new coarsest operator (rows, fixed flags, network
+        inputs) and the coarsest residual of every learned-correction call."""
+        check("btd_learned_log", self._h, int(bool(on)), int(capacity_ops), int(capacity_calls))
 
     def launch_count(self, substeps, newton_iterations, pcg_iterations):
         """Kernel launches of `substeps` substeps with the given Newton and PCG iteration totals."""

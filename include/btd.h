@@ -208,6 +208,11 @@ int btd_set_newton_tolerance(btd_solver* s, float tolerance);
  * device-side while-node; 0 launches the same kernels one by one with the PCG stop read back by
  * the host after every iteration (for per-kernel profilers, which cannot see into such graphs). */
 int btd_set_graph_mode(btd_solver* s, int32_t use_graphs);
+/* Extension: precision of the Newton right-hand side (the nonlinear residual -grad Phi): 1 (default)
+ * evaluates its terms in FP64 from the FP32 state, so each Newton iteration refines in FP64 what the
+ * FP32 operator and PCG solve for; 0 evaluates them in FP32 as the reference's shader does
+ * (assemble.wgsl:152-334). The operator stays FP32 either way. */
+int btd_set_gradient_precision(btd_solver* s, int32_t fp64);
 /* Extension: PCG cap and relative-residual stop (0 = fixed count as the reference). */
 int btd_set_pcg(btd_solver* s, int32_t max_iterations, double rel_tol);
 
@@ -337,6 +342,64 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton_iterations,
  * serialised by the caller. */
 int btd_matvec_noalloc(int32_t nx, int32_t ny, const void* op, const void* fixed, const void* x, void* y, double* xy,
                        void* stream);
+
+/* ---- Learned coarse correction (no counterpart in the reference; the reference's coarsest V-cycle
+ * level is two alternating line sweeps, newtonMultigrid.ts:495-502, solver.ts:584-598). Half-way through
+ * the coarsest sweeps the V-cycle adds the Galerkin correction Phi (Phi^T A Phi)^-1 Phi^T (b - A x) on a
+ * basis of BTD_LEARNED_K vectors that a 3-layer MLP (20 -> 64 -> 64 -> 24, tanh, BF16 weights and
+ * activations, FP32 accumulation, evaluated on the tensor cores) builds per coarsest node from local
+ * data: lattice position, the node's diagonal block, the fraction of fixed neighbours, and damage and
+ * contact flags restricted from the fine lattice. The basis is built once per PCG solve. Single-layer
+ * lattices whose coarsest level has at most BTD_LEARNED_MAX_NODES nodes. */
+#define BTD_LEARNED_WEIGHTS 7064 /* W1[20][64] b1[64] W2[64][64] b2[64] W3[64][24] b3[24], row-major [in][out] */
+#define BTD_LEARNED_K 8
+#define BTD_LEARNED_MAX_NODES 576
+/* Sets the network (weights: BTD_LEARNED_WEIGHTS floats, or NULL to keep the current ones) and turns the
+ * correction on or off. guard: a PCG solve whose mean contraction per iteration (||r_k|| / ||r_0||)^(1/k)
+ * exceeds it after three iterations goes on with the plain V-cycle, PCG restarted from its iterate.
+ * BTD_E_INVALID for a wrong count, non-finite weights, a multi-layer lattice or too large a coarsest level. */
+int btd_set_learned(btd_solver* s, const float* weights, int32_t count, int32_t on, double guard);
+/* out[5]: PCG solves with the correction on, corrections applied, solves that fell back, logged
+ * operators, logged calls. */
+int btd_learned_stats(btd_solver* s, int64_t* out);
+/* The last solve's basis: phi (3 M x 8 floats, row 3 n + c), the Cholesky factor of Phi^T A Phi (64
+ * doubles, lower, row-major), dead columns (8; all -1 when no basis was built), the coarsest nodes'
+ * flags (M bytes: 1 damage, 2 contact); any pointer may be NULL; nodes receives M. */
+int btd_learned_basis(btd_solver* s, float* phi, double* G, int32_t* dead, uint8_t* flags, int32_t* nodes);
+/* Logs training material on the device while on: every new coarsest operator (its rows, fixed flags and
+ * the network inputs of its nodes; at most cap_ops) and the coarsest residual at every correction call
+ * (at most cap_calls). Turning it on starts a new log. The log feeds btd_trainer_add_log. */
+int btd_learned_log(btd_solver* s, int32_t on, int32_t cap_ops, int32_t cap_calls);
+
+/* ---- Training of the learned correction's network on the GPU (no counterpart in the reference).
+ * Material: per coarsest operator its whitened form At = L^-1 A L^-T over the free unknowns (D_i = L_i
+ * L_i^T the diagonal blocks) and its nodes' network inputs; per correction call the whitened residual r
+ * and the exact correction d = At^-1 r. Objective: the mean over calls of 1 - q, q = u^T G^-1 u / r^T d
+ * the share of the call's error energy the basis captures (u = Psi^T r, G = Psi^T At Psi). The network
+ * runs forward and backward in BF16 on the tensor cores with FP32 accumulation; Adam on FP32 weights. */
+typedef struct btd_trainer btd_trainer;
+int btd_trainer_create(btd_trainer** out);
+int btd_trainer_destroy(btd_trainer* t);
+/* Adds one operator of host material (FP64): At (3n x 3n), X (n x 20), R and D (calls x 3n). `group`
+ * labels it for btd_trainer_train's group weights. */
+int btd_trainer_add_op(btd_trainer* t, int32_t nodes, const double* At, const double* X, int32_t calls, const double* R,
+                       const double* D, int32_t group);
+/* Adds the solver's learned log (btd_learned_log) on the device: whitens every logged operator, factors it
+ * (dense Cholesky, FP64) and solves every logged call's exact correction. Operators whose free diagonal
+ * blocks are not all positive definite, or whose whitened form is not, are dropped (as are their calls). */
+int btd_trainer_add_log(btd_trainer* t, btd_solver* s, int32_t group, int32_t* ops_added);
+int btd_trainer_counts(btd_trainer* t, int32_t* ops, int32_t* calls);
+/* Reads operator `op`'s material back (any pointer may be NULL; sizes as in btd_trainer_add_op, FP32). */
+int btd_trainer_read_op(btd_trainer* t, int32_t op, int32_t* nodes, int32_t* calls, float* At, float* X, float* R, float* D,
+                        double* E);
+/* Loss and gradient (BTD_LEARNED_WEIGHTS floats) over all calls of the listed operators (1..16). */
+int btd_trainer_loss_grad(btd_trainer* t, const float* weights, const int32_t* ops, int32_t n_ops, double* loss, float* grad);
+/* `steps` Adam steps (lr decaying tenfold over the run) on minibatches of `batch_ops` operators (all
+ * their calls), drawn without replacement within a step in proportion to group_weights[group] / the
+ * group's operator count (all alike when group_weights is NULL); weights in and out; loss_history
+ * (steps floats, may be NULL) receives each step's minibatch loss. */
+int btd_trainer_train(btd_trainer* t, float* weights, int32_t steps, int32_t batch_ops, float lr, uint64_t seed,
+                      const float* group_weights, int32_t n_groups, float* loss_history);
 
 /* Test hook for the bounded device-side waits (no counterpart in the reference): the first bound of
  * the smoother's wait for its staging copies, in tries (negative: the default, 2^20). With 0 the

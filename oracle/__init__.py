@@ -88,6 +88,7 @@ def lib():
             "ora_learned_call": ([vp, C.c_int32, vp, vp, vp], C.c_int),
             "ora_learned_stats": ([vp, vp], C.c_int),
             "ora_learned_forward": ([vp, vp, C.c_int64, vp], C.c_int),
+            "ora_learned_basis_of": ([vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp], C.c_int),
         }
         for name, (a, r) in sig.items():
             getattr(h, name).argtypes = a
@@ -396,6 +397,19 @@ class Oracle:
             _call("ora_learned_call", h, q, C.byref(op), _ptr(r), _ptr(d))
             calls.append((op.value, r, d))
         return ops, calls
+
+    def learned_basis_of(self, weights, A, fixed, nx, ny, flags):
+        """The learned basis of a given coarsest operator (A (M, 25, 3, 3), fixed (M,), flags (M, 2) damage
+        and contact): (X (M, 20), Phi (3 M, 8), G factor (8, 8), dead (8,)), or None if none was built."""
+        M = nx * ny
+        w = np.ascontiguousarray(weights, np.float64)
+        A = np.ascontiguousarray(A, np.float64).reshape(-1)
+        fx = np.ascontiguousarray(fixed, np.uint8)
+        fl = np.ascontiguousarray(flags, np.float32).reshape(-1)
+        X, phi, G, dead = np.zeros((M, 20)), np.zeros((3 * M, 8)), np.zeros((8, 8)), np.zeros(8, np.int32)
+        rc = lib().ora_learned_basis_of(C.c_void_p(self._h), _ptr(w), _ptr(A), _ptr(fx), nx, ny, _ptr(fl), _ptr(X), _ptr(phi),
+                                        _ptr(G), _ptr(dead))
+        return None if rc != 0 else (X, phi, G, dead)
 
     def learned_stats(self):
         """dict(applied, fallbacks, solves) since creation."""

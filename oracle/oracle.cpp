@@ -3656,4 +3656,39 @@ int ora_learned_forward(const double* w, const double* X, int64_t rows, double* 
   return 0;
 }
 
+// The learned basis of a given coarsest operator (one nx x ny layer, A in the 25-offset layout, fixed
+// flags, 2 input flags per node: damage, contact): the node inputs X (M x LC_IN, zero rows for nodes
+// without a positive definite block), Phi (3 M x LC_K), the Cholesky factor of Phi^T A Phi (LC_K^2) and
+// its dropped columns; returns -1 if no basis could be built. Checks the CUDA path's basis kernel.
+int ora_learned_basis_of(ora_solver* o, const double* w, const double* A, const uint8_t* fixed, int32_t nx, int32_t ny,
+                         const float* flags, double* X, double* phi, double* G, int32_t* dead) {
+  try {
+    Solver& s = o->s;
+    auto op = std::make_shared<StencilOperator>(std::vector<LatticeLayer>{{nx, ny, 0}});
+    std::copy(A, A + op->A.size(), op->A.begin());
+    std::copy(fixed, fixed + op->N, op->fixed.begin());
+    const LearnedCoarse saved = s.lc;
+    s.lc.w.assign(w, w + LC_WEIGHTS);
+    s.lc.flags.assign(flags, flags + 2 * static_cast<size_t>(op->N));
+    std::vector<double> L, Xv;
+    std::vector<uint8_t> ok;
+    s.learnedInputs(*op, L, ok, Xv);
+    if (X) std::copy(Xv.begin(), Xv.end(), X);
+    std::vector<MGLevel> levels{{op, nullptr}};
+    s.learnedBasis(levels);
+    const bool built = s.lc.basisOp == op.get();
+    if (built) {
+      if (phi) std::copy(s.lc.phi.begin(), s.lc.phi.end(), phi);
+      if (G) std::copy(s.lc.G.begin(), s.lc.G.end(), G);
+      if (dead)
+        for (int k = 0; k < LC_K; ++k) dead[k] = s.lc.dead[k];
+    }
+    s.lc = saved;
+    return built ? 0 : -1;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
 }  // extern "C"

@@ -128,6 +128,8 @@ int32_t ora_learned_calls(ora_solver* s);
 int ora_learned_call(ora_solver* s, int32_t q, int32_t* op, double* r, double* d);
 int ora_learned_stats(ora_solver* s, int64_t* applied_fallbacks_solves);
 int ora_learned_forward(const double* weights, const double* X, int64_t rows, double* out);
+int ora_learned_basis_of(ora_solver* s, const double* weights, const double* A, const uint8_t* fixed, int32_t nx, int32_t ny,
+                         const float* flags, double* X, double* phi, double* G, int32_t* dead);
 
 /* Block pentadiagonal solve (newtonMultigrid.ts:435-473). */
 int ora_solve_penta(int32_t n, const double* D, const double* E, const double* F, const double* r, double* x,
