@@ -145,9 +145,12 @@ def solver_params(btd, w, settings=None):
     return p
 
 
-def gpu_arm(btd, w, patch, settings=None):
-    """A GpuSolver set up as the workload (floor, drape, grips) and its per-substep driver."""
+def gpu_arm(btd, w, patch, settings=None, learned=None):
+    """A GpuSolver set up as the workload (floor, drape, grips; the learned coarse correction with the
+    given weights) and its per-substep driver."""
     g = btd.GpuSolver(patch.sc, solver_params(btd, w, settings))
+    if learned is not None:
+        g.set_learned(learned, on=True, guard=btd.configs.CONFIG4["guard"])
     if w.get("product"):
         g.settle_drape()  # the product starts from its settled drape (drape.bin / settleDrape)
     elif w.get("contact") and not w.get("tearing"):
@@ -173,6 +176,18 @@ def timed_substeps(g, drive, first, count):
     return total
 
 
+def learned_weights(btd):
+    """The learned coarse correction's network: the committed weights (trained on the GPU by
+    break-that-denim_b200/train_learned.py), else trained here on the GPU (about a minute)."""
+    path = btd.learned.DEFAULT_PATH
+    if os.path.exists(path):
+        return btd.learned.load(path), {"weights": os.path.basename(path), "trained": "on the GPU by train_learned.py"}
+    t = time.perf_counter()
+    w, hist = btd.learned.train_network(verbose=False)
+    return w, {"weights": "trained in this run on the GPU", "train_s": time.perf_counter() - t,
+               "final_loss": float(np.mean(hist[-50:]))}
+
+
 # Multigrid settings measured beside the reference's schedule (hierarchy lagged from a substep's first
 # Newton iteration, newtonMultigrid.ts:579; coarsest level at most 400 nodes, solver.ts:70): the
 # Galerkin hierarchy rebuilt at every Newton iteration, and that coarsened down to at most 30 nodes.
@@ -181,10 +196,11 @@ def timed_substeps(g, drive, first, count):
 MG_VARIANTS = {"rebuilt": dict(lag_coarse=0), "rebuilt_deep": dict(lag_coarse=0, max_coarsest_nodes=30)}
 
 
-def measure_arm(btd, w, patch, steps, warmup, settings=None):
-    """The workload's substeps W + 1 .. W + K on a fresh solver with `settings`: Newton steps/s from the
-    device-timed substeps, PCG iterations per Newton step, levels and kernel launches."""
-    g, drive = gpu_arm(btd, w, patch, settings)
+def measure_arm(btd, w, patch, steps, warmup, settings=None, learned=None):
+    """The workload's substeps W + 1 .. W + K on a fresh solver with `settings` (and the learned coarse
+    correction when weights are given): Newton steps/s from the device-timed substeps, PCG iterations
+    per Newton step, levels and kernel launches."""
+    g, drive = gpu_arm(btd, w, patch, settings, learned)
     try:
         for s in range(1, warmup + 1):
             drive(s)
@@ -194,10 +210,13 @@ def measure_arm(btd, w, patch, steps, warmup, settings=None):
         ms = timed_substeps(g, drive, warmup + 1, steps)
         g.synchronize()
         c = g.counter_dict()
-        return {"settings": dict(settings or {}), "levels": g.level_count(), "value": c["newton"] / (ms / 1e3),
-                "unit": "Newton steps/s", "ms_per_step": ms / steps,
-                "pcg_iterations_per_newton": c["pcg_total"] / max(1, c["newton"]),
-                "gpu_launches": int(g.launch_count(steps, c["newton"], c["pcg_total"]))}
+        out = {"settings": dict(settings or {}), "learned": learned is not None, "levels": g.level_count(),
+               "value": c["newton"] / (ms / 1e3), "unit": "Newton steps/s", "ms_per_step": ms / steps,
+               "pcg_iterations_per_newton": c["pcg_total"] / max(1, c["newton"]),
+               "gpu_launches": int(g.launch_count(steps, c["newton"], c["pcg_total"]))}
+        if learned is not None:
+            out["learned_stats"] = g.learned_stats()
+        return out
     finally:
         g.close()
 
@@ -596,7 +615,10 @@ def main():
     btd = package()
     patch = Patch.build(btd, w)
     sc = patch.sc
-    gpu, drive = gpu_arm(btd, w, patch)
+    # the metric's learned arm (the tearing workload): the learned coarse correction on top of the
+    # reference's schedule; the plain arm is measured beside it on the same substep window
+    learned, learned_info = (learned_weights(btd) if w.get("tearing") else (None, None))
+    gpu, drive = gpu_arm(btd, w, patch, learned=learned)
     if args.eager:
         gpu.set_graph_mode(False)
 
@@ -652,9 +674,10 @@ def main():
             traffic = None
     gpu.close()
 
+    learned_stats = gpu.learned_stats() if learned is not None else None
     # ---- end to end through the C ABI from pinned host buffers: the state in (the previous step's
     # output), the grip targets, one substep, the state out; substeps W + 1 .. W + K of a fresh solver
-    g2, drive2 = gpu_arm(btd, w, patch)
+    g2, drive2 = gpu_arm(btd, w, patch, learned=learned)
     for s in range(1, args.warmup + 1):
         drive2(s)
         g2.substep()
@@ -681,15 +704,20 @@ def main():
         t_e2e = across_ranks(dist, [t_e2e], "max")[0]
     e2e = world * newton_e2e / t_e2e
 
-    # ---- other multigrid settings on the same substep window (one GPU only)
-    variants = None
+    # ---- the plain arm and other multigrid settings on the same substep window (one GPU only)
+    variants, plain = None, None
+    if learned is not None:
+        plain = measure_arm(btd, w, patch, args.steps, args.warmup, {})
     if world == 1 and not w.get("product"):
         variants = {}
         for name, settings in MG_VARIANTS.items():
-            try:
-                variants[name] = measure_arm(btd, w, patch, args.steps, args.warmup, settings)
-            except Exception as e:  # reported, never fatal to the default measurement
-                variants[name] = {"settings": dict(settings), "error": f"{type(e).__name__}: {e}"}
+            for lw, suffix in ((None, ""), (learned, "_learned")):
+                if lw is None and suffix:
+                    continue
+                try:
+                    variants[name + suffix] = measure_arm(btd, w, patch, args.steps, args.warmup, settings, lw)
+                except Exception as e:  # reported, never fatal to the default measurement
+                    variants[name + suffix] = {"settings": dict(settings), "error": f"{type(e).__name__}: {e}"}
 
     if rank != 0:
         if dist is not None:
@@ -719,7 +747,15 @@ def main():
     line["config"]["levels"] = levels
     if variants is not None:
         line["config"]["mg_variants"] = variants
-    line["config"]["learned_arm"] = "not on the CUDA path: this value is plain MG-PCG"
+    if learned is not None:
+        line["config"]["arm"] = ("learned: the learned coarse correction (BF16 MLP basis on the coarsest level, "
+                                 "guard 0.9) on the reference's schedule (hierarchy lagged from each substep's first "
+                                 "Newton iteration, coarsest level <= 400 nodes)")
+        line["config"]["learned"] = dict(learned_info, stats=learned_stats)
+        line["config"]["plain"] = plain
+        line["config"]["learned_over_plain"] = value / plain["value"]
+    else:
+        line["config"]["arm"] = "plain MG-PCG (the reference's schedule)"
     if w.get("product"):
         line["config"]["ms_per_substep"] = ms_step
         line["config"]["reference_published"] = {

@@ -118,6 +118,63 @@ __device__ __forceinline__ Sym axialBlock(float kPar, float kPerp, float3 e) {
   return {d * e.x * e.x + kPerp, d * e.x * e.y, d * e.x * e.z, d * e.y * e.y + kPerp, d * e.y * e.z, d * e.z * e.z + kPerp};
 }
 
+// PSD projection of a symmetric 3 x 3 block by eigen-clamping in FP64: the cyclic Jacobi method (Golub
+// and Van Loan, Matrix Computations, section 8.5: plane rotations zeroing the off-diagonal entries in
+// row order, repeated until they vanish against the diagonal) gives A = V diag(l) V^T; the projection is
+// V diag(max(l, 0)) V^T. a and out: xx xy xz yy yz zz.
+__device__ __forceinline__ void eigenClamp3(const double (&a)[6], double (&out)[6]) {
+  double A[3][3] = {{a[0], a[1], a[2]}, {a[1], a[3], a[4]}, {a[2], a[4], a[5]}};
+  double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int sweep = 0; sweep < 12; ++sweep) {
+    const double off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+    const double dia = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
+    if (!(off > 1e-32 * dia)) break;
+    for (int p = 0; p < 2; ++p)
+      for (int q = p + 1; q < 3; ++q) {
+        if (A[p][q] == 0.0) continue;
+        // rotation (c, s) with t = tan of the angle that zeroes A[p][q]
+        const double theta = (A[q][q] - A[p][p]) / (2.0 * A[p][q]);
+        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < 3; ++k) {  // A <- A J (columns p, q)
+          const double akp = A[k][p], akq = A[k][q];
+          A[k][p] = c * akp - s * akq;
+          A[k][q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < 3; ++k) {  // A <- J^T A (rows p, q)
+          const double apk = A[p][k], aqk = A[q][k];
+          A[p][k] = c * apk - s * aqk;
+          A[q][k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < 3; ++k) {  // V <- V J
+          const double vkp = V[k][p], vkq = V[k][q];
+          V[k][p] = c * vkp - s * vkq;
+          V[k][q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  const double l[3] = {fmax(A[0][0], 0.0), fmax(A[1][1], 0.0), fmax(A[2][2], 0.0)};
+  auto e = [&](int r, int c) { return V[r][0] * l[0] * V[c][0] + V[r][1] * l[1] * V[c][1] + V[r][2] * l[2] * V[c][2]; };
+  out[0] = e(0, 0), out[1] = e(0, 1), out[2] = e(0, 2), out[3] = e(1, 1), out[4] = e(1, 2), out[5] = e(2, 2);
+}
+
+// The spring block of a near-degenerate element (a span or shear diagonal collapsed to under 1 % of its
+// rest length, where the closed-form projection's FP32 direction loses its digits or is undefined): the
+// exact Hessian K e e^T + (f / l) (I - e e^T) of the spring energy, formed in FP64 from the element
+// vector d (FP64) and eigen-clamped; a zero-length element gets max(K, 0) I.
+__device__ __forceinline__ Sym springBlockFP64(double K, double f, double dx, double dy, double dz) {
+  const double l = sqrt(dx * dx + dy * dy + dz * dz);
+  if (!(l > 0.0)) {
+    const float k = (float)fmax(K, 0.0);
+    return {k, 0.f, 0.f, k, 0.f, k};
+  }
+  const double ex = dx / l, ey = dy / l, ez = dz / l, kp = f / l, d = K - kp;
+  const double a[6] = {d * ex * ex + kp, d * ex * ey, d * ex * ez, d * ey * ey + kp, d * ey * ez, d * ez * ez + kp};
+  double o[6];
+  eigenClamp3(a, o);
+  return {(float)o[0], (float)o[1], (float)o[2], (float)o[3], (float)o[4], (float)o[5]};
+}
+
 // ---------------------------------------------------------------------------------------------- float3
 
 __device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
@@ -149,6 +206,15 @@ __device__ __forceinline__ bool finite3(float3 v) { return finite1(v.x) && finit
 // wrote (the smoother's line factors), never its predecessor's output.
 __device__ __forceinline__ void pdlWait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 __device__ __forceinline__ void pdlLaunchNext() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+// rotationCurve (common.wgsl:274-283): R(th) r - r - th x r, what rotating r by th adds to its tangent step.
+__device__ __forceinline__ float3 rotationCurve(float3 th, float3 r) {
+  const float phi = len3(th);
+  if (phi < 1e-9f) return make_float3(0, 0, 0);
+  const float3 k = (1.f / phi) * th;
+  const float3 kr = cross3(k, r), kkr = cross3(k, kr);
+  return (sinf(phi) - phi) * kr + (1.f - cosf(phi)) * kkr;
+}
 
 // ---------------------------------------------------------------------------------------------- M3
 

@@ -11,6 +11,7 @@
 #include "common.cuh"
 #include "k_learned.cuh"
 #include "k_mg.cuh"
+#include "k_rigid.cuh"
 #include "k_step.cuh"
 
 namespace btd {
@@ -119,6 +120,62 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_init(PcgArgs a) {
   }
 }
 
+// Symmetric fp32 block times an FP64 vector, in FP64.
+__device__ __forceinline__ void symVecAddD(const Sym& A, const double* x, double& y0, double& y1, double& y2) {
+  y0 += (double)A.xx * x[0] + (double)A.xy * x[1] + (double)A.xz * x[2];
+  y1 += (double)A.xy * x[0] + (double)A.yy * x[1] + (double)A.yz * x[2];
+  y2 += (double)A.xz * x[0] + (double)A.yz * x[1] + (double)A.zz * x[2];
+}
+
+// The PCG start from the detached pieces' rigid modes (encodeRigidStart, solver.ts:651-657): delta = x0
+// (t + w x r on each piece's nodes, zero elsewhere), r = b - A x0 in FP64 (fixed rows 0), z = 0.
+__global__ void __launch_bounds__(RED_THREADS) k_pcg_init_rigid(PcgArgs a, StepArgs S, RigidArgs R) {
+  pdlWait();
+  pdlLaunchNext();
+  double v[1] = {0.0};
+  const DLevel& F = a.F;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < F.N; n += gridDim.x * blockDim.x) {
+    const Dv x0 = rigidStartAt(S, R, n);
+    a.dd[3 * n] = x0.x, a.dd[3 * n + 1] = x0.y, a.dd[3 * n + 2] = x0.z;
+    a.delta[n] = make_float4((float)x0.x, (float)x0.y, (float)x0.z, 0.f);
+    a.F.X[n] = make_float4(0, 0, 0, 0);
+    const float4 b = F.B[n];
+    a.b0[n] = b;
+    float3 r = make_float3(0, 0, 0);
+    if (!F.fixed[n]) {
+      int i, j, l;
+      nodeAt(F, n, &i, &j, &l);
+      const DLevelLayer L = layerOf(F, l);
+      double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+      const double xn[3] = {x0.x, x0.y, x0.z};
+      symVecAddD(FineRows::diag(F.op, F.N, n), xn, y0, y1, y2);
+#pragma unroll
+      for (int k = 0; k < FineRows::NC; ++k) {
+        const int2 off = FineRows::offset(k);
+        const int m = levelNode(L, i + off.x, j + off.y);
+        if (m < 0 || !inPiece(R, m)) continue;
+        const Dv xm = rigidStartAt(S, R, m);
+        const double q[3] = {xm.x, xm.y, xm.z};
+        symVecAddD(FineRows::coupling(F.op, F.N, n, k), q, y0, y1, y2);
+      }
+      r = make_float3((float)(b.x - y0), (float)(b.y - y1), (float)(b.z - y2));
+    }
+    F.B[n] = make_float4(r.x, r.y, r.z, 0.f);
+    v[0] += (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
+  }
+  double out[1];
+  if (gridReduce<1>(a.red, v, out) && threadIdx.x == 0) {
+    Scalars& s = *a.scal;
+    s.r0 = sqrt(out[0]);
+    s.rr = out[0];
+    s.rel = s.r0 > 0.0 ? 1.0 : 0.0;
+    s.pcgIt = 0;
+    s.converged = 0;
+    s.check = 0;
+    s.restart = 0;
+  }
+}
+
 // rz' = r . z; first: rz = rz', beta unused; else beta = rz' / rz, rz = rz'.
 __global__ void __launch_bounds__(RED_THREADS) k_pcg_dot_rz(PcgArgs a, int first) {
   pdlWait();
@@ -156,13 +213,6 @@ __global__ void k_pcg_update_p(PcgArgs a, int first) {
   float beta = (float)a.scal->beta;
   float3 p = z + beta * f3(a.p[n]);
   a.p[n] = make_float4(p.x, p.y, p.z, 0.f);
-}
-
-// Symmetric fp32 block times an FP64 vector, in FP64.
-__device__ __forceinline__ void symVecAddD(const Sym& A, const double* x, double& y0, double& y1, double& y2) {
-  y0 += (double)A.xx * x[0] + (double)A.xy * x[1] + (double)A.xz * x[2];
-  y1 += (double)A.xy * x[0] + (double)A.yy * x[1] + (double)A.yz * x[2];
-  y2 += (double)A.xz * x[0] + (double)A.yz * x[1] + (double)A.zz * x[2];
 }
 
 // Ap = A p (fixed rows 0), p . Ap; alpha = rz / pAp (0 and stop when pAp <= 0, as pcg() breaks).
@@ -371,6 +421,10 @@ struct EnergyArgs {
   StepArgs S;
   const float4* __restrict__ delta;
   Reduce red;
+  // detached pieces (null: none): a node of a piece with a valid frame steps along the rotation of its
+  // piece's rigid start (curveW.xyz the rotation, w 1 when on; curveR the arm from the centroid)
+  const float4* __restrict__ curveW;
+  const float4* __restrict__ curveR;
 };
 
 __device__ __forceinline__ float3 dirOf(const EnergyArgs& a, int n) {
@@ -391,10 +445,21 @@ __device__ void nodeDelta(const EnergyArgs& a, int n, float* acc, float* mag) {
     acc[k] += v;
     mag[k] += fabsf(v);
   };
-  auto quad = [&](float3 g, Sym H, float3 s) {
+  // node m's step at step length k (steps, energy.wgsl:63-72): alpha d, plus on a detached piece the
+  // rotation curve of its rigid part; alpha being a power of two, alpha d is exact, so the differences
+  // of steps below equal alpha times the differences of directions bit for bit when no piece is set
+  auto stepAt = [&](int m, int k) -> float3 {
+    float3 sk = ALPHA[k] * dirOf(a, m);
+    if (a.curveW && !a.S.pinned[m]) {
+      const float4 w = a.curveW[m];
+      if (w.w > 0.f) sk += rotationCurve(ALPHA[k] * f3(w), f3(a.curveR[m]));
+    }
+    return sk;
+  };
+  auto quad = [&](float3 g, Sym H, int m) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      float3 sk = ALPHA[k] * s;
+      float3 sk = stepAt(m, k);
       add1(k, dot3(g, sk));
       add1(k, 0.5f * dot3(sk, H * sk));
     }
@@ -405,12 +470,11 @@ __device__ void nodeDelta(const EnergyArgs& a, int n, float* acc, float* mag) {
   const DLayer& L = A.layers[st.layer];
   const float h = P.h;
   const float3 d0 = f3(A.dx[n]);
-  const float3 dn = dirOf(a, n);
   if (!A.pinned[n]) {
     float w = st.mass / (h * h);
-    quad(w * (d0 - f3(A.pred[n])), symId(w), dn);
+    quad(w * (d0 - f3(A.pred[n])), symId(w), n);
     float4 e0 = A.ext[3 * n], e1 = A.ext[3 * n + 1], e2 = A.ext[3 * n + 2];
-    quad(f3(e0), Sym{e1.x, e1.y, e1.z, e1.w, e2.x, e2.y}, dn);
+    quad(f3(e0), Sym{e1.x, e1.y, e1.z, e1.w, e2.x, e2.y}, n);
     if (P.floorOn) {
       float reach = 0.5f * L.thickness + P.floorBulge;
       float s0 = reach - (A.x[n].z + d0.z - P.floorZ);
@@ -418,11 +482,11 @@ __device__ void nodeDelta(const EnergyArgs& a, int n, float* acc, float* mag) {
         float kc = P.floorStiffness;
         float lam = kc * s0 * s0 / reach;
         float kf = P.floorFriction * lam / fmaxf(sqrtf(d0.x * d0.x + d0.y * d0.y), P.floorFrictionSpeed * h);
-        quad(make_float3(kf * d0.x, kf * d0.y, -lam), Sym{kf, 0, 0, kf, 0, 2.f * kc * s0 / reach}, dn);
+        quad(make_float3(kf * d0.x, kf * d0.y, -lam), Sym{kf, 0, 0, kf, 0, 2.f * kc * s0 / reach}, n);
       }
     }
     Sym Dd = airDragBlock(A, n, L, i, j, h);
-    quad(Dd * d0, Dd, dn);
+    quad(Dd * d0, Dd, n);
   }
 #pragma unroll
   for (int f = 0; f < 2; ++f) {
@@ -434,13 +498,12 @@ __device__ void nodeDelta(const EnergyArgs& a, int n, float* acc, float* mag) {
       const float Lr = s.rest;
       const float3 en = f3(A.x[next]) - f3(A.x[n]);
       const float3 ec = en + f3(A.dx[next]) - d0;
-      const float3 de = dirOf(a, next) - dn;
       const float l0 = len3(ec), ln = len3(en);
       const float T0 = s.intact * axialTension(y, l0 / Lr - 1.f);
       const float c = y.axialVisc / (Lr * h);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        float2 r = lenChange(ec, ALPHA[k] * de, l0);
+        float2 r = lenChange(ec, stepAt(next, k) - stepAt(n, k), l0);
         float Ta = s.intact * axialTension(y, r.y / Lr - 1.f);
         add1(k, 0.5f * (T0 + Ta) * r.x);
         add1(k, 0.5f * c * r.x * (r.y + l0 - 2.f * ln));
@@ -454,11 +517,10 @@ __device__ void nodeDelta(const EnergyArgs& a, int n, float* acc, float* mag) {
       const float kd = ke * y.bendVisc / h;
       const float3 rn = geo.x * f3(A.x[prev]) - 2.f * f3(A.x[n]) + geo.y * f3(A.x[next]);
       const float3 r0 = rn + geo.x * f3(A.dx[prev]) - 2.f * d0 + geo.y * f3(A.dx[next]);
-      const float3 dr1 = geo.x * dirOf(a, prev) - 2.f * dn + geo.y * dirOf(a, next);
       const float q0 = dot3(r0, r0), l0 = sqrtf(q0), lrn = len3(rn);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        float3 dr = ALPHA[k] * dr1;
+        float3 dr = geo.x * stepAt(prev, k) - 2.f * stepAt(n, k) + geo.y * stepAt(next, k);
         float dq = 2.f * dot3(r0, dr) + dot3(dr, dr);
         add1(k, 0.5f * ke * bendPsiDelta(q0, q0 + dq, dq, geo.w));
         float2 rl = lenChange(r0, dr, l0);
@@ -483,12 +545,11 @@ __device__ void nodeDelta(const EnergyArgs& a, int n, float* acc, float* mag) {
       if (!on[q]) continue;
       const int p = pa[q], o = pb[q];
       const float3 ec = (f3(A.x[o]) + f3(A.dx[o])) - (f3(A.x[p]) + f3(A.dx[p]));
-      const float3 de = dirOf(a, o) - dirOf(a, p);
       const float l0 = len3(ec);
       const float f0 = shearLaw(ks, jam, Ld, l0).x;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        float2 rr = lenChange(ec, ALPHA[k] * de, l0);
+        float2 rr = lenChange(ec, stepAt(o, k) - stepAt(p, k), l0);
         add1(k, 0.5f * (f0 + shearLaw(ks, jam, Ld, rr.y).x) * rr.x);
       }
     }

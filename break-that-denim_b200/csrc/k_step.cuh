@@ -26,6 +26,13 @@ struct StepArgs {
   const float4* __restrict__ cmeta;  // 2 per node: contact bounds (own, reciprocal); nullptr: none
   uint32_t* counters;
   Scalars* scal;
+  // detached pieces (pieceCount 0: none): the assembly writes each piece node's external block into kx
+  int pieceCount;
+  const uint32_t* __restrict__ pieceOf;
+  float* kx;
+  // the rotation curves of the pieces' nodes for the update (null: none)
+  const float4* __restrict__ curveW;
+  const float4* __restrict__ curveR;
 };
 
 __global__ void k_predict(StepArgs a) {
@@ -55,6 +62,7 @@ __device__ __forceinline__ bool activeSpan(const Seg* __restrict__ segs, int own
 struct SegForce {
   float fs, kPar, kPerp;
   float3 e;
+  float l, L;
 };
 // Axial response of the span owned by a toward b (family f) at the current iterate (segForce,
 // assemble.wgsl:53-65; solver.ts(ref):254-277).
@@ -69,7 +77,7 @@ __device__ __forceinline__ SegForce segForce(const StepArgs& A, int a, int b, in
   float T = s.intact * axialTension(y, eps), K = s.intact * axialStiffness(y, eps);
   float c = y.axialVisc / (L * h);
   float fs = T + c * (l - ln);
-  return {fs, fmaxf(K, 0.f) / L + c, fmaxf(fs, 0.f) / l, (1.f / l) * e};
+  return {fs, fmaxf(K, 0.f) / L + c, fmaxf(fs, 0.f) / l, (1.f / l) * e, l, L};
 }
 
 struct Triple {
@@ -276,6 +284,19 @@ __device__ Dv gradientD(const StepArgs& A, int n, const SimParams& P, const Node
   return g;
 }
 
+// PSD block of a spring element (an axial span a -> b, or a shear diagonal): the closed-form projection
+// kPar e e^T + kPerp (I - e e^T) (newtonMultigrid.ts:127-130, 154-157), except for a near-degenerate
+// element - collapsed below 1 % of its rest length - whose block is the FP64 eigen-clamp of its exact
+// Hessian (springBlockFP64).
+constexpr float DEGENERATE_LENGTH = 1e-2f;
+__device__ __forceinline__ Sym springBlock(const StepArgs& A, int a, int b, float K, float f, float kPerp, float3 e, float l, float L) {
+  if (l >= DEGENERATE_LENGTH * L) return axialBlock(K, kPerp, e);
+  const float4 xa = A.x[a], xb = A.x[b], da = A.dx[a], db = A.dx[b];
+  const double dx = ((double)xb.x - xa.x) + ((double)db.x - da.x), dy = ((double)xb.y - xa.y) + ((double)db.y - da.y),
+               dz = ((double)xb.z - xa.z) + ((double)db.z - da.z);
+  return springBlockFP64(K, f, dx, dy, dz);
+}
+
 // Normal stiffness of an active contact bound relative to the node's own diagonal (assemble.wgsl:142).
 constexpr float ACTIVE_BOUND = 100.f;
 
@@ -325,6 +346,10 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
       onFloorCore = zc <= P.floorZ + half * (1.f + 1e-3f);
     }
   }
+  // a detached piece's node: its external block (inertia, drag, contact, grips, floor; the active bounds
+  // below) for the rigid frame (assemble.wgsl:172-190, 323-327)
+  const bool pieceNode = A.pieceCount > 0 && A.pieceOf[n] < (uint32_t)A.pieceCount;
+  Sym Dext = D;
 
   // couplings [+u, -u, +v, -v] axial/bending, scalars [+2u, -2u, +2v, -2v]
   Sym C1[4] = {symZero(), symZero(), symZero(), symZero()};
@@ -342,14 +367,14 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
     if (actPrev) {
       SegForce s = segForce(A, prev, n, f, L, h);
       g += s.fs * s.e;
-      Sym H = axialBlock(s.kPar, s.kPerp, s.e);
+      Sym H = springBlock(A, prev, n, s.kPar, s.fs, s.kPerp, s.e, s.l, s.L);
       D = D + H;
       if (freePrev) C1[km] = C1[km] + H * -1.f;
     }
     if (actNext) {
       SegForce s = segForce(A, n, next, f, L, h);
       g -= s.fs * s.e;
-      Sym H = axialBlock(s.kPar, s.kPerp, s.e);
+      Sym H = springBlock(A, n, next, s.kPar, s.fs, s.kPerp, s.e, s.l, s.L);
       D = D + H;
       if (freeNext) C1[kp] = C1[kp] + H * -1.f;
     }
@@ -392,7 +417,8 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
     float2 cs = cellShear(A, L, ci, cj);
     float2 sl = shearLaw(cs.x, cs.y, shearRest(A, L, ci, cj), len);
     g -= sl.x * e;
-    Sym H = axialBlock(sl.y, fmaxf(sl.x, 0.f) / len, e);
+    const float Ld = shearRest(A, L, ci, cj);
+    Sym H = springBlock(A, n, p, sl.y, sl.x, fmaxf(sl.x, 0.f) / len, e, len, Ld);
     D = D + H;
     if (!A.pinned[p]) CD[c] = H * -1.f;
   }
@@ -405,10 +431,17 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
       float4 m = A.cmeta[2 * n + b];
       if (m.w >= 1e8f || (m.x == 0.f && m.y == 0.f && m.z == 0.f)) continue;
       float3 mv = f3(m);
-      if (-dot3(dxn, mv) >= m.w - 1e-3f * fabsf(m.w) && dot3(g, mv) > 0.f) D = D + axialBlock(kAct, 0.f, mv);
+      if (-dot3(dxn, mv) >= m.w - 1e-3f * fabsf(m.w) && dot3(g, mv) > 0.f) {
+        D = D + axialBlock(kAct, 0.f, mv);
+        Dext = Dext + axialBlock(kAct, 0.f, mv);
+      }
     }
   }
-  if (onFloorCore && g.z > 0.f) D = D + axialBlock(kAct, 0.f, make_float3(0, 0, 1));
+  if (onFloorCore && g.z > 0.f) {
+    D = D + axialBlock(kAct, 0.f, make_float3(0, 0, 1));
+    Dext = Dext + axialBlock(kAct, 0.f, make_float3(0, 0, 1));
+  }
+  if (pieceNode) storeSymAt(A.kx + 6 * (size_t)n, 0, Dext);
 
   storeSymAt(row, 0, D);
 #pragma unroll
@@ -473,7 +506,13 @@ __global__ void k_newton_apply(StepArgs A, const float4* __restrict__ delta, int
   float alpha = A.scal->lineAlpha;
   float3 dl = f3(delta[n]);
   float3 dn = (finite3(dl) && finite1(alpha)) ? dl : make_float3(0, 0, 0);
-  float3 nd = floorBound(A, P, n, old, feasible(A, n, old + alpha * dn));
+  float3 step = alpha * dn;
+  // curveApply (energy.wgsl:293-302): a detached piece's node moves along the rotation of its rigid start
+  if (A.curveW && alpha > 0.f) {
+    const float4 w = A.curveW[n];
+    if (w.w > 0.f) step += rotationCurve(alpha * f3(w), f3(A.curveR[n]));
+  }
+  float3 nd = floorBound(A, P, n, old, feasible(A, n, old + step));
   float upd = len3(nd - old);
   A.dx[n] = make_float4(nd.x, nd.y, nd.z, upd);
   atomicMax(&A.counters[CNT_UPDATE + iteration], __float_as_uint(upd));

@@ -28,6 +28,7 @@
 #include "k_history.cuh"
 #include "k_mg.cuh"
 #include "k_pcg.cuh"
+#include "k_rigid.cuh"
 #include "k_smooth.cuh"
 #include "k_step.cuh"
 
@@ -259,7 +260,22 @@ struct btd_solver {
     a.cmeta = contactOn() ? cmeta : nullptr;
     a.counters = dCounters;
     a.scal = dScal;
+    a.pieceCount = pieceCount;
+    a.pieceOf = dPieceOf;
+    a.kx = dKx;
+    a.curveW = pieceCount > 0 ? dCurveW : nullptr;
+    a.curveR = pieceCount > 0 ? dCurveR : nullptr;
     return a;
+  }
+  // detached pieces (setPieces, solver.ts:664-676): piece of each node, node lists, rigid frames and steps
+  int pieceCount = 0;
+  uint32_t *dPieceOf = nullptr, *dPieceStart = nullptr, *dPieceNodes = nullptr;
+  size_t pieceNodesCap = 0;
+  float *dKx = nullptr, *dKr = nullptr;
+  double *dFrame = nullptr, *dStep = nullptr;
+  float4 *dCurveW = nullptr, *dCurveR = nullptr;
+  RigidArgs rigidArgs() const {
+    return RigidArgs{pieceCount, dPieceOf, dPieceStart, dPieceNodes, dKx, dKr, dFrame, dStep, dCurveW, dCurveR};
   }
   Reduce reduce() const { return {dPartials, dTicket}; }
   GripArgs gripArgs() const {
@@ -318,6 +334,10 @@ struct btd_solver {
   // then the start of the projected iterate.
   void encPredict(cudaStream_t s, bool grips) {
     k_predict<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs());
+    if (pieceCount > 0) {  // detached pieces start from their rotation over the substep (solver.ts:698-704)
+      k_spin_reduce<<<pieceCount, RIGID_THREADS, 0, s>>>(stepArgs(), rigidArgs());
+      k_spin_apply<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs(), rigidArgs());
+    }
     if (grips) k_grip_lead<<<GRIPS, 256, 0, s>>>(gripArgs());
     if (contactOn()) encDetect(s);
     k_project_start<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs());
@@ -379,8 +399,21 @@ struct btd_solver {
 
   void encAssemble(cudaStream_t s, bool coarse) {
     k_assemble<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs(), levels[0].op, levels[0].B);
+    if (pieceCount > 0) {  // the pieces' rigid frames at this iterate (encodeAssemble, solver.ts:615-616)
+      k_rigid_rotation<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs(), rigidArgs());
+      k_rigid_frame<<<pieceCount, RIGID_THREADS, 0, s>>>(stepArgs(), rigidArgs());
+    }
     encFactor(s, 0);
     if (coarse) encHierarchy(s);
+  }
+  // PCG's start: zero, or each detached piece's rigid response (encodeRigidStart, solver.ts:651-657).
+  void encPcgInit(cudaStream_t s, const PcgArgs& a) {
+    if (pieceCount > 0) {
+      k_rigid_start<<<pieceCount, RIGID_THREADS, 0, s>>>(stepArgs(), rigidArgs(), levels[0].B);
+      k_pcg_init_rigid<<<redBlocks, RED_THREADS, 0, s>>>(a, stepArgs(), rigidArgs());
+    } else {
+      k_pcg_init<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    }
   }
 
   // Line factors of level k, every line in one launch (after its operator changed).
@@ -486,7 +519,7 @@ struct btd_solver {
     CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
     PcgArgs a = pcgArgs(h, 1);
     encLearnedBasis(s);
-    k_pcg_init<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    encPcgInit(s, a);
     encVCycle(s, 0);
     launch(k_pcg_dot_rz, redBlocks, RED_THREADS, 0, s, a, 1);
     launch(k_pcg_update_p, blocksFor(N, 256), 256, 0, s, a, 1);
@@ -512,7 +545,7 @@ struct btd_solver {
   void runPCGEager(cudaStream_t s) {
     PcgArgs a = pcgArgs(0, 0);
     encLearnedBasis(s);
-    k_pcg_init<<<redBlocks, RED_THREADS, 0, s>>>(a);
+    encPcgInit(s, a);
     encVCycle(s, 0);
     launch(k_pcg_dot_rz, redBlocks, RED_THREADS, 0, s, a, 1);
     launch(k_pcg_update_p, blocksFor(N, 256), 256, 0, s, a, 1);
@@ -556,11 +589,15 @@ struct btd_solver {
   }
 
   void encLineSearch(cudaStream_t s) {
+    // pieces step along the rotation of their rigid start (encodeLineSearch, solver.ts:680-681)
+    if (pieceCount > 0) k_rigid_curves<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs(), rigidArgs());
     if (params.line_search) {
       EnergyArgs e;
       e.S = stepArgs();
       e.delta = delta;
       e.red = reduce();
+      e.curveW = pieceCount > 0 ? dCurveW : nullptr;
+      e.curveR = pieceCount > 0 ? dCurveR : nullptr;
       k_energy<<<redBlocks, RED_THREADS, 0, s>>>(e);
     } else {
       k_set_alpha<<<1, 1, 0, s>>>(dScal, dCounters, 1.f);
@@ -1599,10 +1636,12 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
     const int64_t grips = s->gripsOn() ? 1 : 0;
     // self-contact adds detection (6 kernels) once per substep and terms + gather per Newton iteration
     const int64_t contact = s->contactOn() ? 1 : 0;
-    const int64_t perNewton = 2 + (1 + V + 5) + 1 + 1 + grips + 2 * contact;
+    // detached pieces add rotation + frame after the assembly, start (+ the init it replaces) and curves
+    const int64_t rigid = s->pieceCount > 0 ? 1 : 0;
+    const int64_t perNewton = 2 + (1 + V + 5) + 1 + 1 + grips + 2 * contact + 4 * rigid;
     const int64_t hierarchy = 3 * (L - 1);
     const int64_t hierPerSubstep = s->params.lag_coarse ? hierarchy : hierarchy * (newton / std::max(1, substeps));
-    const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips + 6 * contact;
+    const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips + 6 * contact + 2 * rigid;
     // each optional (gated) Newton iteration slot adds its gate kernel, run or not
     const int64_t gates = s->gatedBound(0, 0) - s->unconditional(0);
     *out = (int64_t)substeps * (perSubstep + hierPerSubstep + gates) + (int64_t)newton * perNewton + (int64_t)(pcg - newton) * (V + 5);
@@ -1776,10 +1815,98 @@ int learnedLogView(btd_solver* s, LearnedLogView* v) {
 }  // namespace btd
 }  // extern "C++"
 
+// Test hook: the FP64 eigen-clamp of symmetric 3 x 3 blocks (mode 0: in = 6 doubles xx xy xz yy yz zz per
+// block) or the spring block of a near-degenerate element (mode 1: in = K, f, dx, dy, dz, unused).
+__global__ void k_debug_projection(const double* in, double* out, int count, int mode) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= count) return;
+  const double* a = in + 6 * q;
+  double* o = out + 6 * q;
+  if (mode == 0) {
+    const double m[6] = {a[0], a[1], a[2], a[3], a[4], a[5]};
+    double r[6];
+    eigenClamp3(m, r);
+    for (int k = 0; k < 6; ++k) o[k] = r[k];
+  } else {
+    const Sym S = springBlockFP64(a[0], a[1], a[2], a[3], a[4]);
+    o[0] = S.xx, o[1] = S.xy, o[2] = S.xz, o[3] = S.yy, o[4] = S.yz, o[5] = S.zz;
+  }
+}
+
+extern "C" int btd_debug_projection(const double* in, double* out, int32_t count, int32_t mode) {
+  GUARD({
+    if (!in || !out || count < 1 || count > (1 << 20) || (mode != 0 && mode != 1))
+      throw std::invalid_argument("btd_debug_projection: 1..2^20 blocks, mode 0 or 1");
+    double *din = nullptr, *dout = nullptr;
+    const size_t bytes = sizeof(double) * 6 * (size_t)count;
+    CK(cudaMalloc(&din, bytes));
+    cudaError_t e = cudaMalloc(&dout, bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(din, in, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      k_debug_projection<<<(count + 127) / 128, 128>>>(din, dout, count, mode);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(din);
+    if (dout) cudaFree(dout);
+    CK(e);
+  });
+}
+
 extern "C" int btd_set_wait_bound(int32_t first_tries) {
   GUARD({
     const int v = first_tries < 0 ? MBAR_TRIES : std::min<int>(first_tries, MBAR_TRIES);
     CK(cudaMemcpyToSymbol(g_mbarFirstTries, &v, sizeof v));
+  });
+}
+
+// setPieces (solver.ts:664-676; topology.ts:7-22): the detached pieces of the topology analysis.
+int btd_set_pieces(btd_solver* s, const uint32_t* piece_of, const uint32_t* start, const uint32_t* nodes, int32_t count) {
+  GUARD({
+    checkSolver(s);
+    if (count < 0 || count > MAX_PIECES) throw std::invalid_argument("btd_set_pieces: 0.." + std::to_string(MAX_PIECES) + " pieces");
+    const int N = s->N;
+    if (count > 0) {
+      if (!piece_of || !start || !nodes) throw std::invalid_argument("btd_set_pieces: null piece arrays");
+      if (start[0] != 0) throw std::invalid_argument("btd_set_pieces: start[0] must be 0");
+      for (int p = 0; p < count; ++p)
+        if (start[p + 1] < start[p]) throw std::invalid_argument("btd_set_pieces: start must not decrease");
+      const uint32_t total = start[count];
+      if (total > (uint32_t)N) throw std::invalid_argument("btd_set_pieces: more piece nodes than nodes");
+      for (int p = 0; p < count; ++p)
+        for (uint32_t k = start[p]; k < start[p + 1]; ++k) {
+          if (nodes[k] >= (uint32_t)N) throw std::invalid_argument("btd_set_pieces: node out of range");
+          if (piece_of[nodes[k]] != (uint32_t)p) throw std::invalid_argument("btd_set_pieces: piece_of disagrees with the node lists");
+        }
+      for (int n = 0; n < N; ++n)
+        if (piece_of[n] != NO_PIECE && piece_of[n] >= (uint32_t)count)
+          throw std::invalid_argument("btd_set_pieces: piece_of names a piece beyond count");
+      if (!s->dPieceOf) {
+        s->dPieceOf = s->alloc<uint32_t>(N);
+        s->dPieceStart = s->alloc<uint32_t>(MAX_PIECES + 1);
+        s->dKx = s->alloc<float>(6 * (size_t)N);
+        s->dKr = s->alloc<float>(6 * (size_t)N);
+        s->dFrame = s->alloc<double>(40 * (size_t)MAX_PIECES);
+        s->dStep = s->alloc<double>(6 * (size_t)MAX_PIECES);
+        s->dCurveW = s->alloc<float4>(N);
+        s->dCurveR = s->alloc<float4>(N);
+      }
+      if (total > s->pieceNodesCap) {
+        if (s->dPieceNodes) {
+          s->allocs.erase(std::remove(s->allocs.begin(), s->allocs.end(), (void*)s->dPieceNodes), s->allocs.end());
+          cudaFree(s->dPieceNodes);
+        }
+        s->pieceNodesCap = std::max<size_t>(total, 1);
+        s->dPieceNodes = s->alloc<uint32_t>(s->pieceNodesCap);
+      }
+      CK(cudaMemcpyAsync(s->dPieceOf, piece_of, sizeof(uint32_t) * N, cudaMemcpyHostToDevice, s->stream));
+      CK(cudaMemcpyAsync(s->dPieceStart, start, sizeof(uint32_t) * (count + 1), cudaMemcpyHostToDevice, s->stream));
+      if (total) CK(cudaMemcpyAsync(s->dPieceNodes, nodes, sizeof(uint32_t) * total, cudaMemcpyHostToDevice, s->stream));
+    }
+    const bool changed = count != s->pieceCount || count > 0;
+    s->pieceCount = count;
+    if (changed) resetGraphs(s);  // the piece count is a launch dimension of the captured kernels
+    s->sync();
   });
 }
 

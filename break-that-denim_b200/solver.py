@@ -244,6 +244,16 @@ class GpuSolver:
 
     STAGES = {"matvec": 0, "smooth": 1, "assemble": 2, "vcycle": 3, "hierarchy": 4, "substep": 5}
 
+    def set_pieces(self, piece_of, start, nodes):
+        """setPieces (solver.ts:664-676): detached pieces as the topology analysis labels them (piece of each
+        node or 0xFFFFFFFF, start offsets, node lists); empty start clears."""
+        start = np.ascontiguousarray(start, np.uint32)
+        count = max(0, len(start) - 1)
+        po = np.ascontiguousarray(piece_of, np.uint32)
+        nd = np.ascontiguousarray(nodes, np.uint32)
+        check("btd_set_pieces", self._h, po.ctypes.data_as(C.c_void_p), start.ctypes.data_as(C.c_void_p),
+              nd.ctypes.data_as(C.c_void_p) if nd.size else None, count)
+
     # ---- learned coarse correction (extension; no counterpart in the reference)
     LEARNED_WEIGHTS = 7064  # W1[20][64] b1[64] W2[64][64] b2[64] W3[64][24] b3[24], row-major [in][out]
 

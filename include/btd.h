@@ -242,6 +242,14 @@ int btd_stage_newton(btd_solver* s, int32_t iteration);/* encodeNewtonIteration 
 int btd_stage_finalize(btd_solver* s);                 /* encodeFinalize: commit, damage, slip */
 int btd_stage_damage(btd_solver* s);                   /* encodeDamage */
 
+/* setPieces (solver.ts:664-676): the detached pieces found by the topology analysis (topology.ts:7-22),
+ * as piece_of (N: the piece of each node, 0xFFFFFFFF for none), start (count + 1 offsets into nodes) and
+ * nodes (each piece's nodes). Each piece's six rigid modes then give PCG its start, its nodes step along
+ * the rotation of that start in the line search and update, and each substep starts a spinning piece on
+ * its rotation (rigid_frame.wgsl, rigid_apply.wgsl, rigid_spin.wgsl). count = 0 clears; at most 4096
+ * pieces. BTD_E_INVALID when the arrays disagree. */
+int btd_set_pieces(btd_solver* s, const uint32_t* piece_of, const uint32_t* start, const uint32_t* nodes, int32_t count);
+
 /* Multigrid levels (solver.ts:105-118, 333-352). */
 int btd_level_count(btd_solver* s, int32_t* out);
 int btd_level_nodes(btd_solver* s, int32_t level, int32_t* out);
@@ -400,6 +408,13 @@ int btd_trainer_loss_grad(btd_trainer* t, const float* weights, const int32_t* o
  * (steps floats, may be NULL) receives each step's minibatch loss. */
 int btd_trainer_train(btd_trainer* t, float* weights, int32_t steps, int32_t batch_ops, float lr, uint64_t seed,
                       const float* group_weights, int32_t n_groups, float* loss_history);
+
+/* Test hook for the PSD projection of near-degenerate element blocks (no counterpart in the reference,
+ * whose projections are closed forms, newtonMultigrid.ts:127-157): runs the device routine on `count`
+ * blocks of 6 doubles. mode 0: the FP64 eigen-clamp (cyclic Jacobi) of symmetric 3 x 3 blocks given as
+ * xx xy xz yy yz zz; mode 1: the spring block of a near-degenerate element from (K, f, dx, dy, dz, -),
+ * the eigen-clamp of K e e^T + (f / l) (I - e e^T). Output: 6 doubles per block. */
+int btd_debug_projection(const double* in, double* out, int32_t count, int32_t mode);
 
 /* Test hook for the bounded device-side waits (no counterpart in the reference): the first bound of
  * the smoother's wait for its staging copies, in tries (negative: the default, 2^20). With 0 the

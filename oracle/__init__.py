@@ -88,6 +88,7 @@ def lib():
             "ora_learned_call": ([vp, C.c_int32, vp, vp, vp], C.c_int),
             "ora_learned_stats": ([vp, vp], C.c_int),
             "ora_learned_forward": ([vp, vp, C.c_int64, vp], C.c_int),
+            "ora_break_margins": ([vp, vp], C.c_int),
             "ora_learned_basis_of": ([vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp], C.c_int),
         }
         for name, (a, r) in sig.items():
@@ -204,6 +205,13 @@ class Oracle:
         _call("ora_set_field", C.c_void_p(self._h), _ptr(np.ascontiguousarray(damage, np.uint8)))
 
     # ---- the yarn damage field's steps on this solver's field and spans (yarnField.ts)
+    def break_margins(self):
+        """Per (crossing, family) the last damage update's relative distance to the separation threshold of
+        the yarn there (cut or pull-out; +inf where none was evaluated)."""
+        d = np.zeros(2 * self.scene.C)
+        _call("ora_break_margins", C.c_void_p(self._h), _ptr(d))
+        return d
+
     def field_layer(self, layer=0):
         """dict(offset, K, M, bu, bv, nx, ny, node_offset) of a layer's field."""
         out = np.zeros(8, np.int32)

@@ -503,6 +503,10 @@ struct Solver {
   std::vector<uint32_t> cutMask;
   std::vector<uint16_t> segFlags;
   std::vector<uint8_t> fieldDamage;
+  // per (crossing, family), the last damage update's relative distance to the separation threshold of
+  // the yarn acting there: eps / (eps_peak + eps_soft) - 1 for a cut (yarnDamage reaches 1), delta /
+  // ((d - 1/2) pitch) - 1 for a pull-out; +inf where nothing was evaluated (test instrumentation)
+  std::vector<double> breakMargin;
   std::vector<int> nbr;
   std::vector<int> layerOf;
   std::vector<Grip> grips;
@@ -1708,6 +1712,12 @@ void Solver::updateField() {
               bestOmega = shareFactor(L, sep.data(), f, local % L.K, local / L.K, reach, transfer / fieldStrength[2 * best + f]);
             }
             int code = damageCode(yarnDamage(y, B, areaOf(fieldArea[2 * best + f]), fieldStrength[2 * best + f], soft, eps * bestOmega));
+            {
+              const double ep = strainAtTension(y, (static_cast<double>(fieldStrength[2 * best + f]) * B) / areaOf(fieldArea[2 * best + f]));
+              const double m = eps * bestOmega / (ep + soft) - 1;
+              double& bm = breakMargin[2 * best + f];
+              if (std::fabs(m) < std::fabs(bm)) bm = m;
+            }
             if (code > fieldDamage[2 * best + f]) fieldDamage[2 * best + f] = static_cast<uint8_t>(code);
           }
         }
@@ -1735,6 +1745,11 @@ int Solver::pullOut() {
           double delta = recoilLength(L.yarns[f], bundleOf(L, f), areaOf(fieldArea[2 * c + f]), fieldStrength[2 * c + f], eps,
                                       L.crossingFriction, crossingNormal0[n] / (L.bu * L.bv), L.crossingWrap, tCross, pitch);
           if (delta >= (d - 0.5) * pitch) marked.push_back(2 * c + f);
+          {
+            const double m = delta / ((d - 0.5) * pitch) - 1;
+            double& bm = breakMargin[2 * c + f];
+            if (std::fabs(m) < std::fabs(bm)) bm = m;
+          }
         }
       }
   for (int q : marked) fieldDamage[q] = DAMAGE_PULLED;
@@ -1795,6 +1810,7 @@ int Solver::coupleSpans() {
 
 // updateDamage (solver.ts(ref):659-666).
 void Solver::updateDamage() {
+  breakMargin.assign(fieldDamage.size(), INFINITY);
   for (int q = 0; q < 2 * N; ++q) strain[q] = segActive(q) ? segLength(q) / restLength[q] - 1 : NAN;
   updateField();
   pullOut();
@@ -3302,6 +3318,14 @@ int ora_set_field(ora_solver* o, const uint8_t* d) {
 }
 int ora_get_field(ora_solver* o, uint8_t* d) {
   std::copy(o->s.fieldDamage.begin(), o->s.fieldDamage.end(), d);
+  return 0;
+}
+int ora_break_margins(ora_solver* o, double* out) {
+  if (o->s.breakMargin.size() != o->s.fieldDamage.size()) {
+    std::fill(out, out + o->s.fieldDamage.size(), INFINITY);
+    return 0;
+  }
+  std::copy(o->s.breakMargin.begin(), o->s.breakMargin.end(), out);
   return 0;
 }
 int ora_set_history(ora_solver* o, int32_t on) {

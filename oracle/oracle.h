@@ -128,6 +128,9 @@ int32_t ora_learned_calls(ora_solver* s);
 int ora_learned_call(ora_solver* s, int32_t q, int32_t* op, double* r, double* d);
 int ora_learned_stats(ora_solver* s, int64_t* applied_fallbacks_solves);
 int ora_learned_forward(const double* weights, const double* X, int64_t rows, double* out);
+/* Test instrumentation: per (crossing, family) the last damage update's relative distance to the
+ * separation threshold (cut: eps / (eps_peak + eps_soft) - 1; pull-out: delta / ((d - 1/2) pitch) - 1). */
+int ora_break_margins(ora_solver* s, double* out);
 int ora_learned_basis_of(ora_solver* s, const double* weights, const double* A, const uint8_t* fixed, int32_t nx, int32_t ny,
                          const float* flags, double* X, double* phi, double* G, int32_t* dead);
 

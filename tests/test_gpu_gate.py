@@ -77,3 +77,38 @@ def test_substep_min_and_max_iterations():
     assert n == [3, 3]
     s = solver(1, 3, 0.0)
     assert s.launch_count(1, 3, 12) > solver(1, 1, 0.0).launch_count(1, 3, 12)
+
+
+def test_gated_substeps_match_the_oracle_with_the_same_gate():
+    """The gated schedule against the oracle driven through the same gate (gate.wgsl:12-23): from the
+    same state, the oracle runs newton_iterations Newton iterations, then more up to newton_max while the
+    last one moved some node by more than the tolerance; the GPU's substep graph decides on the device.
+    Per substep the same number of Newton iterations runs and the positions agree."""
+    import sys
+
+    from helpers import MG, copy_state
+    from oracle import Oracle
+
+    sc = btd.configs.hanging_patch(NP, 0.15, seed=5)
+    _, _, u0 = run(solver(1, 4, 0.0), 1)
+    tol = float(np.sqrt(u0[0][1] * u0[0][2]))
+    gpu = solver(1, 4, tol)
+    cpu = Oracle(sc, h=H, newton_iterations=1, pcg_iterations=500, pcg_rel_tol=1e-6, **MG)
+    errs = []
+    for s in range(8):
+        copy_state(cpu, gpu)
+        gpu.clear_counters()
+        gpu.substep()
+        ng = gpu.counter_dict()["newton"]
+        cpu.predict()
+        nc = 0
+        while nc < 4:
+            r = cpu.newton_step()
+            nc += 1
+            if not r["max_update"] > tol:
+                break
+        cpu.finalize()
+        assert ng == nc, (s, ng, nc)
+        xc = cpu.x
+        errs.append(np.abs(gpu.x.astype(np.float64) - xc).max() / np.abs(xc).max())
+    assert np.median(errs) < 1e-5 and max(errs) < 3e-4, errs

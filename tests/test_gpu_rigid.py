@@ -1,0 +1,149 @@
+"""Detached pieces' rigid modes on the CUDA path (rigid_frame.wgsl, rigid_apply.wgsl, rigid_spin.wgsl;
+solver.ts:612-716) against the oracle's restatement, on the reference's own detached-piece contracts
+(tests/gpu/detached.ts): a free 4 x 4 piece thrown with 10 rad/s about its normal keeps its shape and
+spin and falls (tumble, :139-192); a comb cut out of a mounted sheet falls as freely as drag lets it at
+the shipped settings of two Newton and two PCG iterations, and hovers without its piece set (cutOut,
+:305-352); a free layer as one piece reaches the converged solve's velocity in two PCG iterations.
+Each scene runs on both sides from the same state with the same pieces (the host topology analysis),
+and the GPU's trajectory is compared with the oracle's.
+"""
+import numpy as np
+import pytest
+
+import btd_b200 as btd
+from btd_b200.scene import SEG_BROKEN
+from btd_b200.topology import Lattice, label_pieces, pack_bits, search
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+G = 9.81
+H = 1 / 120
+SHIPPED = dict(h=H, newton_iterations=2, pcg_iterations=2, pcg_rel_tol=0.0, max_coarsest_nodes=400, coarse_sweeps=2,
+               line_colors=3, lag_coarse=True, line_search=True)
+
+
+def gpu_params(**kw):
+    return btd.default_params(self_contact=0, **kw)
+
+
+def pieces_of(flags, sc):
+    bits = pack_bits(flags, np.zeros(sc.N, np.float32))
+    lattice = Lattice(sc.layers, sc.N)
+    freed = search(bits, sc.pinned, (), lattice)
+    piece_of, start, nodes, _ = label_pieces(bits, freed, lattice)
+    return piece_of, start, nodes
+
+
+def test_tumbling_piece_matches_the_oracle():
+    m = btd.material_preset(0)
+    sc = btd.compile_scene([btd.layer_spec(m, 0.011, 0.011, bundle=(9, 6), z=0.1, seed=3)])
+    sc.pinned[:] = 0
+    x = sc.position.reshape(-1, 3).astype(np.float32).astype(np.float64)
+    c = x.mean(axis=0)
+    v = np.zeros_like(x)
+    v[:, 0] = -10.0 * (x[:, 1] - c[1])
+    v[:, 1] = 10.0 * (x[:, 0] - c[0])
+    v = v.astype(np.float32).astype(np.float64)
+    cpu = Oracle(sc, **SHIPPED)
+    gpu = btd.GpuSolver(sc, gpu_params())
+    cpu.set_state(x, v)
+    gpu.set_state(x, v)
+    piece_of, start, nodes = pieces_of(cpu.segments()["seg_flags"], sc)
+    assert len(start) == 2 and len(nodes) == 16
+    cpu.set_pieces(piece_of, start, nodes)
+    gpu.set_pieces(piece_of, start, nodes)
+    steps = 6 * round(0.25 / 6 / H)
+    for _ in range(steps):
+        cpu.substep()
+    gpu.substeps(steps)
+    xg, vg = (a[:, :3].astype(np.float64) for a in gpu.state())
+    xc, vc = cpu.x, cpu.v
+    moved = np.abs(xc - x).max()
+    assert np.abs(xg - xc).max() < 0.01 * moved, (np.abs(xg - xc).max(), moved)
+    com, vcom = xg.mean(axis=0), vg.mean(axis=0)
+    r, u = xg - com, vg - vcom
+    spin = np.sum(r[:, 0] * u[:, 1] - r[:, 1] * u[:, 0]) / np.sum(r[:, 0] ** 2 + r[:, 1] ** 2)
+    assert spin > 8.0, spin
+    assert vcom[2] < -0.5 * G * steps * H
+
+
+def comb_scene():
+    m = btd.material_preset(0)
+    sc = btd.compile_scene([btd.layer_spec(m, 0.06, 0.055, bundle=(9, 6), z=0.0, seed=3)])
+    L = sc.layers[0]
+    nx, ny = L.nx, L.ny
+    i, j = np.arange(sc.N) % nx, np.arange(sc.N) // nx
+    sc.pinned[:] = ((i == 0) | (j == 0) | (i == nx - 1) | (j == ny - 1)).astype(np.uint8)
+    i0, j0 = (nx - 8) // 2, (ny - 7) // 2
+    inside = lambda a, b: i0 <= a < i0 + 8 and j0 <= b < j0 + 7  # noqa: E731
+    flags = sc.seg_flags.astype(np.uint16).copy()
+    piece = []
+    for b in range(j0 - 1, j0 + 8):
+        for a in range(i0 - 1, i0 + 9):
+            n = b * nx + a
+            if inside(a, b) != inside(a + 1, b):
+                flags[2 * n] |= SEG_BROKEN
+            if inside(a, b) != inside(a, b + 1):
+                flags[2 * n + 1] |= SEG_BROKEN
+            if not inside(a, b):
+                continue
+            piece.append(n)
+            if b > j0 and inside(a + 1, b):
+                flags[2 * n] |= SEG_BROKEN
+    return sc, flags, piece
+
+
+@pytest.mark.parametrize("with_pieces", [True, False])
+def test_comb_cut_out_matches_the_oracle(with_pieces):
+    sc, flags, piece = comb_scene()
+    cpu = Oracle(sc, **SHIPPED)
+    gpu = btd.GpuSolver(sc, gpu_params())
+    cpu.set_segments(seg_flags=flags)
+    gpu.set_segments(seg_flags=flags.astype(np.uint32))
+    if with_pieces:
+        piece_of, start, nodes = pieces_of(flags, sc)
+        assert sorted(nodes.tolist()) == sorted(piece)
+        cpu.set_pieces(piece_of, start, nodes)
+        gpu.set_pieces(piece_of, start, nodes)
+    steps = round(0.25 / H)
+    for _ in range(steps):
+        cpu.substep()
+    gpu.substeps(steps)
+    vz_c = cpu.v[piece, 2].mean()
+    vz_g = float(gpu.state()[1][piece, 2].mean())
+    t = steps * H
+    if with_pieces:
+        assert -vz_g > 0.5 * G * t, (vz_g, G * t)
+    else:
+        assert -vz_g < 0.2 * G * t, (vz_g, G * t)
+    assert abs(vz_g - vz_c) < 0.02 * abs(vz_c) + 1e-4, (vz_g, vz_c)
+
+
+def test_rigid_start_reaches_the_converged_velocity():
+    m = btd.material_preset(0)
+    sc = btd.compile_scene([btd.layer_spec(m, 0.02, 0.02, bundle=(1, 1), z=0.1, seed=3)])
+    sc.pinned[:] = 0
+    out = {}
+    for name, pcg, pieces in (("rigid", 2, True), ("converged", 200, False)):
+        g = btd.GpuSolver(sc, gpu_params(pcg_iterations=pcg))
+        if pieces:
+            g.set_pieces(np.zeros(sc.N, np.uint32), np.array([0, sc.N], np.uint32), np.arange(sc.N, dtype=np.uint32))
+        g.substeps(10)
+        out[name] = float(g.state()[1][:, 2].mean())
+        g.close()
+    assert abs(out["rigid"] - out["converged"]) < 1e-4 * abs(out["converged"]), out
+
+
+def test_set_pieces_rejects_inconsistent_arrays():
+    sc = btd.configs.hanging_patch(8, 0.05)
+    g = btd.GpuSolver(sc, gpu_params())
+    po = np.full(sc.N, 0xFFFFFFFF, np.uint32)
+    po[:3] = 0
+    with pytest.raises(btd.BtdError):
+        g.set_pieces(po, np.array([0, 3], np.uint32), np.array([0, 1, 5], np.uint32))  # node 5 is not in piece 0
+    g.set_pieces(po, np.array([0, 3], np.uint32), np.array([0, 1, 2], np.uint32))
+    g.substeps(2)
+    g.set_pieces(po, np.array([], np.uint32), np.array([], np.uint32))  # cleared
+    g.substeps(1)
+    assert np.isfinite(g.x).all()
