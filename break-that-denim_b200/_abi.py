@@ -145,6 +145,7 @@ class Params(C.Structure):
         ("line_search", C.c_int32),
         ("lag_coarse", C.c_int32),
         ("overlap_launches", C.c_int32),
+        ("cross_layer", C.c_int32),
     ]
 
 

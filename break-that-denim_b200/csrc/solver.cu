@@ -25,6 +25,7 @@
 #include "k_contact.cuh"
 #include "k_grip.cuh"
 #include "k_learned.cuh"
+#include "k_xcontact.cuh"
 #include "k_history.cuh"
 #include "k_mg.cuh"
 #include "k_pcg.cuh"
@@ -185,6 +186,27 @@ struct btd_solver {
   float4* cmeta = nullptr;
   int* ctAcc = nullptr;
   bool contactOn() const { return params.self_contact != 0 && cmeta != nullptr; }
+  // cross-layer contact in place of self-contact (solver.ts:364)
+  unsigned* xcCells = nullptr;
+  int* xcItems = nullptr;
+  bool xcOn() const { return contactOn() && xcCells != nullptr; }
+  float xcDist[4] = {0, 0, 0, 0};
+  XcArgs xcArgs() const {
+    XcArgs a;
+    a.N = N;
+    a.nodes = dNodes;
+    a.P = dP;
+    a.x = x;
+    a.dx = dx;
+    a.cells = xcCells;
+    a.items = xcItems;
+    a.cand = reinterpret_cast<int*>(ctPairs);
+    a.cmeta = cmeta;
+    a.ext = ext;
+    a.flag = lcEnabled ? lcCtFlag : nullptr;
+    for (int q = 0; q < 4; ++q) a.dist[q] = xcDist[q];
+    return a;
+  }
   ContactArgs contactArgs() const {
     ContactArgs a;
     a.N = N;
@@ -345,6 +367,16 @@ struct btd_solver {
 
   // SelfContact.encodeClear + encodeDetect (selfcontact.ts:137-152).
   void encDetect(cudaStream_t s) {
+    if (xcOn()) {  // contact.ts encodeDetect: count, scan, fill, detect on the (cell, layer) hash
+      const XcArgs a = xcArgs();
+      const int T = (int)XC_MASK + 1;
+      CK(cudaMemsetAsync(xcCells, 0, sizeof(unsigned) * 2 * (size_t)T, s));
+      k_xc_count<<<blocksFor(N, 128), 128, 0, s>>>(a);
+      k_ct_scan<<<1, CT_SCAN_THREADS, 0, s>>>(xcCells, T);
+      k_xc_fill<<<blocksFor(N, 128), 128, 0, s>>>(a);
+      k_xc_detect<<<blocksFor(N, 128), 128, 0, s>>>(a, nLayers);
+      return;
+    }
     const ContactArgs a = contactArgs();
     const int T = 1 << CT_TABLE_BITS;
     CK(cudaMemsetAsync(ctCells, 0, sizeof(unsigned) * 2 * (size_t)T, s));
@@ -360,6 +392,10 @@ struct btd_solver {
   // written over ext (grips add theirs after).
   void encContactTerms(cudaStream_t s) {
     if (!contactOn()) return;
+    if (xcOn()) {
+      k_xc_terms<<<blocksFor(N, 128), 128, 0, s>>>(xcArgs());
+      return;
+    }
     const ContactArgs a = contactArgs();
     k_ct_terms<<<blocksFor(N, 128), 128, 0, s>>>(a);
     k_ct_gather<<<blocksFor(N, 128), 128, 0, s>>>(a);
@@ -799,6 +835,7 @@ int btd_default_params(btd_params* out) {
   p.line_search = 1;
   p.lag_coarse = 1;
   p.overlap_launches = 1;
+  p.cross_layer = 0;
   *out = p;
   return BTD_OK;
 }
@@ -899,6 +936,16 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
       s->ctPairs = s->alloc<unsigned>((CT_K + 2) * (size_t)N);
       s->cmeta = s->alloc<float4>(2 * (size_t)N);
       s->ctAcc = s->alloc<int>(CT_ACC * (size_t)N);
+      if (prm->cross_layer && sc->n_layers > 1) {
+        s->xcCells = s->alloc<unsigned>(2 * ((size_t)XC_MASK + 1));
+        s->xcItems = s->alloc<int>(N);
+        // contact distance of a layer pair: the mean of their thicknesses (contact.ts:49-50)
+        auto thick = [&](int l) { return l < sc->n_layers ? sc->layers[l].material.thickness : 0.0; };
+        s->xcDist[0] = (float)(0.5 * (thick(0) + thick(1)));
+        s->xcDist[1] = (float)(0.5 * (thick(0) + thick(2)));
+        s->xcDist[2] = (float)(0.5 * (thick(1) + thick(2)));
+        s->xcDist[3] = 0.f;
+      }
     }
     s->dGripSlots = s->alloc<GripSlot>(GRIPS);
     s->dGripEntries = s->alloc<GripEntry>((size_t)GRIPS * GRIP_ENTRIES);
@@ -1638,10 +1685,11 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
     const int64_t contact = s->contactOn() ? 1 : 0;
     // detached pieces add rotation + frame after the assembly, start (+ the init it replaces) and curves
     const int64_t rigid = s->pieceCount > 0 ? 1 : 0;
-    const int64_t perNewton = 2 + (1 + V + 5) + 1 + 1 + grips + 2 * contact + 4 * rigid;
+    const int64_t xc = s->xcOn() ? 1 : 0;  // cross-layer contact: terms in one kernel, detection in four
+    const int64_t perNewton = 2 + (1 + V + 5) + 1 + 1 + grips + (2 - xc) * contact + 4 * rigid;
     const int64_t hierarchy = 3 * (L - 1);
     const int64_t hierPerSubstep = s->params.lag_coarse ? hierarchy : hierarchy * (newton / std::max(1, substeps));
-    const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips + 6 * contact + 2 * rigid;
+    const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips + (6 - 2 * xc) * contact + 2 * rigid;
     // each optional (gated) Newton iteration slot adds its gate kernel, run or not
     const int64_t gates = s->gatedBound(0, 0) - s->unconditional(0);
     *out = (int64_t)substeps * (perSubstep + hierPerSubstep + gates) + (int64_t)newton * perNewton + (int64_t)(pcg - newton) * (V + 5);

@@ -147,6 +147,9 @@ typedef struct btd_params {
   int32_t overlap_launches;  /* extension: kernels of the PCG loop start while their predecessor drains
                                 (programmatic dependent launch; the smoother stages its line factors
                                 meanwhile); 0 serialises them; 1 */
+  int32_t cross_layer;       /* with self_contact on a scene of several layers: node-node contact between
+                                the layers in place of self-contact, as the reference does (solver.ts:364;
+                                contact.ts, contact.wgsl); 0 */
 } btd_params;
 
 /* GPU_DEFAULTS (solver.ts:61-72). */
