@@ -9,8 +9,8 @@ from . import _abi, configs, drape, learned, topology
 from .scene import (Scene, bundle_weave, compile_scene, default_spec, layer_spec, material_preset, SEG_BROKEN,
                     SEG_EXISTS, SEG_INITIAL_DEFECT, SEG_SLIPPED)
 from ._abi import BtdError
-from .solver import COARSE_ROW, FINE_ROW, GpuSolver, batch_substeps, default_params
+from .solver import COARSE_ROW, FINE_ROW, Batch, GpuSolver, batch_substeps, default_params
 
 __all__ = ["Scene", "bundle_weave", "compile_scene", "default_spec", "layer_spec", "material_preset", "SEG_BROKEN",
            "SEG_EXISTS", "SEG_INITIAL_DEFECT", "SEG_SLIPPED", "GpuSolver", "default_params", "FINE_ROW", "COARSE_ROW",
-           "configs", "drape", "learned", "topology", "BtdError", "batch_substeps"]
+           "configs", "drape", "learned", "topology", "BtdError", "batch_substeps", "Batch"]

@@ -210,6 +210,10 @@ SIGNATURES = {
     "btd_release_grip": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_read_grip": ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, _p(C.c_int32)], C.c_int),
     "btd_set_wait_bound": ([C.c_int32], C.c_int),
+    "btd_batch_create": ([C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
+    "btd_batch_run": ([C.c_void_p, C.c_int32], C.c_int),
+    "btd_batch_destroy": ([C.c_void_p], C.c_int),
+    "btd_autotune": ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "btd_set_pieces": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32], C.c_int),
     "btd_debug_projection": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_int32], C.c_int),
     "btd_set_gradient_precision": ([C.c_void_p, C.c_int32], C.c_int),

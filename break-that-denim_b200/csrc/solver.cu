@@ -255,6 +255,7 @@ struct btd_solver {
   std::map<int, cudaGraphExec_t> substepExec;
   cudaGraphExec_t pcgExec = nullptr;
   bool useGraphs = true;
+  bool batchGrips = false;  // grips held when a batch graph holding this solver was captured
   void* flushBuf = nullptr;  // profiling only: rewritten to evict L2 between timed launches
 
   template <class T>
@@ -1155,6 +1156,119 @@ int btd_batch_substeps(btd_solver* const* solvers, int32_t count, int32_t subste
   });
 }
 
+}  // extern "C"
+
+// A batch of solvers stepped by one graph: one substep of every solver, each on its own stream inside
+// one capture (forked from and joined to the batch stream), so a whole batch substep is one
+// cudaGraphLaunch whose branches the device runs side by side (each with its own device-side PCG loops).
+struct btd_batch {
+  std::vector<btd_solver*> solvers;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  std::vector<cudaEvent_t> ready, done;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+  ~btd_batch() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (exec) cudaGraphExecDestroy(exec);
+    for (cudaEvent_t e : ready) cudaEventDestroy(e);
+    for (cudaEvent_t e : done) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  void capture() {
+    if (exec) {
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+    try {
+      CK(cudaEventRecord(fork, stream));
+      for (size_t b = 0; b < solvers.size(); ++b) {
+        btd_solver* s = solvers[b];
+        CK(cudaStreamWaitEvent(s->stream, fork, 0));
+        s->encSubstep(s->stream, s->unconditional(0), s->gatedBound(0, 0), s->gripsOn());
+        CK(cudaEventRecord(done[b], s->stream));
+        CK(cudaStreamWaitEvent(stream, done[b], 0));
+      }
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    cudaGraph_t g;
+    CK(cudaStreamEndCapture(stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+  }
+};
+
+extern "C" {
+
+int btd_batch_create(btd_solver* const* solvers, int32_t count, btd_batch** out) {
+  if (!solvers || count < 1 || !out) {
+    btd::setError("btd_batch_create: solvers, count >= 1 and an output");
+    return BTD_E_INVALID;
+  }
+  std::unique_ptr<btd_batch> b(new btd_batch());
+  GUARD({
+    for (int k = 0; k < count; ++k) {
+      checkSolver(solvers[k]);
+      if (!solvers[k]->useGraphs) throw std::invalid_argument("btd_batch_create: a solver in eager mode");
+      for (int q = 0; q < k; ++q)
+        if (solvers[q] == solvers[k]) throw std::invalid_argument("btd_batch_create: a solver twice");
+    }
+    b->solvers.assign(solvers, solvers + count);
+    CK(cudaGetDevice(&b->device));
+    CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming));
+    b->ready.resize(count);
+    b->done.resize(count);
+    for (int k = 0; k < count; ++k) {
+      CK(cudaEventCreateWithFlags(&b->ready[k], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&b->done[k], cudaEventDisableTiming));
+    }
+    for (btd_solver* s : b->solvers) s->sync();
+    b->capture();
+    for (btd_solver* s : b->solvers) s->batchGrips = s->gripsOn();
+    *out = b.release();
+  });
+}
+
+int btd_batch_destroy(btd_batch* b) {
+  delete b;
+  return BTD_OK;
+}
+
+int btd_batch_run(btd_batch* b, int32_t substeps) {
+  GUARD({
+    if (!b || substeps < 0) throw std::invalid_argument("btd_batch_run: null batch or negative count");
+    // a grip attached or released since the capture changes a solver's substep: capture again
+    bool stale = false;
+    for (btd_solver* s : b->solvers) stale = stale || s->gripsOn() != s->batchGrips;
+    if (stale) {
+      for (btd_solver* s : b->solvers) s->sync();
+      b->capture();
+      for (btd_solver* s : b->solvers) s->batchGrips = s->gripsOn();
+    }
+    for (int k = 0; k < substeps; ++k) {
+      // the batch stream waits for what each solver's stream holds (grip targets, state writes),
+      // then every solver's stream waits for the batch substep
+      for (size_t q = 0; q < b->solvers.size(); ++q) {
+        CK(cudaEventRecord(b->ready[q], b->solvers[q]->stream));
+        CK(cudaStreamWaitEvent(b->stream, b->ready[q], 0));
+      }
+      CK(cudaGraphLaunch(b->exec, b->stream));
+      CK(cudaEventRecord(b->join, b->stream));
+      for (btd_solver* s : b->solvers) CK(cudaStreamWaitEvent(s->stream, b->join, 0));
+    }
+  });
+}
+
 int btd_synchronize(btd_solver* s) {
   GUARD({
     checkSolver(s);
@@ -1614,6 +1728,54 @@ int btd_read_grip(btd_solver* s, int32_t slot, int32_t* nodes, float* weights, i
       if (weights) weights[k] = e[k].w;
     }
     if (handle12) std::memcpy(handle12, goal, sizeof goal);
+  });
+}
+
+static void resetGraphs(btd_solver* s);
+
+// The sweep's launch shape per level, chosen by measurement: for every level the CTA size (a multiple of
+// 32 from 64 to SM_SWEEP_THREADS) and, on lines longer than 128 nodes, the staging tile (the whole line
+// or 128 nodes) are timed on the level's current operator with CUDA events (the mean of `reps` sweeps
+// after one untimed), and the fastest is kept. A sweep's arithmetic does not depend on either (every
+// loop strides by the CTA size; a tile only changes how much of the line is staged at once), so the
+// results are the same bit for bit. The captured graphs are dropped and captured again with the choice.
+int btd_autotune(btd_solver* s, int32_t reps, int32_t* threads_out, int32_t* tile_out, float* ms_out) {
+  GUARD({
+    checkSolver(s);
+    if (reps < 1) throw std::invalid_argument("btd_autotune: reps >= 1");
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (size_t k = 0; k < s->levels.size(); ++k) {
+      Level& L = s->levels[k];
+      std::vector<int> tiles{L.tile};
+      if (L.maxLine > 128 && L.tile != 128) tiles.push_back(128);
+      int bestT = L.threads, bestTile = L.tile;
+      float best = 1e30f;
+      for (int tile : tiles)
+        for (int T = 64; T <= SM_SWEEP_THREADS; T += 32) {
+          L.tile = tile;
+          L.threads = T;
+          s->encSmooth(s->stream, (int)k, false);  // untimed: first touch
+          CK(cudaEventRecord(e0, s->stream));
+          for (int r = 0; r < reps; ++r) s->encSmooth(s->stream, (int)k, false);
+          CK(cudaEventRecord(e1, s->stream));
+          CK(cudaEventSynchronize(e1));
+          float t = 0.f;
+          CK(cudaEventElapsedTime(&t, e0, e1));
+          t /= reps;
+          if (t < best) best = t, bestT = T, bestTile = tile;
+        }
+      L.threads = bestT;
+      L.tile = bestTile;
+      if (threads_out) threads_out[k] = bestT;
+      if (tile_out) tile_out[k] = bestTile;
+      if (ms_out) ms_out[k] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaGetLastError());
+    resetGraphs(s);
   });
 }
 

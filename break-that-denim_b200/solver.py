@@ -288,6 +288,15 @@ class GpuSolver:
         inputs) and the coarsest residual of every learned-correction call."""
         check("btd_learned_log", self._h, int(bool(on)), int(capacity_ops), int(capacity_calls))
 
+    def autotune(self, reps=10):
+        """Time every level's sweep launch shapes (CTA size, staging tile) on the current operator and keep
+        the fastest; returns [(threads, tile, ms)] per level."""
+        L = self.level_count()
+        t, tile, ms = np.zeros(L, np.int32), np.zeros(L, np.int32), np.zeros(L, np.float32)
+        check("btd_autotune", self._h, int(reps), t.ctypes.data_as(C.c_void_p), tile.ctypes.data_as(C.c_void_p),
+              ms.ctypes.data_as(C.c_void_p))
+        return [(int(a), int(b), float(c)) for a, b, c in zip(t, tile, ms)]
+
     def launch_count(self, substeps, newton_iterations, pcg_iterations):
         """Kernel launches of `substeps` substeps with the given Newton and PCG iteration totals."""
         out = C.c_int64()
@@ -361,3 +370,25 @@ def batch_substeps(solvers, substeps):
     """btd_batch_substeps: `substeps` substeps of every solver, concurrently on their own streams."""
     arr = (C.c_void_p * len(solvers))(*[s._h for s in solvers])
     check("btd_batch_substeps", arr, len(solvers), substeps)
+
+
+class Batch:
+    """A batch of solvers stepped by one graph launch per substep (btd_batch_*)."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s._h.value for s in self.solvers])
+        h = C.c_void_p()
+        check("btd_batch_create", arr, len(self.solvers), C.byref(h))
+        self._h = h
+
+    def run(self, substeps=1):
+        check("btd_batch_run", self._h, int(substeps))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _abi.lib().btd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

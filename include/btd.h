@@ -178,6 +178,17 @@ int btd_substeps(btd_solver* s, int32_t count);
  * With more patches than CUDA_DEVICE_MAX_CONNECTIONS (8 unless the process sets it, at most 32)
  * streams share hardware queues. Synchronise each solver (btd_synchronize) before reading it. */
 int btd_batch_substeps(btd_solver* const* solvers, int32_t count, int32_t substeps);
+/* A batch as one graph (no counterpart in the reference): one substep of every solver, each on its own
+ * stream inside one capture, so a batch substep is a single cudaGraphLaunch whose branches run side by
+ * side, each with its own device-side PCG loops. btd_batch_run launches it `substeps` times, each after
+ * the work already queued on every solver's stream (grip targets, state writes) and before what comes
+ * after it there; its results are those of btd_substeps on each solver alone. The batch graph holds the
+ * solvers' settings at creation: create it again after a solver's learned correction, pieces or graph
+ * mode change (a grip attached or released is picked up by itself). Solvers must outlive the batch. */
+typedef struct btd_batch btd_batch;
+int btd_batch_create(btd_solver* const* solvers, int32_t count, btd_batch** out);
+int btd_batch_run(btd_batch* b, int32_t substeps);
+int btd_batch_destroy(btd_batch* b);
 /* Wait for all submitted work (the reference's onSubmittedWorkDone). */
 /* Wait for the solver's stream (onSubmittedWorkDone). Returns BTD_E_TIMEOUT, once, when a bounded
  * device-side wait (a staging copy's completion) ran out since the last call: the kernels never hang
@@ -337,6 +348,14 @@ int btd_profile_stage(btd_solver* s, int32_t which, int32_t reps, int32_t flush,
 /* Kernel launches of substeps that ran `newton_iterations` Newton iterations and `pcg_iterations`
  * PCG iterations in total (the graph's nodes that are kernels, loop bodies counted per pass). */
 int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton_iterations, int32_t pcg_iterations, int64_t* out);
+/* Autotuner of the yarn-line sweeps' launch shapes (no counterpart in the reference, whose workgroup
+ * size is fixed at 128, smooth.wgsl:86): for every multigrid level the CTA size (multiples of 32 from 64
+ * to 256) and, on lines longer than 128 nodes, the staging tile (whole line or 128 nodes) are timed on
+ * the level's current operator (CUDA events, the mean of `reps` sweeps) and the fastest is kept for
+ * every later sweep; results are unchanged bit for bit. Needs an assembled system (after a substep or
+ * btd_stage_assemble). Per level (btd_level_count entries, any pointer may be NULL): the chosen CTA
+ * size, tile, and the sweep's time in ms. */
+int btd_autotune(btd_solver* s, int32_t reps, int32_t* threads, int32_t* tile, float* ms);
 
 /* y = A x and x . y for a single-layer nx x ny fine operator on caller-owned DEVICE buffers (op in
  * the fine-row layout of btd_device_buffer, fixed flags as uint32, x and y 4 floats per node, xy one

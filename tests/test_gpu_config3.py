@@ -43,3 +43,39 @@ def test_batch_equals_each_patch_alone():
     for s, _ in batch:
         assert np.isfinite(s.x).all()
         s.close()
+
+
+def test_batch_graph_equals_each_patch_alone():
+    """The batch as one graph (btd_batch_create / btd_batch_run): every patch's substep a branch of a
+    single graph launch, grip targets queued on each patch's stream before it; each patch ends bit for
+    bit where it ends alone, also after the sweeps' launch shapes were autotuned."""
+    c = btd.configs.CONFIG3
+    patches = btd.configs.config3(count=12, sides=(16, 64))
+    steps = 12
+    batch = [make(p) for p in patches]
+    s0, a0 = batch[0]
+    s0.set_target((a0 + c["h"] * patches[0][1]["velocity"]).astype(np.float32))
+    s0.substep()  # an assembled system to tune on (patch 0 is one substep ahead)
+    batch[0][0].autotune(reps=3)
+    first = batch[0][0].x.copy()
+    graph = btd.Batch([s for s, _ in batch])
+    for k in range(1, steps + 1):
+        for i, ((s, anchor), (_, g)) in enumerate(zip(batch, patches)):
+            kk = k + 1 if i == 0 else k
+            s.set_target((anchor + kk * c["h"] * g["velocity"]).astype(np.float32))
+        graph.run(1)
+    for s, _ in batch:
+        s.synchronize()
+    for i, ((s, _), p) in enumerate(zip(batch, patches)):
+        alone, anchor = make(p)
+        total = steps + 1 if i == 0 else steps
+        for k in range(1, total + 1):
+            alone.set_target((anchor + k * c["h"] * p[1]["velocity"]).astype(np.float32))
+            alone.substep()
+            if i == 0 and k == 1:
+                assert np.array_equal(alone.x, first)
+        assert np.array_equal(alone.x, s.x), i
+        alone.close()
+    graph.close()
+    for s, _ in batch:
+        s.close()
