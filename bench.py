@@ -463,11 +463,16 @@ def run_batch(args, w, rank, world, local, dist):
     t_setup = time.perf_counter() - t_setup
     step = [0]
 
+    graph = [None]
+
     def advance():
         step[0] += 1
         for s, a, (_, g) in zip(solvers, anchors, patches):
             s.set_target((a + step[0] * c["h"] * g["velocity"]).astype(np.float32))
-        btd.batch_substeps(solvers, 1)
+        if graph[0] is not None:
+            graph[0].run(1)
+        else:
+            btd.batch_substeps(solvers, 1)
 
     def barrier():
         if dist is not None:
@@ -478,6 +483,15 @@ def run_batch(args, w, rank, world, local, dist):
 
     for _ in range(args.warmup):
         advance()
+    barrier()
+    # the sweeps' launch shapes of every patch picked by the autotuner on its current operators, then
+    # the batch as one graph: one launch per batch substep
+    t_tune = time.perf_counter()
+    if not args.batch_streams:
+        for s in solvers:
+            s.autotune(reps=3)
+        graph[0] = btd.Batch(solvers)
+    t_tune = time.perf_counter() - t_tune
     barrier()
     for s in solvers:
         s.clear_counters()
@@ -519,7 +533,10 @@ def run_batch(args, w, rank, world, local, dist):
     for _ in range(args.steps):
         for s, (xh, vh) in zip(solvers, host):
             lib_check("btd_set_state", s._h, xh.data_ptr(), vh.data_ptr())
-        btd.batch_substeps(solvers, 1)
+        if graph[0] is not None:
+            graph[0].run(1)
+        else:
+            btd.batch_substeps(solvers, 1)
         for s, (xh, vh) in zip(solvers, host):
             lib_check("btd_get_state", s._h, xh.data_ptr(), vh.data_ptr())
     barrier()
@@ -533,6 +550,8 @@ def run_batch(args, w, rank, world, local, dist):
         newton_e2e, bytes_step, launches = across_ranks(dist, [newton_e2e, bytes_step, launches], "sum")
         gathered = [None] * world
         dist.all_gather_object(gathered, stats)
+    if graph[0] is not None:
+        graph[0].close()
     for s in solvers:
         s.close()
     if rank != 0:
@@ -555,7 +574,10 @@ def run_batch(args, w, rank, world, local, dist):
                    "pcg_iterations_per_newton": float(per.mean()),
                    "pcg_iterations_per_newton_histogram": {"edges": HIST_EDGES, "patches": hist.tolist()},
                    "l2": "inputs larger than L2 (every patch's state and operators, about 1.5 GB)",
-                   "setup_s": t_setup, "parallelism": f"patches sharded x{world}"},
+                   "setup_s": t_setup, "autotune_and_capture_s": t_tune,
+                   "launch": ("one graph per batch substep (btd_batch_run), sweep shapes autotuned per patch"
+                              if not args.batch_streams else "one graph per patch, round robin over streams"),
+                   "parallelism": f"patches sharded x{world}"},
         "e2e": {"value": newton_e2e / t_e2e, "unit": "Newton steps/s", "h2d_bytes_per_step": int(bytes_step),
                 "d2h_bytes_per_step": int(bytes_step)},
         "gpu_launches": int(launches),
@@ -585,6 +607,7 @@ def main():
     ap.add_argument("--eager", action="store_true", help="launch kernel by kernel (for per-kernel profilers)")
     ap.add_argument("--patches", type=int, default=512, help="patches of the batch workload")
     ap.add_argument("--dump-patches", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--batch-streams", action="store_true", help="batch workload: one graph per patch on its stream")
     args = ap.parse_args()
     if args.dump_patches:
         dump_patches(args, args.dump_patches)
