@@ -50,6 +50,15 @@ def test_two_sheets_contact_matches_oracle():
     cpu = Oracle(sc, h=h, newton_iterations=4, pcg_iterations=500, pcg_rel_tol=1e-6, self_contact=True, **MG)
     gpu = btd.GpuSolver(sc, btd.configs.solver_params(h, 4, 1e-6, self_contact=1))
     x0, _ = copy_state(cpu, gpu)
+    # the free upper sheet is a detached piece (nothing anchors it): its rigid modes on both sides
+    from btd_b200.topology import Lattice, label_pieces, pack_bits, search
+
+    bits = pack_bits(cpu.segments()["seg_flags"], np.zeros(sc.N, np.float32))
+    lattice = Lattice(sc.layers, sc.N)
+    piece_of, start, nodes, _ = label_pieces(bits, search(bits, sc.pinned, (), lattice), lattice)
+    assert len(start) == 2 and len(nodes) == sc.N - n
+    cpu.set_pieces(piece_of, start, nodes)
+    gpu.set_pieces(piece_of, start, nodes)
     for _ in range(60):
         cpu.substep()
         gpu.substep()

@@ -25,13 +25,30 @@ def gaps(x, n):
     return x[n:, 2][ok] - zl[ok]
 
 
-def pair(sc):
+def pair(sc, pieces=False):
+    """The oracle and the GPU from the same float32 state; with pieces, the layers nothing anchors are
+    set as detached pieces on both (as the reference's topology analysis hands them to its solver)."""
     cpu = Oracle(sc, h=H, newton_iterations=4, pcg_iterations=200, pcg_rel_tol=1e-6, self_contact=True, cross_layer=True, **MG)
     gpu = btd.GpuSolver(sc, btd.configs.solver_params(H, 4, 1e-6, pcg_cap=200, self_contact=1, cross_layer=1))
+    x = sc.position.reshape(-1, 3).astype(np.float32).astype(np.float64)
+    cpu.set_state(x)
+    gpu.set_state(x)
+    if pieces:
+        from btd_b200.topology import Lattice, label_pieces, pack_bits, search
+
+        bits = pack_bits(cpu.segments()["seg_flags"], np.zeros(sc.N, np.float32))
+        lattice = Lattice(sc.layers, sc.N)
+        piece_of, start, nodes, _ = label_pieces(bits, search(bits, sc.pinned, (), lattice), lattice)
+        assert len(start) >= 2
+        cpu.set_pieces(piece_of, start, nodes)
+        gpu.set_pieces(piece_of, start, nodes)
     return cpu, gpu
 
 
 def test_a_ply_laid_on_a_mounted_ply_rests_at_the_contact_distance():
+    """The upper ply is free: nothing anchors it, so it is a detached piece whose rigid modes start
+    every Newton direction (the reference gives it to its solver so; without them the near-singular
+    free ply is beyond an FP32 preconditioner at rel-res 1e-6)."""
     m = btd.material_preset(0)
     sc = btd.compile_scene([btd.layer_spec(m, 0.015, 0.015, bundle=(1, 1), z=z, seed=3) for z in (0.0, 0.0009)])
     L0 = sc.layers[0]
@@ -39,7 +56,7 @@ def test_a_ply_laid_on_a_mounted_ply_rests_at_the_contact_distance():
     i, j = np.arange(n) % L0.nx, np.arange(n) // L0.nx
     sc.pinned[:] = 0
     sc.pinned[:n] = ((i == 0) | (j == 0) | (i == L0.nx - 1) | (j == L0.ny - 1)).astype(np.uint8)
-    cpu, gpu = pair(sc)
+    cpu, gpu = pair(sc, pieces=True)
     worst = np.inf
     for s in range(60):
         cpu.substep()

@@ -136,7 +136,7 @@ def test_basis_matches_the_oracle(weights):
 
 
 def test_learned_pcg_matches_the_oracle(weights):
-    cpu, gpu = staged(weights)
+    cpu, gpu = staged(weights, steps_before=6)
     A0, _ = gpu.read_operator(0)
     b = gpu.read_vector("B")
     cpu.build_levels(A0)

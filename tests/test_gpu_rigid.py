@@ -121,19 +121,23 @@ def test_comb_cut_out_matches_the_oracle(with_pieces):
 
 
 def test_rigid_start_reaches_the_converged_velocity():
+    """A free layer as one piece: two PCG iterations from the rigid start give the velocity of the
+    oracle's converged solve (200 iterations in FP64). (A free layer has no anchor, so its rigid modes
+    are resisted by inertia and drag alone: a plain FP32 V-cycle cannot precondition that near-singular
+    system to rel-res 1e-6, which is why the reference solves detached material this way.)"""
     m = btd.material_preset(0)
     sc = btd.compile_scene([btd.layer_spec(m, 0.02, 0.02, bundle=(1, 1), z=0.1, seed=3)])
     sc.pinned[:] = 0
-    out = {}
-    for name, pcg, pieces in (("rigid", 2, True), ("converged", 500, False)):
-        # the converged solve stops at relative residual 1e-9 (200 fixed iterations in the oracle's FP64)
-        g = btd.GpuSolver(sc, gpu_params(pcg_iterations=pcg, pcg_rel_tol=0.0 if pieces else 1e-9))
-        if pieces:
-            g.set_pieces(np.zeros(sc.N, np.uint32), np.array([0, sc.N], np.uint32), np.arange(sc.N, dtype=np.uint32))
-        g.substeps(10)
-        out[name] = float(g.state()[1][:, 2].mean())
-        g.close()
-    assert abs(out["rigid"] - out["converged"]) < 1e-4 * abs(out["converged"]), out
+    g = btd.GpuSolver(sc, gpu_params())
+    g.set_pieces(np.zeros(sc.N, np.uint32), np.array([0, sc.N], np.uint32), np.arange(sc.N, dtype=np.uint32))
+    g.substeps(10)
+    rigid = float(g.state()[1][:, 2].mean())
+    o = Oracle(sc, **{**SHIPPED, "pcg_iterations": 200})
+    o.set_state(sc.position.reshape(-1, 3).astype(np.float32).astype(np.float64))
+    for _ in range(10):
+        o.substep()
+    converged = float(o.v[:, 2].mean())
+    assert abs(rigid - converged) < 1e-4 * abs(converged), (rigid, converged)
 
 
 def test_set_pieces_rejects_inconsistent_arrays():
