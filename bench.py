@@ -677,6 +677,7 @@ def main():
     value = world * newton_total / t_dev
     launches = gpu.launch_count(args.steps, newton_total, pcg_total)
     levels = gpu.level_count()
+    learned_stats = gpu.learned_stats() if learned is not None else None
 
     # ---- roofline of the dominant kernel (fine-level smoother sweep), live, cold L2 per launch, on the
     # system of the last timed substep
@@ -697,7 +698,6 @@ def main():
             traffic = None
     gpu.close()
 
-    learned_stats = gpu.learned_stats() if learned is not None else None
     # ---- end to end through the C ABI from pinned host buffers: the state in (the previous step's
     # output), the grip targets, one substep, the state out; substeps W + 1 .. W + K of a fresh solver
     g2, drive2 = gpu_arm(btd, w, patch, learned=learned)

@@ -24,7 +24,7 @@ def test_autotuned_run_equals_the_untuned_one(n):
     assert len(choice) == b.level_count()
     for threads, tile, ms in choice:
         assert threads % 32 == 0 and 64 <= threads <= 256
-        assert tile == 128 or tile >= 17
+        assert 0 < tile <= 256
         assert ms > 0
     if n > 128:
         assert any(t in (128, 200) for _, t, _ in choice)

@@ -27,9 +27,12 @@ def gaps(x, n):
 
 def pair(sc, pieces=False):
     """The oracle and the GPU from the same float32 state; with pieces, the layers nothing anchors are
-    set as detached pieces on both (as the reference's topology analysis hands them to its solver)."""
-    cpu = Oracle(sc, h=H, newton_iterations=4, pcg_iterations=200, pcg_rel_tol=1e-6, self_contact=True, cross_layer=True, **MG)
-    gpu = btd.GpuSolver(sc, btd.configs.solver_params(H, 4, 1e-6, pcg_cap=200, self_contact=1, cross_layer=1))
+    set as detached pieces on both (as the reference's topology analysis hands them to its solver), and
+    both run the reference's shipped PCG schedule of two iterations a Newton iteration, from the pieces'
+    rigid start (a free ply's system is beyond an FP32 V-cycle at rel-res 1e-6)."""
+    pcg, tol = (2, 0.0) if pieces else (200, 1e-6)
+    cpu = Oracle(sc, h=H, newton_iterations=4, pcg_iterations=pcg, pcg_rel_tol=tol, self_contact=True, cross_layer=True, **MG)
+    gpu = btd.GpuSolver(sc, btd.configs.solver_params(H, 4, tol, pcg_cap=pcg, self_contact=1, cross_layer=1))
     x = sc.position.reshape(-1, 3).astype(np.float32).astype(np.float64)
     cpu.set_state(x)
     gpu.set_state(x)
