@@ -645,11 +645,13 @@ def main():
     if args.eager:
         gpu.set_graph_mode(False)
 
+    current = [gpu]
+
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
-        gpu.synchronize()
+        current[0].synchronize()
 
     # warm-up: substeps 1..W (captures the substep graph, fills caches)
     for s in range(1, args.warmup + 1):
@@ -701,6 +703,7 @@ def main():
     # ---- end to end through the C ABI from pinned host buffers: the state in (the previous step's
     # output), the grip targets, one substep, the state out; substeps W + 1 .. W + K of a fresh solver
     g2, drive2 = gpu_arm(btd, w, patch, learned=learned)
+    current[0] = g2
     for s in range(1, args.warmup + 1):
         drive2(s)
         g2.substep()
