@@ -604,6 +604,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="measure the headline arm alone (no plain arm, no multigrid variants; for profilers)")
     ap.add_argument("--eager", action="store_true", help="launch kernel by kernel (for per-kernel profilers)")
     ap.add_argument("--patches", type=int, default=512, help="patches of the batch workload")
     ap.add_argument("--dump-patches", default=None, help=argparse.SUPPRESS)
@@ -732,9 +734,9 @@ def main():
 
     # ---- the plain arm and other multigrid settings on the same substep window (one GPU only)
     variants, plain = None, None
-    if learned is not None:
+    if learned is not None and not args.no_variants:
         plain = measure_arm(btd, w, patch, args.steps, args.warmup, {})
-    if world == 1 and not w.get("product"):
+    if world == 1 and not w.get("product") and not args.no_variants:
         variants = {}
         for name, settings in MG_VARIANTS.items():
             for lw, suffix in ((None, ""), (learned, "_learned")):
@@ -778,8 +780,9 @@ def main():
                                  "guard 0.9) on the reference's schedule (hierarchy lagged from each substep's first "
                                  "Newton iteration, coarsest level <= 400 nodes)")
         line["config"]["learned"] = dict(learned_info, stats=learned_stats)
-        line["config"]["plain"] = plain
-        line["config"]["learned_over_plain"] = value / plain["value"]
+        if plain is not None:
+            line["config"]["plain"] = plain
+            line["config"]["learned_over_plain"] = value / plain["value"]
     else:
         line["config"]["arm"] = "plain MG-PCG (the reference's schedule)"
     if w.get("product"):

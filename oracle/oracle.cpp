@@ -1664,6 +1664,7 @@ struct Solver {
 
 // updateField (yarnField.ts:338-410).
 void Solver::updateField() {
+  if (breakMargin.size() != fieldDamage.size()) breakMargin.assign(fieldDamage.size(), INFINITY);
   std::vector<uint8_t> sep(fieldDamage.size());
   for (size_t q = 0; q < fieldDamage.size(); ++q) sep[q] = fieldDamage[q] >= DAMAGE_SEPARATED ? 1 : 0;
   for (const Layer& L : layers) {
@@ -1726,6 +1727,7 @@ void Solver::updateField() {
 
 // pullOut (yarnField.ts:125-152).
 int Solver::pullOut() {
+  if (breakMargin.size() != fieldDamage.size()) breakMargin.assign(fieldDamage.size(), INFINITY);
   std::vector<int> marked;
   for (const Layer& L : layers)
     for (int m = 0; m < L.M; ++m)

@@ -1,8 +1,8 @@
 """Cross-layer contact (contact.ts:7-19, contact.wgsl:31-164) on the CUDA path against the oracle's
 restatement, on the contracts the oracle's own tests pin (two plies at crossing pitch, contact distance
-the mean of their thicknesses, 0.7 mm): a ply laid on a mounted ply rests at the contact distance, and
-mounted plies overlapping by half of it are pushed apart to it; from the same start the GPU's plies
-follow the oracle's. The reference gives a multi-layer scene this contact in place of self-contact
+the mean of their thicknesses, 0.7 mm): a free ply laid on a mounted ply never sinks into it and
+follows the oracle substep by substep, and mounted plies overlapping by half of it are pushed apart to
+it, the GPU's plies following the oracle's from the same start. The reference gives a multi-layer scene this contact in place of self-contact
 (solver.ts:364); the solver does so with the cross_layer parameter.
 """
 import numpy as np
@@ -10,6 +10,7 @@ import pytest
 from scipy.interpolate import LinearNDInterpolator
 
 import btd_b200 as btd
+from helpers import copy_state
 from oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -48,11 +49,7 @@ def pair(sc, pieces=False):
     return cpu, gpu
 
 
-def test_a_ply_laid_on_a_mounted_ply_rests_at_the_contact_distance():
-    """The upper ply is free: nothing anchors it, so it is a detached piece whose rigid modes start
-    every Newton direction, at the reference's shipped schedule of two PCG iterations (without them the
-    near-singular free ply is beyond an FP32 preconditioner). Over 60 substeps it never comes closer to
-    the lower ply than 0.75 of the contact distance, and its gaps follow the oracle's."""
+def laid_ply_scene():
     m = btd.material_preset(0)
     sc = btd.compile_scene([btd.layer_spec(m, 0.015, 0.015, bundle=(1, 1), z=z, seed=3) for z in (0.0, 0.0009)])
     L0 = sc.layers[0]
@@ -60,17 +57,46 @@ def test_a_ply_laid_on_a_mounted_ply_rests_at_the_contact_distance():
     i, j = np.arange(n) % L0.nx, np.arange(n) // L0.nx
     sc.pinned[:] = 0
     sc.pinned[:n] = ((i == 0) | (j == 0) | (i == L0.nx - 1) | (j == L0.ny - 1)).astype(np.uint8)
+    return sc, n
+
+
+def test_a_ply_laid_on_a_mounted_ply_follows_the_oracle_substep_by_substep():
+    """The upper ply is free: nothing anchors it, so it is a detached piece whose rigid modes start
+    every Newton direction, at the reference's shipped schedule of two PCG iterations (without them the
+    near-singular free ply is beyond an FP32 preconditioner). Dropped 0.2 mm onto the mounted ply, it
+    bounces on the contact bounds, and that trajectory is sensitive: in the oracle alone a 1e-9 m
+    perturbation of the start grows to 1e-4 m in three substeps and to the size of the motion by the
+    fifteenth. So the GPU is compared with the oracle one substep at a time, each from the oracle's
+    state rounded to float32, over the oracle's first 30 substeps; the largest node error of a substep
+    is measured against the substep's largest displacement."""
+    sc, n = laid_ply_scene()
     cpu, gpu = pair(sc, pieces=True)
-    worst = np.inf
+    errs = []
+    for _ in range(30):
+        x0, _ = copy_state(cpu, gpu)
+        cpu.substep()
+        gpu.substep()
+        moved = np.abs(cpu.x - x0).max()
+        errs.append(np.abs(gpu.x.astype(np.float64) - cpu.x).max() / moved)
+    errs = np.array(errs)
+    assert np.median(errs) < 0.05 and errs.max() < 0.3, np.round(errs, 4).tolist()
+
+
+def test_a_ply_laid_on_a_mounted_ply_never_sinks_into_it():
+    """Over 60 substeps from the drop, on each side alone, the free ply never comes closer to the
+    lower ply than 0.75 of the contact distance, nor leaves it (median gap within 3 contact distances)."""
+    sc, n = laid_ply_scene()
+    cpu, gpu = pair(sc, pieces=True)
+    worst = {"gpu": np.inf, "oracle": np.inf}
     for s in range(60):
         cpu.substep()
         gpu.substep()
         if s % 5 == 4:
-            worst = min(worst, gaps(gpu.x.astype(np.float64), n).min())
-    g, gc = gaps(gpu.x.astype(np.float64), n), gaps(cpu.x, n)
-    assert worst > 0.75 * R, worst
-    assert abs(np.median(g) - np.median(gc)) < 0.1 * R, (np.median(g), np.median(gc))
-    assert abs(g.min() - gc.min()) < 0.1 * R, (g.min(), gc.min())
+            for side, x in (("gpu", gpu.x.astype(np.float64)), ("oracle", cpu.x)):
+                g = gaps(x, n)
+                worst[side] = min(worst[side], g.min())
+                assert np.median(g) < 3 * R, (side, s, np.median(g))
+    assert min(worst.values()) > 0.75 * R, worst
 
 
 def test_overlapping_mounted_plies_are_pushed_apart_like_the_oracle():
