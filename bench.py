@@ -28,6 +28,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "break-that-denim_b200")
 METRIC = "Newton steps/s at rel-res 1e-6: learned-precond vs plain MG-PCG, 1 B200"
 FALLBACK_HBM_GBS = 6650.0
+CPU_SAMPLE_BUDGET_S = 20.0  # timed oracle work of the GPU arm's CPU baseline (after its untimed warm-up)
+REFERENCE_BUDGET_S = 120.0  # timed oracle work of the reference arm (after its untimed warm-up)
 
 # workloads: (lattice side, patch size m, dt, Newton iterations, relative residual)
 WORKLOADS = {
@@ -213,6 +215,7 @@ def measure_arm(btd, w, patch, steps, warmup, settings=None, learned=None):
         out = {"settings": dict(settings or {}), "learned": learned is not None, "levels": g.level_count(),
                "value": c["newton"] / (ms / 1e3), "unit": "Newton steps/s", "ms_per_step": ms / steps,
                "pcg_iterations_per_newton": c["pcg_total"] / max(1, c["newton"]),
+               "solves_short_of_tolerance": c["pcg_missed"], "worst_rel_residual": c["rel_residual_max"],
                "gpu_launches": int(g.launch_count(steps, c["newton"], c["pcg_total"]))}
         if learned is not None:
             out["learned_stats"] = g.learned_stats()
@@ -255,20 +258,50 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock and throttle-reason samples during the timed region."""
+    """SM clock and throttle-reason samples during the timed region: NVML polled every 5 ms (short
+    timed regions still get samples), else nvidia-smi every 200 ms. Reads only."""
 
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.rows = []  # (sm MHz, max sm MHz, [reason names])
         self.proc = None
+        self.stop = threading.Event()
+        self.source = None
 
     def __enter__(self):
         try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(int(self.index))
+            bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop.is_set():
+                    try:
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), float(mx),
+                                          [n for n, b in zip(self.NAMES, bits) if r & b]))
+                    except Exception:
+                        pass
+                    self.stop.wait(0.005)
+
+            self.source = "nvml"
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            pass
+        try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.source = "nvidia-smi"
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except Exception:
@@ -277,9 +310,16 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([c.strip() for c in line.split(",")])
+            r = [c.strip() for c in line.split(",")]
+            if len(r) < 8 or not r[0].replace(".", "").isdigit():
+                continue
+            self.rows.append((float(r[0]), float(r[1]) if r[1].replace(".", "").isdigit() else None,
+                              [self.NAMES[k] for k in range(4) if r[4 + k] == "Active"]))
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.source == "nvml":
+            self.thread.join(timeout=1)
         if self.proc:
             self.proc.terminate()
             try:
@@ -290,17 +330,18 @@ class ClockSampler:
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 4 + k and r[4 + k] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.rows)}
+        sm = [r[0] for r in self.rows]
+        mx = [r[1] for r in self.rows if r[1]]
+        reasons = sorted({n for r in self.rows for n in r[2]})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows), "source": self.source}
 
 
-def cpu_sample(w, patch, substeps, threads=0, warmup=0):
+def cpu_sample(w, patch, substeps, threads=0, warmup=0, budget=None):
     """The oracle (the reference's CPU solver restated, FP64, OpenMP) on substeps warmup + 1 ..
-    warmup + substeps of the workload (the warm-up ones untimed); returns Newton steps/s, seconds, cores."""
+    warmup + substeps of the workload (the warm-up ones untimed), or fewer when `budget` seconds of
+    timed work run out first (a bounded sample: at least one substep); returns Newton steps/s, seconds,
+    cores and the substeps timed."""
     o, drive = workload_oracle(w, patch, threads)
     cores = threads if threads > 0 else (os.cpu_count() or 1)
     if w.get("contact") and not w.get("product") and not w.get("tearing"):
@@ -312,16 +353,20 @@ def cpu_sample(w, patch, substeps, threads=0, warmup=0):
         t = time.perf_counter()
         o.newton_step()
         dt = time.perf_counter() - t
-        return 1.0 / dt, dt, cores
+        return 1.0 / dt, dt, cores, 0
     for s in range(1, warmup + 1):
         drive(s)
         o.substep()
     t = time.perf_counter()
+    done = 0
     for s in range(warmup + 1, warmup + substeps + 1):
         drive(s)
         o.substep()
+        done += 1
+        if budget is not None and time.perf_counter() - t >= budget:
+            break
     dt = time.perf_counter() - t
-    return substeps * w["newton"] / dt, dt, cores
+    return done * w["newton"] / dt, dt, cores, done
 
 
 def across_ranks(dist, values, op="max", device="cuda"):
@@ -336,16 +381,37 @@ def across_ranks(dist, values, op="max", device="cuda"):
     return [float(v) for v in t.tolist()]
 
 
-def cpu_sample_single_core(w, patch):
-    """The oracle on one host thread, bounded: the first substep's prediction and first Newton
-    iteration of the workload (a whole substep takes tens of seconds on one core at 256 x 256)."""
-    o, drive = workload_oracle(w, patch, threads=1)
-    drive(1)
+def cpu_baselines(w, patch, warmup, steps, budget):
+    """The oracle on the GPU arm's substep window: substeps 1..warmup untimed on all host cores, then
+    substeps warmup + 1 .. timed on all cores until `steps` or `budget` seconds (at least one), then the
+    next substep's prediction and first Newton iteration on one core. Returns (Newton steps/s, seconds,
+    cores, substeps timed) on all cores and (Newton steps/s, seconds, substep) on one."""
+    import ctypes
+
+    o, drive = workload_oracle(w, patch)
+    cores = os.cpu_count() or 1
+    for s in range(1, warmup + 1):
+        drive(s)
+        o.substep()
+    t = time.perf_counter()
+    done = 0
+    for s in range(warmup + 1, warmup + steps + 1):
+        drive(s)
+        o.substep()
+        done += 1
+        if time.perf_counter() - t >= budget:
+            break
+    dt = time.perf_counter() - t
+    gomp = ctypes.CDLL("libgomp.so.1")
+    gomp.omp_set_num_threads(1)
+    s1 = warmup + done + 1
+    drive(s1)
     t = time.perf_counter()
     o.predict()
     o.newton_step()
-    dt = time.perf_counter() - t
-    return 1.0 / dt, dt
+    dt1 = time.perf_counter() - t
+    gomp.omp_set_num_threads(cores)
+    return (done * w["newton"] / dt, dt, cores, done), (1.0 / dt1, dt1, s1)
 
 
 def batch_patches(btd, count):
@@ -427,8 +493,9 @@ def run_reference(args, w, rank):
         sample = f"substeps {args.warmup + 1}..{args.warmup + steps} of the first {len(patches)} patches (warm-up untimed)"
         scaling = "strong"
     else:
-        value, dt, cores = cpu_sample(w, patches[0], steps, warmup=args.warmup)
-        sample = f"substeps {args.warmup + 1}..{args.warmup + steps} x {w['newton']} Newton of the workload (warm-up untimed)"
+        value, dt, cores, done = cpu_sample(w, patches[0], steps, warmup=args.warmup, budget=REFERENCE_BUDGET_S)
+        sample = (f"substeps {args.warmup + 1}..{args.warmup + done} x {w['newton']} Newton of the workload (warm-up untimed"
+                  + (f"; {steps - done} of the {steps} steps left out when {REFERENCE_BUDGET_S} s of timed work ran out)" if done < steps else ")"))
         scaling = "weak"
         if w.get("contact") and not w.get("tearing"):
             sample = "the first substep's second Newton iteration (contacts engaged)"
@@ -606,7 +673,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true",
                     help="measure the headline arm alone (no plain arm, no multigrid variants; for profilers)")
-    ap.add_argument("--eager", action="store_true", help="launch kernel by kernel (for per-kernel profilers)")
+    ap.add_argument("--eager", action="store_true", help="launch the timed substeps kernel by kernel (for per-kernel profilers)")
     ap.add_argument("--patches", type=int, default=512, help="patches of the batch workload")
     ap.add_argument("--dump-patches", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--batch-streams", action="store_true", help="batch workload: one graph per patch on its stream")
@@ -644,8 +711,6 @@ def main():
     # reference's schedule; the plain arm is measured beside it on the same substep window
     learned, learned_info = (learned_weights(btd) if w.get("tearing") else (None, None))
     gpu, drive = gpu_arm(btd, w, patch, learned=learned)
-    if args.eager:
-        gpu.set_graph_mode(False)
 
     current = [gpu]
 
@@ -661,6 +726,8 @@ def main():
         gpu.substep()
     gpu.synchronize()
     gpu.clear_counters()
+    if args.eager:  # the timed substeps kernel by kernel, the warm-up's graphs left out of a profiler's count
+        gpu.set_graph_mode(False)
 
     # ---- device-timed region: substeps W + 1 .. W + K, cold L2 before each (flush outside the events)
     barrier()
@@ -758,6 +825,7 @@ def main():
         "data": "synthetic",
         "config": {"workload": args.workload, "description": w["desc"], "nodes": N, "levels": None,
                    "newton_per_step": w["newton"], "pcg_iterations_per_newton": pcg_total / max(1, newton_total),
+                   "solves_short_of_tolerance": c["pcg_missed"], "worst_rel_residual": c["rel_residual_max"],
                    "substeps_timed": [args.warmup + 1, args.warmup + args.steps],
                    "l2": "flushed before every timed step (256 MiB rewrite outside the events)",
                    "parallelism": f"replicas x{world}"},
@@ -792,15 +860,17 @@ def main():
             "source": "docs/decisions/2026-10-10-feedback-round2.md:11-14 (2 Newton x 2 PCG 6.9 ms + self-contact 0.6 ms)",
             "substep_time_ratio": PRODUCT_PUBLISHED_MS / ms_step}
     if world == 1 and not args.no_cpu_baseline:
-        v_cpu, dt_cpu, cores = cpu_sample(w, patch, 1)
-        what = ("the first substep's second Newton iteration (contacts engaged)" if w.get("contact") and not w.get("product")
-                and not w.get("tearing") else f"substep 1 ({w['newton']} Newton) of the workload from its initial state")
-        line["cpu_baseline"] = {"value": v_cpu, "unit": "Newton steps/s", "cores": cores, "kind": "port",
-                                "sample": f"{what}, {dt_cpu:.1f} s"}
-        if not w.get("contact") or w.get("product") or w.get("tearing"):
-            v1, dt1 = cpu_sample_single_core(w, patch)
+        if w.get("contact") and not w.get("product") and not w.get("tearing"):
+            v_cpu, dt_cpu, cores, _ = cpu_sample(w, patch, 1)
+            line["cpu_baseline"] = {"value": v_cpu, "unit": "Newton steps/s", "cores": cores, "kind": "port",
+                                    "sample": f"the first substep's second Newton iteration (contacts engaged), {dt_cpu:.1f} s"}
+        else:
+            (v_cpu, dt_cpu, cores, done), (v1, dt1, s1) = cpu_baselines(w, patch, args.warmup, args.steps, CPU_SAMPLE_BUDGET_S)
+            line["cpu_baseline"] = {"value": v_cpu, "unit": "Newton steps/s", "cores": cores, "kind": "port",
+                                    "sample": f"substeps {args.warmup + 1}..{args.warmup + done} ({w['newton']} Newton each) of the "
+                                              f"timed window, {dt_cpu:.1f} s (substeps 1..{args.warmup} untimed)"}
             line["cpu_baseline_single_core"] = {"value": v1, "unit": "Newton steps/s", "cores": 1, "kind": "port",
-                                                "sample": f"the first substep's prediction and first Newton iteration, {dt1:.1f} s"}
+                                                "sample": f"substep {s1}'s prediction and first Newton iteration, {dt1:.1f} s"}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

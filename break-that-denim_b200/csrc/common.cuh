@@ -88,7 +88,8 @@ struct Scalars {
 // [12] rejections, [16] PCG iterations last, [17] PCG iterations total, [18] Newton iterations,
 // [19] last relative residual (f32 bits), [20] device error flags.
 constexpr int CNT_RUPTURES = 0, CNT_PULLED = 1, CNT_MAXSPEED = 2, CNT_ALPHA = 3, CNT_UPDATE = 4, CNT_REJECT = 12,
-              CNT_PCG_LAST = 16, CNT_PCG_TOTAL = 17, CNT_NEWTON = 18, CNT_REL = 19, CNT_ERROR = 20, CNT_SIZE = 32;
+              CNT_PCG_LAST = 16, CNT_PCG_TOTAL = 17, CNT_NEWTON = 18, CNT_REL = 19, CNT_ERROR = 20, CNT_REL_MAX = 21,
+              CNT_PCG_MISSED = 22, CNT_SIZE = 32;
 
 // ---------------------------------------------------------------------------------------------- Sym
 
@@ -158,21 +159,41 @@ __device__ __forceinline__ void eigenClamp3(const double (&a)[6], double (&out)[
   out[0] = e(0, 0), out[1] = e(0, 1), out[2] = e(0, 2), out[3] = e(1, 1), out[4] = e(1, 2), out[5] = e(2, 2);
 }
 
+// Symmetric 3 x 3 block in FP64 (xx xy xz yy yz zz).
+struct SymD {
+  double xx, xy, xz, yy, yz, zz;
+};
+__device__ __forceinline__ SymD symD(const Sym& a) { return {a.xx, a.xy, a.xz, a.yy, a.yz, a.zz}; }
+__device__ __forceinline__ SymD symZeroD() { return {0, 0, 0, 0, 0, 0}; }
+__device__ __forceinline__ SymD symIdD(double s) { return {s, 0, 0, s, 0, s}; }
+__device__ __forceinline__ SymD operator+(SymD a, SymD b) {
+  return {a.xx + b.xx, a.xy + b.xy, a.xz + b.xz, a.yy + b.yy, a.yz + b.yz, a.zz + b.zz};
+}
+__device__ __forceinline__ SymD operator*(SymD a, double s) { return {a.xx * s, a.xy * s, a.xz * s, a.yy * s, a.yz * s, a.zz * s}; }
+__device__ __forceinline__ Sym symF(const SymD& a) {
+  return {(float)a.xx, (float)a.xy, (float)a.xz, (float)a.yy, (float)a.yz, (float)a.zz};
+}
+// kPar e e^T + kPerp (I - e e^T) with e a unit vector, in FP64: exactly PSD for kPar, kPerp >= 0.
+__device__ __forceinline__ SymD axialBlockD(double kPar, double kPerp, double ex, double ey, double ez) {
+  const double d = kPar - kPerp;
+  return {d * ex * ex + kPerp, d * ex * ey, d * ex * ez, d * ey * ey + kPerp, d * ey * ez, d * ez * ez + kPerp};
+}
+
 // The spring block of a near-degenerate element (a span or shear diagonal collapsed to under 1 % of its
 // rest length, where the closed-form projection's FP32 direction loses its digits or is undefined): the
 // exact Hessian K e e^T + (f / l) (I - e e^T) of the spring energy, formed in FP64 from the element
 // vector d (FP64) and eigen-clamped; a zero-length element gets max(K, 0) I.
-__device__ __forceinline__ Sym springBlockFP64(double K, double f, double dx, double dy, double dz) {
+__device__ __forceinline__ SymD springBlockFP64D(double K, double f, double dx, double dy, double dz) {
   const double l = sqrt(dx * dx + dy * dy + dz * dz);
-  if (!(l > 0.0)) {
-    const float k = (float)fmax(K, 0.0);
-    return {k, 0.f, 0.f, k, 0.f, k};
-  }
+  if (!(l > 0.0)) return symIdD(fmax(K, 0.0));
   const double ex = dx / l, ey = dy / l, ez = dz / l, kp = f / l, d = K - kp;
   const double a[6] = {d * ex * ex + kp, d * ex * ey, d * ex * ez, d * ey * ey + kp, d * ey * ez, d * ez * ez + kp};
   double o[6];
   eigenClamp3(a, o);
-  return {(float)o[0], (float)o[1], (float)o[2], (float)o[3], (float)o[4], (float)o[5]};
+  return {o[0], o[1], o[2], o[3], o[4], o[5]};
+}
+__device__ __forceinline__ Sym springBlockFP64(double K, double f, double dx, double dy, double dz) {
+  return symF(springBlockFP64D(K, f, dx, dy, dz));
 }
 
 // ---------------------------------------------------------------------------------------------- float3
@@ -440,6 +461,27 @@ __device__ __forceinline__ Sym fineCouplingBlock(const float4* __restrict__ op, 
 }
 // Coarse row: block of offset index o = (dj + 2) * 5 + (di + 2).
 __device__ __forceinline__ Sym coarseBlock(const float4* __restrict__ op, int N, int n, int o) { return loadSymAt(op, N, n, 6 * o); }
+
+// The fine row in FP64, the operator PCG solves with: the same 58 values as the fp32 row (value v in
+// plane v / 2 of N double2), its element blocks exactly PSD in FP64 and summed in FP64, so that a row's
+// stiff terms cancel on a rigid translation as they do in exact arithmetic.
+constexpr int FINE64_PLANES = 29;
+__device__ __forceinline__ SymD loadSymD(const double2* __restrict__ op, int N, int n, int f) {
+  const double2 a = __ldg(&op[(size_t)(f >> 1) * N + n]), b = __ldg(&op[(size_t)((f >> 1) + 1) * N + n]),
+                c = __ldg(&op[(size_t)((f >> 1) + 2) * N + n]);
+  return {a.x, a.y, b.x, b.y, c.x, c.y};
+}
+// Coupling k (0..11) of an FP64 fine row; k = -1 the diagonal block.
+__device__ __forceinline__ SymD fine64Block(const double2* __restrict__ op, int N, int n, int k) {
+  if (k < 8) return loadSymD(op, N, n, 6 * (k + 1));
+  const double2 a = __ldg(&op[(size_t)(27 + ((k - 8) >> 1)) * N + n]);
+  return symIdD(((k - 8) & 1) ? a.y : a.x);
+}
+__device__ __forceinline__ void symDVecAdd(const SymD& A, const double* x, double& y0, double& y1, double& y2) {
+  y0 += A.xx * x[0] + A.xy * x[1] + A.xz * x[2];
+  y1 += A.xy * x[0] + A.yy * x[1] + A.yz * x[2];
+  y2 += A.xz * x[0] + A.yz * x[1] + A.zz * x[2];
+}
 
 __device__ __forceinline__ void storeSymAt(float* row, int f, Sym s) {
   row[f] = s.xx, row[f + 1] = s.xy, row[f + 2] = s.xz, row[f + 3] = s.yy, row[f + 4] = s.yz, row[f + 5] = s.zz;

@@ -87,6 +87,9 @@ struct PcgArgs {
   cudaGraphConditionalHandle cond;  // PCG while-node condition
   int useCond;
   LcState* lc;  // the learned coarse correction's state (null: not enabled)
+  // the fine operator in FP64 (null: the fp32 rows): the operator PCG solves with - its products, the
+  // true residual and the rigid start's residual - while the V-cycle keeps the fp32 rows
+  const double2* op64;
 };
 
 __device__ __forceinline__ double safeDiv(double a, double b) {
@@ -127,6 +130,34 @@ __device__ __forceinline__ void symVecAddD(const Sym& A, const double* x, double
   y2 += (double)A.xz * x[0] + (double)A.yz * x[1] + (double)A.zz * x[2];
 }
 
+// y += (row n of the operator PCG solves with) x, in FP64: the FP64 row when there is one, else the fp32
+// row's products summed in FP64. xAt(m, q) puts node m's x in q and returns false for a node whose x is
+// zero (skipped).
+template <class XAt>
+__device__ __forceinline__ void pcgRowApply(const PcgArgs& a, int n, XAt xAt, double& y0, double& y1, double& y2) {
+  const DLevel& F = a.F;
+  int i, j, l;
+  nodeAt(F, n, &i, &j, &l);
+  const DLevelLayer L = layerOf(F, l);
+  double q[3];
+  if (xAt(n, q)) {
+    if (a.op64)
+      symDVecAdd(loadSymD(a.op64, F.N, n, 0), q, y0, y1, y2);
+    else
+      symVecAddD(FineRows::diag(F.op, F.N, n), q, y0, y1, y2);
+  }
+#pragma unroll
+  for (int k = 0; k < FineRows::NC; ++k) {
+    const int2 off = FineRows::offset(k);
+    const int m = levelNode(L, i + off.x, j + off.y);
+    if (m < 0 || !xAt(m, q)) continue;
+    if (a.op64)
+      symDVecAdd(fine64Block(a.op64, F.N, n, k), q, y0, y1, y2);
+    else
+      symVecAddD(FineRows::coupling(F.op, F.N, n, k), q, y0, y1, y2);
+  }
+}
+
 // The PCG start from the detached pieces' rigid modes (encodeRigidStart, solver.ts:651-657): delta = x0
 // (t + w x r on each piece's nodes, zero elsewhere), r = b - A x0 in FP64 (fixed rows 0), z = 0.
 __global__ void __launch_bounds__(RED_THREADS) k_pcg_init_rigid(PcgArgs a, StepArgs S, RigidArgs R) {
@@ -143,21 +174,16 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_init_rigid(PcgArgs a, StepA
     a.b0[n] = b;
     float3 r = make_float3(0, 0, 0);
     if (!F.fixed[n]) {
-      int i, j, l;
-      nodeAt(F, n, &i, &j, &l);
-      const DLevelLayer L = layerOf(F, l);
       double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-      const double xn[3] = {x0.x, x0.y, x0.z};
-      symVecAddD(FineRows::diag(F.op, F.N, n), xn, y0, y1, y2);
-#pragma unroll
-      for (int k = 0; k < FineRows::NC; ++k) {
-        const int2 off = FineRows::offset(k);
-        const int m = levelNode(L, i + off.x, j + off.y);
-        if (m < 0 || !inPiece(R, m)) continue;
-        const Dv xm = rigidStartAt(S, R, m);
-        const double q[3] = {xm.x, xm.y, xm.z};
-        symVecAddD(FineRows::coupling(F.op, F.N, n, k), q, y0, y1, y2);
-      }
+      pcgRowApply(
+          a, n,
+          [&](int m, double* q) {
+            if (!inPiece(R, m)) return false;
+            const Dv xm = rigidStartAt(S, R, m);
+            q[0] = xm.x, q[1] = xm.y, q[2] = xm.z;
+            return true;
+          },
+          y0, y1, y2);
       r = make_float3((float)(b.x - y0), (float)(b.y - y1), (float)(b.z - y2));
     }
     F.B[n] = make_float4(r.x, r.y, r.z, 0.f);
@@ -226,24 +252,17 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_matvec(PcgArgs a) {
     float3 y = make_float3(0, 0, 0);
     const uint32_t fixedRow = F.fixed[n];
     {
-      int i, j, l;
-      nodeAt(F, n, &i, &j, &l);
-      const DLevelLayer L = layerOf(F, l);
-      // fp32 products summed in FP64: the recurrence residual then drifts from the true one by the
-      // rounding of the stored Ap only
+      // products summed in FP64: the recurrence residual then drifts from the true one by the rounding
+      // of the stored Ap only
       double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-      const float3 pn = f3(a.p[n]);
-      const double pd[3] = {pn.x, pn.y, pn.z};
-      symVecAddD(FineRows::diag(F.op, F.N, n), pd, y0, y1, y2);
-#pragma unroll
-      for (int k = 0; k < FineRows::NC; ++k) {
-        int2 off = FineRows::offset(k);
-        int m = levelNode(L, i + off.x, j + off.y);
-        if (m < 0) continue;
-        const float3 pm = f3(a.p[m]);
-        const double q[3] = {pm.x, pm.y, pm.z};
-        symVecAddD(FineRows::coupling(F.op, F.N, n, k), q, y0, y1, y2);
-      }
+      pcgRowApply(
+          a, n,
+          [&](int m, double* q) {
+            const float4 pm = a.p[m];
+            q[0] = pm.x, q[1] = pm.y, q[2] = pm.z;
+            return true;
+          },
+          y0, y1, y2);
       if (!fixedRow) y = make_float3((float)y0, (float)y1, (float)y2);
     }
     a.Ap[n] = make_float4(y.x, y.y, y.z, 0.f);
@@ -267,6 +286,10 @@ __device__ __forceinline__ void pcgStop(const PcgArgs& a, Scalars& s) {
   a.counters[CNT_PCG_LAST] = (uint32_t)s.pcgIt;
   atomicAdd(&a.counters[CNT_PCG_TOTAL], (uint32_t)s.pcgIt);
   a.counters[CNT_REL] = __float_as_uint((float)s.rel);
+  // the worst relative residual a solve stopped at (non-negative floats order as their bits; NaN above
+  // all) and the solves that stopped short of the tolerance (cap or breakdown)
+  atomicMax(&a.counters[CNT_REL_MAX], __float_as_uint((float)s.rel));
+  if (a.P->pcgTol > 0.0 && !(s.rel <= a.P->pcgTol)) atomicAdd(&a.counters[CNT_PCG_MISSED], 1u);
 }
 
 // delta += alpha p (accumulated in FP64, kept in fp32 too); r -= alpha Ap; z = 0; ||r||. The
@@ -331,19 +354,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_true_residual(PcgArgs a) {
     const float3 b = f3(a.b0[n]);
     double y0 = 0.0, y1 = 0.0, y2 = 0.0;
     const uint32_t fixedRow = F.fixed[n];
-    {
-      int i, j, l;
-      nodeAt(F, n, &i, &j, &l);
-      const DLevelLayer L = layerOf(F, l);
-      symVecAddD(FineRows::diag(F.op, F.N, n), a.dd + 3 * n, y0, y1, y2);
-#pragma unroll
-      for (int k = 0; k < FineRows::NC; ++k) {
-        int2 off = FineRows::offset(k);
-        int m = levelNode(L, i + off.x, j + off.y);
-        if (m < 0) continue;
-        symVecAddD(FineRows::coupling(F.op, F.N, n, k), a.dd + 3 * m, y0, y1, y2);
-      }
-    }
+    pcgRowApply(
+        a, n,
+        [&](int m, double* q) {
+          q[0] = a.dd[3 * m], q[1] = a.dd[3 * m + 1], q[2] = a.dd[3 * m + 2];
+          return true;
+        },
+        y0, y1, y2);
     if (fixedRow) y0 = y1 = y2 = 0.0;
     const double r0 = (double)b.x - y0, r1 = (double)b.y - y1, r2 = (double)b.z - y2;
     a.F.B[n] = make_float4((float)r0, (float)r1, (float)r2, 0.f);

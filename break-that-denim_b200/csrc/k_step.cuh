@@ -297,10 +297,23 @@ __device__ __forceinline__ Sym springBlock(const StepArgs& A, int a, int b, floa
   return springBlockFP64(K, f, dx, dy, dz);
 }
 
+// The same block in FP64 for the FP64 row: the element's direction from its FP64 vector, so that the
+// block is PSD in FP64 whatever the ratio of kPar to kPerp (its FP32 entries round by ~6e-8 kPar, which
+// for a slack span exceeds kPerp and the inertia of a loose strand).
+__device__ __forceinline__ SymD springBlockD(const StepArgs& A, int a, int b, float K, float f, float kPerp, float l, float L) {
+  const float4 xa = A.x[a], xb = A.x[b], da = A.dx[a], db = A.dx[b];
+  const double dx = ((double)xb.x - xa.x) + ((double)db.x - da.x), dy = ((double)xb.y - xa.y) + ((double)db.y - da.y),
+               dz = ((double)xb.z - xa.z) + ((double)db.z - da.z);
+  if (l < DEGENERATE_LENGTH * L) return springBlockFP64D(K, f, dx, dy, dz);
+  const double ld = sqrt(dx * dx + dy * dy + dz * dz);
+  return axialBlockD(K, kPerp, dx / ld, dy / ld, dz / ld);
+}
+
 // Normal stiffness of an active contact bound relative to the node's own diagonal (assemble.wgsl:142).
 constexpr float ACTIVE_BOUND = 100.f;
 
-__global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict__ op, float4* __restrict__ rhs) {
+__global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict__ op, float4* __restrict__ rhs,
+                                                  double2* __restrict__ op64) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= A.N) return;
   const int N = A.N;
@@ -311,6 +324,9 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
     storeSymAt(row, 0, symId(1.f));
 #pragma unroll
     for (int p = 0; p < FINE_PLANES; ++p) op[(size_t)p * N + n] = make_float4(row[4 * p], row[4 * p + 1], row[4 * p + 2], row[4 * p + 3]);
+    if (op64)
+      for (int q = 0; q < FINE64_PLANES; ++q)  // the identity block: values 0, 3 and 5
+        op64[(size_t)q * N + n] = make_double2(q == 0 ? 1.0 : 0.0, q == 1 || q == 2 ? 1.0 : 0.0);
     rhs[n] = make_float4(0, 0, 0, 0);
     return;
   }
@@ -350,6 +366,9 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
   // below) for the rigid frame (assemble.wgsl:172-190, 323-327)
   const bool pieceNode = A.pieceCount > 0 && A.pieceOf[n] < (uint32_t)A.pieceCount;
   Sym Dext = D;
+  // the FP64 row (op64): the same terms summed in FP64, the spans' blocks formed in FP64
+  SymD D64 = symD(D);
+  SymD C1d[4] = {symZeroD(), symZeroD(), symZeroD(), symZeroD()};
 
   // couplings [+u, -u, +v, -v] axial/bending, scalars [+2u, -2u, +2v, -2v]
   Sym C1[4] = {symZero(), symZero(), symZero(), symZero()};
@@ -370,6 +389,11 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
       Sym H = springBlock(A, prev, n, s.kPar, s.fs, s.kPerp, s.e, s.l, s.L);
       D = D + H;
       if (freePrev) C1[km] = C1[km] + H * -1.f;
+      if (op64) {
+        const SymD Hd = springBlockD(A, prev, n, s.kPar, s.fs, s.kPerp, s.l, s.L);
+        D64 = D64 + Hd;
+        if (freePrev) C1d[km] = C1d[km] + Hd * -1.0;
+      }
     }
     if (actNext) {
       SegForce s = segForce(A, n, next, f, L, h);
@@ -377,6 +401,11 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
       Sym H = springBlock(A, n, next, s.kPar, s.fs, s.kPerp, s.e, s.l, s.L);
       D = D + H;
       if (freeNext) C1[kp] = C1[kp] + H * -1.f;
+      if (op64) {
+        const SymD Hd = springBlockD(A, n, next, s.kPar, s.fs, s.kPerp, s.l, s.L);
+        D64 = D64 + Hd;
+        if (freeNext) C1d[kp] = C1d[kp] + Hd * -1.0;
+      }
     }
     if (actPrev && actNext) {
       Triple t = tripleAt(A, prev, n, next, f, L, h);
@@ -384,12 +413,17 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
       D = D + symId(4.f * t.k);
       if (freeNext) C1[kp] = C1[kp] + symId(-2.f * t.wc * t.k);
       if (freePrev) C1[km] = C1[km] + symId(-2.f * t.wa * t.k);
+      D64 = D64 + symIdD(4.0 * t.k);
+      if (freeNext) C1d[kp] = C1d[kp] + symIdD(-2.0 * t.wc * t.k);
+      if (freePrev) C1d[km] = C1d[km] + symIdD(-2.0 * t.wa * t.k);
     }
     if (actNext && activeSpan(A.segs, next, f) && next2 >= 0) {
       Triple t = tripleAt(A, n, next, next2, f, L, h);
       g += t.wa * tripleGrad(t);
       D = D + symId(t.wa * t.wa * t.k);
       if (freeNext) C1[kp] = C1[kp] + symId(-2.f * t.wa * t.k);
+      D64 = D64 + symIdD((double)t.wa * t.wa * t.k);
+      if (freeNext) C1d[kp] = C1d[kp] + symIdD(-2.0 * t.wa * t.k);
       if (!A.pinned[next2]) C2[kp] += t.wa * t.wc * t.k;
     }
     if (actPrev && activeSpan(A.segs, prev2, f)) {
@@ -397,6 +431,8 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
       g += t.wc * tripleGrad(t);
       D = D + symId(t.wc * t.wc * t.k);
       if (freePrev) C1[km] = C1[km] + symId(-2.f * t.wc * t.k);
+      D64 = D64 + symIdD((double)t.wc * t.wc * t.k);
+      if (freePrev) C1d[km] = C1d[km] + symIdD(-2.0 * t.wc * t.k);
       if (!A.pinned[prev2]) C2[km] += t.wa * t.wc * t.k;
     }
   }
@@ -420,6 +456,7 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
     const float Ld = shearRest(A, L, ci, cj);
     Sym H = springBlock(A, n, p, sl.y, sl.x, fmaxf(sl.x, 0.f) / len, e, len, Ld);
     D = D + H;
+    D64 = D64 + symD(H);
     if (!A.pinned[p]) CD[c] = H * -1.f;
   }
 
@@ -433,13 +470,30 @@ __global__ void __launch_bounds__(128) k_assemble(StepArgs A, float4* __restrict
       float3 mv = f3(m);
       if (-dot3(dxn, mv) >= m.w - 1e-3f * fabsf(m.w) && dot3(g, mv) > 0.f) {
         D = D + axialBlock(kAct, 0.f, mv);
+        D64 = D64 + symD(axialBlock(kAct, 0.f, mv));
         Dext = Dext + axialBlock(kAct, 0.f, mv);
       }
     }
   }
   if (onFloorCore && g.z > 0.f) {
     D = D + axialBlock(kAct, 0.f, make_float3(0, 0, 1));
+    D64 = D64 + symD(axialBlock(kAct, 0.f, make_float3(0, 0, 1)));
     Dext = Dext + axialBlock(kAct, 0.f, make_float3(0, 0, 1));
+  }
+  if (op64) {
+    double r64[58];
+    auto put = [&](int f, const SymD& b) {
+      r64[f] = b.xx, r64[f + 1] = b.xy, r64[f + 2] = b.xz, r64[f + 3] = b.yy, r64[f + 4] = b.yz, r64[f + 5] = b.zz;
+    };
+    put(0, D64);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) put(6 * (k + 1), C1d[k]);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) put(6 * (k + 5), symD(CD[k]));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r64[54 + k] = C2[k];
+#pragma unroll
+    for (int q = 0; q < FINE64_PLANES; ++q) op64[(size_t)q * N + n] = make_double2(r64[2 * q], r64[2 * q + 1]);
   }
   if (pieceNode) storeSymAt(A.kx + 6 * (size_t)n, 0, Dext);
 

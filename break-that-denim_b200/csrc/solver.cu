@@ -171,6 +171,9 @@ struct btd_solver {
   float4 *x = nullptr, *v = nullptr, *dx = nullptr, *pred = nullptr, *ext = nullptr, *delta = nullptr, *p = nullptr,
          *Ap = nullptr, *b0 = nullptr;
   double* deltaD = nullptr;
+  // the fine operator in FP64, the operator PCG solves with (null when the solve takes the fp32 rows)
+  double2* op64 = nullptr;
+  bool opFp64 = true;
   Seg* segs = nullptr;
   float *softening = nullptr, *failSite = nullptr, *tails = nullptr, *strain = nullptr, *strength = nullptr;
   uint8_t *damage = nullptr, *area = nullptr, *sep = nullptr, *marks = nullptr;
@@ -327,6 +330,7 @@ struct btd_solver {
     a.cond = h;
     a.useCond = useCond;
     a.lc = lcOn() ? dLc : nullptr;
+    a.op64 = opFp64 ? op64 : nullptr;
     return a;
   }
   HistArgs histArgs() const {
@@ -435,7 +439,7 @@ struct btd_solver {
   }
 
   void encAssemble(cudaStream_t s, bool coarse) {
-    k_assemble<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs(), levels[0].op, levels[0].B);
+    k_assemble<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs(), levels[0].op, levels[0].B, opFp64 ? op64 : nullptr);
     if (pieceCount > 0) {  // the pieces' rigid frames at this iterate (encodeAssemble, solver.ts:615-616)
       k_rigid_rotation<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs(), rigidArgs());
       k_rigid_frame<<<pieceCount, RIGID_THREADS, 0, s>>>(stepArgs(), rigidArgs());
@@ -957,6 +961,7 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
     s->Ap = s->alloc<float4>(N);
     s->b0 = s->alloc<float4>(N);
     s->deltaD = s->alloc<double>(3 * (size_t)N);
+    s->op64 = s->alloc<double2>((size_t)FINE64_PLANES * N);
     s->segs = s->alloc<Seg>(2 * (size_t)N);
     s->softening = s->alloc<float>(2 * (size_t)N);
     s->failSite = s->alloc<float>(2 * (size_t)N);
@@ -1428,6 +1433,18 @@ int btd_set_gradient_precision(btd_solver* s, int32_t fp64) {
     s->hostP.gradFp64 = fp64 ? 1 : 0;
     s->pushParams();
     s->sync();
+  });
+}
+
+static void resetGraphs(btd_solver* s);
+
+int btd_set_operator_precision(btd_solver* s, int32_t fp64) {
+  GUARD({
+    checkSolver(s);
+    if ((fp64 != 0) != s->opFp64) {
+      s->opFp64 = fp64 != 0;
+      resetGraphs(s);
+    }
   });
 }
 

@@ -15,7 +15,8 @@ FINE_ROW = 72  # the reference's fine row floats (solver.ts:99), for readers of 
 COARSE_ROW = 200
 
 COUNTER_NAMES = {0: "ruptures", 1: "pulled_out", 2: "max_speed", 3: "alpha", 12: "rejected", 16: "pcg_last",
-                 17: "pcg_total", 18: "newton", 19: "rel_residual", 20: "errors"}
+                 17: "pcg_total", 18: "newton", 19: "rel_residual", 20: "errors", 21: "rel_residual_max",
+                 22: "pcg_missed"}
 
 
 def default_params(**kw):
@@ -146,6 +147,11 @@ class GpuSolver:
         """The Newton right-hand side in FP64 (default) or FP32 (the reference shader's precision)."""
         check("btd_set_gradient_precision", self._h, int(bool(fp64)))
 
+    def set_operator_precision(self, fp64=True):
+        """The operator PCG solves with: the fine rows assembled in FP64 as well (default), or the FP32
+        rows throughout (the reference shader's precision); the V-cycle keeps the FP32 rows either way."""
+        check("btd_set_operator_precision", self._h, int(bool(fp64)))
+
     def set_pcg(self, max_iterations, rel_tol=0.0):
         check("btd_set_pcg", self._h, int(max_iterations), float(rel_tol))
 
@@ -161,6 +167,7 @@ class GpuSolver:
         d["max_speed"] = float(f[2])
         d["alpha"] = float(f[3])
         d["rel_residual"] = float(f[19])
+        d["rel_residual_max"] = float(f[21])
         d["max_update"] = [float(f[4 + k]) for k in range(8)]
         return d
 

@@ -227,6 +227,14 @@ int btd_set_graph_mode(btd_solver* s, int32_t use_graphs);
  * FP32 operator and PCG solve for; 0 evaluates them in FP32 as the reference's shader does
  * (assemble.wgsl:152-334). The operator stays FP32 either way. */
 int btd_set_gradient_precision(btd_solver* s, int32_t fp64);
+/* Extension: precision of the operator PCG solves with. 1 (default): the fine operator is also assembled
+ * in FP64 - each span's block formed from its FP64 element vector (exactly PSD), every row summed in
+ * FP64 - and PCG's products, its true residual and the rigid start's residual take it, while the
+ * V-cycle (smoothers, transfers, coarse levels) keeps the FP32 rows. In FP32 a row's large span terms
+ * cancel on a rigid motion only to ~6e-8 of their size, which on torn cloth (loose strands held by
+ * inertia alone, ~3e7 times softer than a span) leaves the FP32 operator indefinite and PCG breaks down
+ * short of rel-res 1e-6. 0: the FP32 rows throughout, as the reference's shaders. */
+int btd_set_operator_precision(btd_solver* s, int32_t fp64);
 /* Extension: PCG cap and relative-residual stop (0 = fixed count as the reference). */
 int btd_set_pcg(btd_solver* s, int32_t max_iterations, double rel_tol);
 
@@ -237,7 +245,11 @@ int btd_set_pcg(btd_solver* s, int32_t max_iterations, double rel_tol);
  * header [magic 0x50415244, version 1, node count, sceneHash] then 4 floats a node) is host code
  * around btd_get_state / btd_set_state and btd_scene_hash. */
 int btd_settle_drape(btd_solver* s);
-/* Counters (solver.ts:218-225); n <= BTD_COUNTERS. btd_clear_counters zeroes them. */
+/* Counters (solver.ts:218-225); n <= BTD_COUNTERS. btd_clear_counters zeroes them. Slots: 0 ruptures,
+ * 1 pull-outs, 2 max speed (f32), 3 line-search step (f32), 4-11 Newton updates (f32), 12 rejected,
+ * 16 last PCG count, 17 PCG total, 18 Newton iterations, 19 last relative residual (f32), 20 errors;
+ * extensions: 21 the largest relative residual a PCG solve stopped at (f32), 22 the solves that stopped
+ * short of the relative-residual tolerance (at the cap or on a breakdown). */
 int btd_read_counters(btd_solver* s, uint32_t* out, int32_t n);
 int btd_clear_counters(btd_solver* s);
 

@@ -37,6 +37,7 @@ class OraParams(C.Structure):
         ("self_contact", C.c_int32),
         ("cross_layer", C.c_int32),
         ("coarse_bf16", C.c_int32),
+        ("fp32_rows", C.c_int32),
     ]
 
 
@@ -128,7 +129,8 @@ class Oracle:
 
     def __init__(self, scene, h=1 / 240, gravity=(0, 0, -9.81), newton_iterations=2, pcg_iterations=4,
                  pcg_rel_tol=0.0, max_coarsest_nodes=48, coarse_sweeps=6, line_colors=3, lag_coarse=False,
-                 line_search=False, threads=0, self_contact=False, cross_layer=False, coarse_bf16=False):
+                 line_search=False, threads=0, self_contact=False, cross_layer=False, coarse_bf16=False,
+                 fp32_rows=0):
         p = OraParams()
         p.h = h
         p.gravity[0], p.gravity[1], p.gravity[2] = gravity
@@ -144,6 +146,7 @@ class Oracle:
         p.self_contact = int(self_contact)
         p.cross_layer = int(cross_layer)
         p.coarse_bf16 = int(coarse_bf16)  # 0 off, 1 all blocks, 2 couplings only
+        p.fp32_rows = int(fp32_rows)  # fine level (units) and coarse levels (tens): 0 kept, 1 float32 blocks, 2 float32 row-sum form
         self.scene = scene
         self.N = scene.N
         self.params = p

@@ -1649,6 +1649,7 @@ struct Solver {
   void rhs(double* b) const;
   std::vector<MGLevel> buildHierarchy(std::shared_ptr<StencilOperator> fine) const;
   void vcycle(const std::vector<MGLevel>& levels, int k, double* x, const double* b) const;
+  std::shared_ptr<StencilOperator> pcgOp;  // precision study (fp32_rows 3): PCG's operator apart from the hierarchy's
   void pcg(const std::vector<MGLevel>& levels, const double* b, double* x, int iterations, double tol, int* done,
            double* rel) const;
   double newtonStep(int* pcgDone, double* rel, double* alphaOut);
@@ -2607,6 +2608,31 @@ void smoothLines(const StencilOperator& A, double* x, const double* b, bool reve
   }
 }
 
+// Precision study: the operator as float32 storage would hold it (ora_params.fp32_rows).
+void roundRows(StencilOperator& A, int mode) {
+  if (mode == 0) return;
+  auto rnd = [](double v) { return static_cast<double>(static_cast<float>(v)); };
+  for (int n = 0; n < A.N; ++n) {
+    double* row = &A.A[static_cast<size_t>(n) * STENCIL * 9];
+    if (mode == 1) {
+      for (int q = 0; q < STENCIL * 9; ++q) row[q] = rnd(row[q]);
+      continue;
+    }
+    double sum[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int o = 0; o < STENCIL; ++o)
+      for (int q = 0; q < 9; ++q) sum[q] += row[9 * o + q];
+    for (int q = 0; q < 9; ++q) sum[q] = rnd(sum[q]);
+    for (int o = 0; o < STENCIL; ++o) {
+      if (o == CENTER) continue;
+      for (int q = 0; q < 9; ++q) {
+        row[9 * o + q] = rnd(row[9 * o + q]);
+        sum[q] -= row[9 * o + q];
+      }
+    }
+    for (int q = 0; q < 9; ++q) row[9 * CENTER + q] = sum[q];
+  }
+}
+
 // buildHierarchy (newtonMultigrid.ts:480-491).
 std::vector<MGLevel> Solver::buildHierarchy(std::shared_ptr<StencilOperator> fine) const {
   std::vector<MGLevel> levels;
@@ -2616,6 +2642,7 @@ std::vector<MGLevel> Solver::buildHierarchy(std::shared_ptr<StencilOperator> fin
     std::vector<LatticeLayer> coarse;
     auto P = buildProlongation(*cur, &coarse);
     auto C = galerkin(*cur, coarse, *P);
+    roundRows(*C, prm.fp32_rows / 10);
     if (prm.coarse_bf16)  // precision study: the coarse rows as BF16 storage would hold them
       for (size_t q = 0; q < C->A.size(); ++q) {
         // 2: the 24 coupling blocks only, the diagonal block kept
@@ -3021,7 +3048,7 @@ double dotv(const double* a, const double* b, size_t n) {
 // pcg (newtonMultigrid.ts:537-576) with the relative-residual stop (extension).
 void Solver::pcg(const std::vector<MGLevel>& levels, const double* b, double* x, int iterations, double tol, int* done,
                  double* relOut) const {
-  const StencilOperator& A = *levels[0].A;
+  const StencilOperator& A = pcgOp ? *pcgOp : *levels[0].A;
   size_t n = 3 * static_cast<size_t>(A.N);
   std::vector<double> r(n), Ap(n), z(n, 0.0), p(n);
   A.apply(x, Ap.data());
@@ -3109,6 +3136,15 @@ double Solver::newtonStep(int* pcgDone, double* rel, double* alphaOut) {
   if (contactOn) crossLayer ? crossTerms() : contactTerms();
   std::vector<double> kx;
   auto A = assembleFineOperator(pieceCount > 0 ? &kx : nullptr);
+  // precision study: 3 keeps the operator PCG solves with exact and rounds the preconditioner's copy
+  pcgOp = nullptr;
+  if (prm.fp32_rows % 10 == 3) {
+    pcgOp = A;
+    A = std::make_shared<StencilOperator>(*A);
+    roundRows(*A, 1);
+  } else {
+    roundRows(*A, prm.fp32_rows % 10);
+  }
   // the detached pieces' rigid modes at this iterate (encodeAssemble, solver.ts:615-616)
   if (pieceCount > 0) rigidFrame(kx);
   std::vector<double> b(3 * static_cast<size_t>(N));

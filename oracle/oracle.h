@@ -45,6 +45,11 @@ typedef struct ora_params {
   int32_t coarse_bf16;       /* extension (precision study): every coarse level's operator rounded to BF16
                                 (nearest, ties to even) as it is built, the next level built from the rounded one;
                                 1 all 25 blocks, 2 the 24 coupling blocks (the diagonal block kept) */
+  int32_t fp32_rows;         /* extension (precision study): the operator as float32 storage would hold it
+                                (nearest); units digit the fine level (after assembly), tens digit every coarse
+                                level (after the Galerkin product): 0 kept, 1 every block rounded, 2 the row-sum
+                                form - the couplings and each row's block sum rounded, the diagonal block the
+                                rounded sum less the rounded couplings */
 } ora_params;
 
 typedef struct ora_solver ora_solver;
