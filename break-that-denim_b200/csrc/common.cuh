@@ -69,7 +69,8 @@ struct SimParams {
   double pcgTol;
   float newtonTol;
   int gradFp64;  // the nonlinear residual (the Newton right-hand side) evaluated in FP64
-  int pad1, pad2;
+  int pcgFlex;   // PCG's beta in the flexible (Polak-Ribiere) form, robust to an inexact preconditioner
+  int pad2;
 };
 
 // Device-side scalars of one Newton iteration (FP64 dots, alpha/beta, convergence state).

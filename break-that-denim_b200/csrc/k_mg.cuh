@@ -233,6 +233,36 @@ __global__ void k_residual_fine(DLevel F) {
   F.R[n] = fixedRow ? make_float4(0, 0, 0, 0) : make_float4(r.x, r.y, r.z, 0.f);
 }
 
+// The same residual from the FP64 fine rows (the operator PCG solves with), every product and sum in
+// FP64: on torn cloth the FP32 row's stiff terms cancel on a loose strand's rigid motion only to ~6e-8
+// of their size, which is larger than the strand's inertia, so the V-cycle would restrict noise there.
+__global__ void k_residual_fine64(DLevel F, const double2* __restrict__ op64) {
+  pdlWait();
+  pdlLaunchNext();
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= F.N) return;
+  int i, j, l;
+  nodeAt(F, n, &i, &j, &l);
+  const DLevelLayer L = layerOf(F, l);
+  const uint32_t fixedRow = F.fixed[n];
+  const float4 b = F.B[n], xn4 = F.X[n];
+  double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+  {
+    const double xn[3] = {xn4.x, xn4.y, xn4.z};
+    symDVecAdd(loadSymD(op64, F.N, n, 0), xn, y0, y1, y2);
+  }
+#pragma unroll
+  for (int q = 0; q < 12; ++q) {
+    const int2 o = fineOffset(q);
+    const int ii = i + o.x, jj = j + o.y;
+    if (ii < 0 || jj < 0 || ii >= L.nx || jj >= L.ny) continue;
+    const float4 xm = F.X[L.offset + jj * L.nx + ii];
+    const double x[3] = {xm.x, xm.y, xm.z};
+    symDVecAdd(fine64Block(op64, F.N, n, q), x, y0, y1, y2);
+  }
+  F.R[n] = fixedRow ? make_float4(0, 0, 0, 0) : make_float4((float)(b.x - y0), (float)(b.y - y1), (float)(b.z - y2), 0.f);
+}
+
 // Row dj = R - 2 of the coarse stencil at node n = (i, j): sum over di of A(n, di, dj) x (di = -2..2).
 template <int R>
 __device__ __forceinline__ float3 coarseRowSum(const DLevel& F, const DLevelLayer& L, int n, int i, int j) {

@@ -90,6 +90,7 @@ struct PcgArgs {
   // the fine operator in FP64 (null: the fp32 rows): the operator PCG solves with - its products, the
   // true residual and the rigid start's residual - while the V-cycle keeps the fp32 rows
   const double2* op64;
+  float4* zPrev;  // the previous preconditioned residual (the flexible beta's)
 };
 
 __device__ __forceinline__ double safeDiv(double a, double b) {
@@ -203,23 +204,33 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_init_rigid(PcgArgs a, StepA
 }
 
 // rz' = r . z; first: rz = rz', beta unused; else beta = rz' / rz, rz = rz'.
+// With P.pcgFlex, beta = max(r' . (z' - z), 0) / rz (the flexible, Polak-Ribiere form: equal to the
+// plain one in exact arithmetic with a fixed SPD preconditioner, and robust to one that is applied
+// inexactly), z kept for the next iteration.
 __global__ void __launch_bounds__(RED_THREADS) k_pcg_dot_rz(PcgArgs a, int first) {
   pdlWait();
   pdlLaunchNext();
-  double v[1] = {0.0};
+  const bool flex = a.P->pcgFlex != 0;
+  double v[2] = {0.0, 0.0};
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < a.F.N; n += gridDim.x * blockDim.x) {
-    float3 r = f3(a.F.B[n]), z = f3(a.F.X[n]);
+    const float4 z4 = a.F.X[n];
+    float3 r = f3(a.F.B[n]), z = f3(z4);
     v[0] += (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
+    if (flex) {
+      const float3 zp = f3(a.zPrev[n]);
+      v[1] += (double)r.x * zp.x + (double)r.y * zp.y + (double)r.z * zp.z;
+      a.zPrev[n] = z4;
+    }
   }
-  double out[1];
-  if (gridReduce<1>(a.red, v, out) && threadIdx.x == 0) {
+  double out[2];
+  if (gridReduce<2>(a.red, v, out) && threadIdx.x == 0) {
     Scalars& s = *a.scal;
     if (first || s.restart) {
       s.beta = 0.0;
       s.rz = out[0];
       s.restart = 0;
     } else {
-      s.beta = safeDiv(out[0], s.rz);
+      s.beta = flex ? fmax(safeDiv(out[0] - out[1], s.rz), 0.0) : safeDiv(out[0], s.rz);
       s.rz = out[0];
     }
   }

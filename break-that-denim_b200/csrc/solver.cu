@@ -174,6 +174,7 @@ struct btd_solver {
   // the fine operator in FP64, the operator PCG solves with (null when the solve takes the fp32 rows)
   double2* op64 = nullptr;
   bool opFp64 = true;
+  float4* zPrev = nullptr;
   Seg* segs = nullptr;
   float *softening = nullptr, *failSite = nullptr, *tails = nullptr, *strain = nullptr, *strength = nullptr;
   uint8_t *damage = nullptr, *area = nullptr, *sep = nullptr, *marks = nullptr;
@@ -331,6 +332,7 @@ struct btd_solver {
     a.useCond = useCond;
     a.lc = lcOn() ? dLc : nullptr;
     a.op64 = opFp64 ? op64 : nullptr;
+    a.zPrev = zPrev;
     return a;
   }
   HistArgs histArgs() const {
@@ -526,7 +528,9 @@ struct btd_solver {
     Level& F = levels[k];
     Level& Cl = levels[k + 1];
     encSmooth(s, k, false);
-    if (F.fine)
+    if (F.fine && opFp64)
+      launch(k_residual_fine64, blocksFor(F.N, 128), 128, 0, s, F.dev(), (const double2*)op64);
+    else if (F.fine)
       launch(k_residual_fine, blocksFor(F.N, 128), 128, 0, s, F.dev());
     else
       launch(k_residual_coarse, blocksFor(8 * F.N, 128), 128, 0, s, F.dev());
@@ -962,6 +966,7 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
     s->b0 = s->alloc<float4>(N);
     s->deltaD = s->alloc<double>(3 * (size_t)N);
     s->op64 = s->alloc<double2>((size_t)FINE64_PLANES * N);
+    s->zPrev = s->alloc<float4>(N);
     s->segs = s->alloc<Seg>(2 * (size_t)N);
     s->softening = s->alloc<float>(2 * (size_t)N);
     s->failSite = s->alloc<float>(2 * (size_t)N);
@@ -1431,6 +1436,15 @@ int btd_set_gradient_precision(btd_solver* s, int32_t fp64) {
   GUARD({
     checkSolver(s);
     s->hostP.gradFp64 = fp64 ? 1 : 0;
+    s->pushParams();
+    s->sync();
+  });
+}
+
+int btd_set_pcg_flexible(btd_solver* s, int32_t on) {
+  GUARD({
+    checkSolver(s);
+    s->hostP.pcgFlex = on ? 1 : 0;
     s->pushParams();
     s->sync();
   });

@@ -152,6 +152,10 @@ class GpuSolver:
         rows throughout (the reference shader's precision); the V-cycle keeps the FP32 rows either way."""
         check("btd_set_operator_precision", self._h, int(bool(fp64)))
 
+    def set_pcg_flexible(self, on=True):
+        """PCG's beta in the flexible (Polak-Ribiere) form, or the reference's form (default)."""
+        check("btd_set_pcg_flexible", self._h, int(bool(on)))
+
     def set_pcg(self, max_iterations, rel_tol=0.0):
         check("btd_set_pcg", self._h, int(max_iterations), float(rel_tol))
 

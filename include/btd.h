@@ -229,12 +229,17 @@ int btd_set_graph_mode(btd_solver* s, int32_t use_graphs);
 int btd_set_gradient_precision(btd_solver* s, int32_t fp64);
 /* Extension: precision of the operator PCG solves with. 1 (default): the fine operator is also assembled
  * in FP64 - each span's block formed from its FP64 element vector (exactly PSD), every row summed in
- * FP64 - and PCG's products, its true residual and the rigid start's residual take it, while the
- * V-cycle (smoothers, transfers, coarse levels) keeps the FP32 rows. In FP32 a row's large span terms
+ * FP64 - and PCG's products, its true residual, the rigid start's residual and the V-cycle's fine
+ * residual take it, while the smoothers, transfers and coarse levels keep the FP32 rows. In FP32 a row's large span terms
  * cancel on a rigid motion only to ~6e-8 of their size, which on torn cloth (loose strands held by
  * inertia alone, ~3e7 times softer than a span) leaves the FP32 operator indefinite and PCG breaks down
  * short of rel-res 1e-6. 0: the FP32 rows throughout, as the reference's shaders. */
 int btd_set_operator_precision(btd_solver* s, int32_t fp64);
+/* Extension: PCG's beta in the flexible (Polak-Ribiere) form, max(r' . (z' - z), 0) / (r . z), which
+ * equals the plain form in exact arithmetic with a fixed SPD preconditioner and stays a descent method
+ * when the preconditioner is applied inexactly (FP32 V-cycle, learned correction); 0 (default) the
+ * reference's form r' . z' / (r . z). */
+int btd_set_pcg_flexible(btd_solver* s, int32_t on);
 /* Extension: PCG cap and relative-residual stop (0 = fixed count as the reference). */
 int btd_set_pcg(btd_solver* s, int32_t max_iterations, double rel_tol);
 

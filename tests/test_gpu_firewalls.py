@@ -93,9 +93,11 @@ def test_non_positive_curvature_stops_pcg_with_a_zero_step():
     torch.cuda.synchronize()
     g.set_pcg(500, 1e-6)
     g.write_vector("B", b)
+    g.set_operator_precision(False)  # PCG's operator: the fp32 rows written above
     g.encode_pcg()
     d = g.read_vector("delta")
     c = g.counter_dict()
+    g.set_operator_precision(True)
     assert np.isfinite(d).all() and np.abs(d).max() == 0.0
     assert c["pcg_last"] == 1
     # the next substep assembles afresh and runs normally

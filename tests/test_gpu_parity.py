@@ -108,13 +108,21 @@ def test_pcg_relative_residual_stop(staged):
 
 def test_pcg_stops_on_the_fp64_true_residual(staged):
     """At rel-res 1e-6 the stop is decided by the outer residual b - A delta computed in FP64 from
-    the fp32 operator and the iterate accumulated in FP64 (an fp32 iterate alone bottoms out near
-    4e-6 on this coupon): recomputed here from the read-back operator, it meets the bound."""
+    the iterate accumulated in FP64 (an fp32 iterate alone bottoms out near 4e-6 on this coupon). With
+    the fp32 rows as PCG's operator it is recomputed here from the read-back operator and meets the
+    bound; with the FP64 rows (the default) the solve reports it met as well."""
     sc, cpu, gpu = staged
     A_gpu, _ = gpu.read_operator(0)
     b = gpu.read_vector("B")
     gpu.set_pcg(500, 1e-6)
     gpu.encode_pcg()
+    assert gpu.counter_dict()["rel_residual"] <= 1e-6
+    gpu.write_vector("B", b)
+    gpu.set_operator_precision(False)
+    try:
+        gpu.encode_pcg()
+    finally:
+        gpu.set_operator_precision(True)
     d = gpu.delta_f64()
     d32 = gpu.read_vector("delta")
     c = gpu.counter_dict()
