@@ -32,6 +32,7 @@
 #include "k_rigid.cuh"
 #include "k_smooth.cuh"
 #include "k_step.cuh"
+#include "k_vtail.cuh"
 
 namespace btd {
 void setError(const std::string& msg);
@@ -174,6 +175,8 @@ struct btd_solver {
   // the fine operator in FP64, the operator PCG solves with (null when the solve takes the fp32 rows)
   double2* op64 = nullptr;
   bool opFp64 = true;
+  // the V-cycle's bottom two levels in one cluster launch (k_vtail) where they qualify
+  bool tailOn = true;
   float4* zPrev = nullptr;
   Seg* segs = nullptr;
   float *softening = nullptr, *failSite = nullptr, *tails = nullptr, *strain = nullptr, *strength = nullptr;
@@ -487,6 +490,63 @@ struct btd_solver {
     CK(cudaLaunchKernelEx(&cfg, k, args...));
   }
 
+  // The bottom two levels qualify for k_vtail: the upper one coarse, both of a single layer, every colour
+  // of both at most TAIL_MAX_CTAS lines; returns the cluster size (0: not eligible or switched off).
+  int tailCtas() const {
+    const int L = (int)levels.size();
+    if (!tailOn || L < 2) return 0;
+    int cl = 0;
+    for (int k = L - 2; k < L; ++k) {
+      const Level& v = levels[k];
+      if (v.fine || v.layers.size() != 1) return 0;
+      for (int c = 0; c < 6; ++c) {
+        if (v.geom[c].table) return 0;
+        cl = std::max(cl, v.colourStart[c + 1] - v.colourStart[c]);
+      }
+    }
+    return cl >= 1 && cl <= TAIL_MAX_CTAS ? cl : 0;
+  }
+  TailLevel tailLevel(int k) const {
+    const Level& v = levels[k];
+    TailLevel t;
+    t.L = v.dev();
+    for (int c = 0; c < 6; ++c) {
+      t.geom[c] = v.geom[c];
+      t.count[c] = v.colourStart[c + 1] - v.colourStart[c];
+    }
+    t.fac = v.fac;
+    t.T = v.tile;
+    return t;
+  }
+  void launchTail(cudaStream_t s, int cl, bool down, int from, int to, bool up) {
+    const int L = (int)levels.size();
+    TailArgs a;
+    a.up = tailLevel(L - 2);
+    a.bottom = tailLevel(L - 1);
+    a.down = down ? 1 : 0;
+    a.sweepsFrom = from;
+    a.sweepsTo = to;
+    a.upward = up ? 1 : 0;
+    a.err = dCounters + CNT_ERROR;
+    const Level& U = levels[L - 2];
+    const Level& B = levels[L - 1];
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cl);
+    cfg.blockDim = dim3(std::max(U.threads, B.threads));
+    cfg.dynamicSmemBytes = std::max(smoothSmemBytes<CoarseRows>(U.maxLine, U.tile), smoothSmemBytes<CoarseRows>(B.maxLine, B.tile));
+    cfg.stream = s;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = params.overlap_launches ? 2 : 1;
+    CK(cudaLaunchKernelEx(&cfg, k_vtail, a));
+  }
+
   void encSmooth(cudaStream_t s, int k, bool reverse) {
     Level& L = levels[k];
     const size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine, L.tile) : smoothSmemBytes<CoarseRows>(L.maxLine, L.tile);
@@ -513,6 +573,18 @@ struct btd_solver {
   // encodeVCycle (solver.ts:584-598): X of level k = V(B) with X zero on entry.
   void encVCycle(cudaStream_t s, int k) {
     int last = (int)levels.size() - 1;
+    const int cl = k == last - 1 ? tailCtas() : 0;
+    if (cl > 0) {  // the bottom two levels in one cluster launch (two around the learned correction)
+      if (lcOn()) {
+        const int half = params.coarse_sweeps / 2;
+        launchTail(s, cl, true, 0, half, false);
+        launch(k_lc_correct, 1, LC_THREADS, 0, s, levels[last].dev(), lcArgs());
+        launchTail(s, cl, false, half, params.coarse_sweeps, true);
+      } else {
+        launchTail(s, cl, true, 0, params.coarse_sweeps, true);
+      }
+      return;
+    }
     if (k == last) {
       if (lcOn()) {
         // the learned coarse space half-way through the coarsest sweeps, which mirror around it
@@ -1075,6 +1147,8 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
         set((const void*)k_smooth<CoarseRows, 1>);
         set((const void*)k_line_factor<FineRows>);
         set((const void*)k_line_factor<CoarseRows>);
+        set((const void*)k_vtail);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_vtail, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         smemErr = e;
       });
       CK(smemErr);
@@ -1438,6 +1512,18 @@ int btd_set_gradient_precision(btd_solver* s, int32_t fp64) {
     s->hostP.gradFp64 = fp64 ? 1 : 0;
     s->pushParams();
     s->sync();
+  });
+}
+
+static void resetGraphs(btd_solver* s);
+
+int btd_set_vcycle_tail(btd_solver* s, int32_t on) {
+  GUARD({
+    checkSolver(s);
+    if ((on != 0) != s->tailOn) {
+      s->tailOn = on != 0;
+      resetGraphs(s);
+    }
   });
 }
 
@@ -1867,8 +1953,12 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
       return (int64_t)c;
     };
     const int L = (int)s->levels.size();
-    int64_t V = s->params.coarse_sweeps * colours(L - 1);
+    const int64_t lc = s->lcOn() ? 1 : 0;
+    int64_t V = s->params.coarse_sweeps * colours(L - 1) + lc;
     for (int k = 0; k + 1 < L; ++k) V += 2 * colours(k) + 3;
+    // the bottom two levels in one cluster launch: their colour launches and transfers become one
+    // launch (two around the learned correction)
+    if (s->tailCtas() > 0) V -= s->params.coarse_sweeps * colours(L - 1) + 2 * colours(L - 2) + 3 - (1 + lc);
     // per Newton iteration: assembly, PCG prologue (init + V-cycle + 5), line search, apply; the
     // hierarchy (weights + RAP per coarse level) on the first iteration; V-cycle + 5 per extra PCG pass
     // held grips add their lead once per substep and their terms once per Newton iteration; the
@@ -1879,7 +1969,8 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
     // detached pieces add rotation + frame after the assembly, start (+ the init it replaces) and curves
     const int64_t rigid = s->pieceCount > 0 ? 1 : 0;
     const int64_t xc = s->xcOn() ? 1 : 0;  // cross-layer contact: terms in one kernel, detection in four
-    const int64_t perNewton = 2 + (1 + V + 5) + 1 + 1 + grips + (2 - xc) * contact + 4 * rigid;
+    // the learned correction adds its flags (fine, then one a coarse level) and basis to every solve
+    const int64_t perNewton = 2 + (1 + V + 5) + 1 + 1 + grips + (2 - xc) * contact + 4 * rigid + lc * (L + 1);
     const int64_t hierarchy = 3 * (L - 1);
     const int64_t hierPerSubstep = s->params.lag_coarse ? hierarchy : hierarchy * (newton / std::max(1, substeps));
     const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips + (6 - 2 * xc) * contact + 2 * rigid;

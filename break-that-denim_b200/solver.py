@@ -148,13 +148,18 @@ class GpuSolver:
         check("btd_set_gradient_precision", self._h, int(bool(fp64)))
 
     def set_operator_precision(self, fp64=True):
-        """The operator PCG solves with: the fine rows assembled in FP64 as well (default), or the FP32
-        rows throughout (the reference shader's precision); the V-cycle keeps the FP32 rows either way."""
+        """The operator PCG solves with: the fine rows assembled in FP64 as well (default; PCG's products and
+        the V-cycle's fine residual take them), or the FP32 rows throughout (the reference shader's
+        precision); the smoothers and coarse levels keep the FP32 rows either way."""
         check("btd_set_operator_precision", self._h, int(bool(fp64)))
 
     def set_pcg_flexible(self, on=True):
         """PCG's beta in the flexible (Polak-Ribiere) form, or the reference's form (default)."""
         check("btd_set_pcg_flexible", self._h, int(bool(on)))
+
+    def set_vcycle_tail(self, on=True):
+        """The V-cycle's bottom two levels in one cluster launch (default) or a launch a colour pass."""
+        check("btd_set_vcycle_tail", self._h, int(bool(on)))
 
     def set_pcg(self, max_iterations, rel_tol=0.0):
         check("btd_set_pcg", self._h, int(max_iterations), float(rel_tol))
