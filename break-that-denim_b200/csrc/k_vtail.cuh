@@ -3,12 +3,14 @@
 // post-sweep) - 27 dependent launches of small grids (one CTA a line, 6-11 lines a colour at 256 x 256)
 // become one, with a cluster barrier between the passes in place of a launch boundary.
 //
-// CTA b of the cluster solves line b of every colour pass (sweepLine, the same device code and the same
-// arithmetic as k_smooth, so the result is the same bit for bit); the residual, restriction and
-// prolongation run over the cluster's threads with the kernels' per-node device code. Every CTA takes
-// every barrier: the passes and their line counts are kernel parameters, the same for all CTAs, and no
-// CTA leaves early. The unknowns one pass writes reach the next pass's CTAs through global memory (L2;
-// the staging loads bypass L1), ordered by a device-scope fence and the barrier's release/acquire.
+// A cluster of 16 CTAs: CTA b solves line b of every colour pass (sweepLine, the same device code and the
+// same arithmetic as k_smooth, so the result is the same bit for bit; CTAs past a colour's line count
+// wait), and the residual, restriction and prolongation run over all the cluster's threads with the
+// kernels' per-node device code. The pass list is a kernel parameter, the same for every CTA, and no CTA
+// leaves early, so every CTA takes every barrier. The unknowns one pass writes reach the next pass's CTAs
+// through global memory (L2; the staging loads bypass L1), ordered by the barrier's release / acquire;
+// each CTA issues its next line's factor copies before the barrier, as k_smooth does before its
+// programmatic-launch wait. Off by default (btd_set_vcycle_tail): measured slower than the launches.
 #pragma once
 
 #include "common.cuh"
@@ -29,12 +31,14 @@ struct TailLevel {
   int T;
 };
 
+// A pass of the tail: a colour pass of one level's sweep, or a transfer over the cluster's threads.
+enum TailKind : int { TAIL_SWEEP = 0, TAIL_RESIDUAL = 1, TAIL_RESTRICT = 2, TAIL_PROLONG = 3 };
+constexpr int TAIL_MAX_PASSES = 64;
+
 struct TailArgs {
-  TailLevel up;      // the level above the coarsest
-  TailLevel bottom;  // the coarsest level
-  int down;          // run the way down: pre-sweep of `up`, its residual, the restriction
-  int sweepsFrom, sweepsTo;  // the coarsest level's sweeps [from, to) (odd ones reversed)
-  int upward;        // run the way up: prolongation into `up`, its post-sweep (reversed)
+  TailLevel lv[2];  // 0: the level above the coarsest, 1: the coarsest level
+  int passes;
+  int8_t kind[TAIL_MAX_PASSES], level[TAIL_MAX_PASSES], colour[TAIL_MAX_PASSES];
   uint32_t* err;
 };
 
@@ -48,70 +52,84 @@ __device__ __forceinline__ unsigned tailCtas() {
   asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
   return r;
 }
-// Every thread of the cluster: this pass's global writes ordered before the next pass's reads.
+// Every thread of the cluster; the barrier's release / acquire order each pass's global writes (the
+// unknowns, residuals, restricted right-hand sides) before the next pass's reads in any CTA.
 __device__ __forceinline__ void tailSync() {
   __syncwarp();
-  __threadfence();
   asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
   asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
-}
-
-__device__ __forceinline__ void tailSweep(const TailLevel& t, bool reverse, float4* sm4, uint64_t* bar, unsigned& phase, uint32_t* err) {
-  const int b = (int)tailRank();
-  for (int q = 0; q < 6; ++q) {
-    const int c = reverse ? 5 - q : q;
-    if (t.count[c] == 0) continue;
-    if (b < t.count[c]) {
-      const LineAt a = lineAt(t.geom[c], b);
-      if (c < 3)
-        sweepLine<CoarseRows, 1>(t.L, a, t.fac, t.T, err, sm4, bar, phase, false);
-      else
-        sweepLine<CoarseRows, 0>(t.L, a, t.fac, t.T, err, sm4, bar, phase, false);
-    }
-    tailSync();
-  }
 }
 
 __global__ void __launch_bounds__(SM_SWEEP_THREADS, 1) k_vtail(TailArgs a) {
   __shared__ uint64_t bar;
   extern __shared__ float4 sm4[];
-  if (threadIdx.x == 0) mbarInit(&bar, 1);
+  const int b = (int)tailRank();
+  // the first pass's line copies (factors and couplings are the factorisation's, launches back) are
+  // issued before waiting for the preceding kernel, as k_smooth does
+  bool prefetched = false;
+  if (threadIdx.x == 0) {
+    mbarInit(&bar, 1);
+    if (a.passes > 0 && a.kind[0] == TAIL_SWEEP && b < a.lv[a.level[0]].count[a.colour[0]]) {
+      const TailLevel& t = a.lv[a.level[0]];
+      issueLineCopies<CoarseRows>(lineAt(t.geom[a.colour[0]], b), t.fac, t.T, sm4, &bar);
+    }
+  }
+  prefetched = a.passes > 0 && a.kind[0] == TAIL_SWEEP && b < a.lv[a.level[0]].count[a.colour[0]];
   pdlWait();
   pdlLaunchNext();
   __syncthreads();
   unsigned phase = 0;
   const int nt = (int)(blockDim.x * tailCtas());
-  const int me = (int)(tailRank() * blockDim.x + threadIdx.x);
-  const DLevel& F = a.up.L;
-  const DLevel& C = a.bottom.L;
-  if (a.down) {
-    tailSweep(a.up, false, sm4, &bar, phase, a.err);
-    // residual of the upper level, eight threads a node (whole warps in every round)
-    for (int it0 = 0; it0 < 8 * F.N; it0 += nt) {
-      const int it = it0 + me;
-      const bool valid = it < 8 * F.N;
-      const int n = valid ? it >> 3 : 0;
-      int i = 0, j = 0, l = 0;
-      if (valid) nodeAt(F, n, &i, &j, &l);
-      coarseResidualLane(F, layerOf(F, l), n, i, j, it & 7, valid);
+  const int me = (int)(b * blockDim.x + threadIdx.x);
+  const DLevel& F = a.lv[0].L;
+  const DLevel& C = a.lv[1].L;
+  for (int p = 0; p < a.passes; ++p) {
+    const int kind = a.kind[p];
+    if (kind == TAIL_SWEEP) {
+      const TailLevel& t = a.lv[a.level[p]];
+      const int c = a.colour[p];
+      if (b < t.count[c]) {
+        const LineAt ln = lineAt(t.geom[c], b);
+        if (c < 3)
+          sweepLine<CoarseRows, 1>(t.L, ln, t.fac, t.T, a.err, sm4, &bar, phase, prefetched);
+        else
+          sweepLine<CoarseRows, 0>(t.L, ln, t.fac, t.T, a.err, sm4, &bar, phase, prefetched);
+      }
+    } else if (kind == TAIL_RESIDUAL) {
+      // eight threads a node, whole warps in every round
+      for (int it0 = 0; it0 < 8 * F.N; it0 += nt) {
+        const int it = it0 + me;
+        const bool valid = it < 8 * F.N;
+        const int n = valid ? it >> 3 : 0;
+        int i = 0, j = 0, l = 0;
+        if (valid) nodeAt(F, n, &i, &j, &l);
+        coarseResidualLane(F, layerOf(F, l), n, i, j, it & 7, valid);
+      }
+    } else if (kind == TAIL_RESTRICT) {
+      for (int I = me; I < C.N; I += nt) {
+        int ci, cj, l;
+        nodeAt(C, I, &ci, &cj, &l);
+        restrictAt(F, C, layerOf(F, l), I, ci, cj);
+      }
+    } else {
+      for (int n = me; n < F.N; n += nt) {
+        int i, j, l;
+        nodeAt(F, n, &i, &j, &l);
+        prolongAt(F, C, layerOf(F, l), layerOf(C, l), n, i, j);
+      }
+    }
+    // the next pass's line copies into this CTA's shared memory before the barrier (they read only the
+    // factorisation's output), once every thread is done with the current contents
+    prefetched = false;
+    if (p + 1 < a.passes && a.kind[p + 1] == TAIL_SWEEP && b < a.lv[a.level[p + 1]].count[a.colour[p + 1]]) {
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        const TailLevel& t = a.lv[a.level[p + 1]];
+        issueLineCopies<CoarseRows>(lineAt(t.geom[a.colour[p + 1]], b), t.fac, t.T, sm4, &bar);
+      }
+      prefetched = true;
     }
     tailSync();
-    for (int I = me; I < C.N; I += nt) {
-      int ci, cj, l;
-      nodeAt(C, I, &ci, &cj, &l);
-      restrictAt(F, C, layerOf(F, l), I, ci, cj);
-    }
-    tailSync();
-  }
-  for (int sw = a.sweepsFrom; sw < a.sweepsTo; ++sw) tailSweep(a.bottom, (sw & 1) == 1, sm4, &bar, phase, a.err);
-  if (a.upward) {
-    for (int n = me; n < F.N; n += nt) {
-      int i, j, l;
-      nodeAt(F, n, &i, &j, &l);
-      prolongAt(F, C, layerOf(F, l), layerOf(C, l), n, i, j);
-    }
-    tailSync();
-    tailSweep(a.up, true, sm4, &bar, phase, a.err);
   }
 }
 

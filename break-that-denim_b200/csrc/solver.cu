@@ -175,8 +175,10 @@ struct btd_solver {
   // the fine operator in FP64, the operator PCG solves with (null when the solve takes the fp32 rows)
   double2* op64 = nullptr;
   bool opFp64 = true;
-  // the V-cycle's bottom two levels in one cluster launch (k_vtail) where they qualify
-  bool tailOn = true;
+  // the V-cycle's bottom two levels in one cluster launch (k_vtail) where they qualify; off by default:
+  // measured slower than the launch-per-pass path (whose programmatic dependent launches already overlap
+  // each pass's staging with the previous pass), 0.366 against 0.326 ms a V-cycle at 256 x 256
+  bool tailOn = false;
   float4* zPrev = nullptr;
   Seg* segs = nullptr;
   float *softening = nullptr, *failSite = nullptr, *tails = nullptr, *strain = nullptr, *strength = nullptr;
@@ -494,7 +496,7 @@ struct btd_solver {
   // of both at most TAIL_MAX_CTAS lines; returns the cluster size (0: not eligible or switched off).
   int tailCtas() const {
     const int L = (int)levels.size();
-    if (!tailOn || L < 2) return 0;
+    if (!tailOn || L < 2 || 15 + 6 * params.coarse_sweeps > TAIL_MAX_PASSES) return 0;
     int cl = 0;
     for (int k = L - 2; k < L; ++k) {
       const Level& v = levels[k];
@@ -518,26 +520,48 @@ struct btd_solver {
     t.T = v.tile;
     return t;
   }
-  void launchTail(cudaStream_t s, int cl, bool down, int from, int to, bool up) {
+  void launchTail(cudaStream_t s, int lines, bool down, int from, int to, bool up) {
     const int L = (int)levels.size();
     TailArgs a;
-    a.up = tailLevel(L - 2);
-    a.bottom = tailLevel(L - 1);
-    a.down = down ? 1 : 0;
-    a.sweepsFrom = from;
-    a.sweepsTo = to;
-    a.upward = up ? 1 : 0;
+    a.lv[0] = tailLevel(L - 2);
+    a.lv[1] = tailLevel(L - 1);
+    a.passes = 0;
+    auto push = [&](int kind, int lv, int c) {
+      if (a.passes >= TAIL_MAX_PASSES) throw std::logic_error("k_vtail: too many passes");
+      a.kind[a.passes] = (int8_t)kind, a.level[a.passes] = (int8_t)lv, a.colour[a.passes] = (int8_t)c;
+      a.passes++;
+    };
+    auto sweep = [&](int lv, bool reverse) {
+      for (int q = 0; q < 6; ++q) {
+        const int c = reverse ? 5 - q : q;
+        if (a.lv[lv].count[c] > 0) push(TAIL_SWEEP, lv, c);
+      }
+    };
+    if (down) {
+      sweep(0, false);
+      push(TAIL_RESIDUAL, 0, 0);
+      push(TAIL_RESTRICT, 0, 0);
+    }
+    for (int sw = from; sw < to; ++sw) sweep(1, (sw & 1) == 1);
+    if (up) {
+      push(TAIL_PROLONG, 0, 0);
+      sweep(0, true);
+    }
     a.err = dCounters + CNT_ERROR;
     const Level& U = levels[L - 2];
     const Level& B = levels[L - 1];
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(cl);
-    cfg.blockDim = dim3(std::max(U.threads, B.threads));
+    // the transfers run over every thread of the cluster: the widest cluster and CTA (the sweeps
+    // stride by the CTA size and leave the CTAs past a colour's line count idle); `lines` (the most
+    // lines of a colour) only has to fit
+    if (lines > TAIL_MAX_CTAS) throw std::logic_error("k_vtail: more lines a colour than CTAs");
+    cfg.gridDim = dim3(TAIL_MAX_CTAS);
+    cfg.blockDim = dim3(SM_SWEEP_THREADS);
     cfg.dynamicSmemBytes = std::max(smoothSmemBytes<CoarseRows>(U.maxLine, U.tile), smoothSmemBytes<CoarseRows>(B.maxLine, B.tile));
     cfg.stream = s;
     cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = cl;
+    at[0].val.clusterDim.x = TAIL_MAX_CTAS;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
     at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;

@@ -158,7 +158,7 @@ class GpuSolver:
         check("btd_set_pcg_flexible", self._h, int(bool(on)))
 
     def set_vcycle_tail(self, on=True):
-        """The V-cycle's bottom two levels in one cluster launch (default) or a launch a colour pass."""
+        """The V-cycle's bottom two levels in one cluster launch, or a launch a colour pass (default)."""
         check("btd_set_vcycle_tail", self._h, int(bool(on)))
 
     def set_pcg(self, max_iterations, rel_tol=0.0):
