@@ -759,7 +759,9 @@ def main():
     bytes_sweep = 2.0 * N * (R0 + 36.0)
     achieved = bytes_sweep / (ms_sweep / 1e3) / 1e9
     ms_mv = gpu.profile_stage("matvec", reps=10, flush=True)
-    mv_gbs = N * (R0 + 24.0) / (ms_mv / 1e3) / 1e9
+    # PCG's matvec reads the FP64 rows (58 doubles a node), p and the fixed flag, and writes Ap
+    R64 = 464.0
+    mv_gbs = N * (R64 + 16.0 + 4.0 + 16.0) / (ms_mv / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
@@ -837,7 +839,8 @@ def main():
         "roofline": {"kernel": "k_smooth<FineRows> (fine yarn-line sweep, 6 colour launches)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind, "algorithmic_bytes_per_sweep": bytes_sweep, "ms_per_sweep": ms_sweep,
-                     "matvec_gbs": mv_gbs, "matvec_ms": ms_mv},
+                     "matvec_gbs": mv_gbs, "matvec_ms": ms_mv, "matvec_frac": mv_gbs / peak,
+                     "matvec_bytes_per_node": R64 + 36.0},
         "clocks": clocks.summary(),
     }
     line["config"]["levels"] = levels
