@@ -34,11 +34,7 @@ def layer_order_kept(x0, x, cell=2e-3, apart=1e-3):
     return worst
 
 
-def test_two_sheets_contact_matches_oracle():
-    """The sheet-on-sheet drop of test_gpu_contact, GPU against the oracle with self-contact: 60
-    substeps within 0.1 of the motion (the free sheet slides on the sagging one under friction near
-    its stick limit, which amplifies rounding differences laterally), and the resting gap between
-    the sheets the same to 0.1 mm."""
+def two_sheets():
     m = btd.material_preset(0)
     sc = btd.compile_scene([btd.layer_spec(m, 0.15, 0.15, bundle=(9, 6), z=z, seed=3) for z in (0.0, 0.004)])
     L0 = sc.layers[0]
@@ -59,12 +55,28 @@ def test_two_sheets_contact_matches_oracle():
     assert len(start) == 2 and len(nodes) == sc.N - n
     cpu.set_pieces(piece_of, start, nodes)
     gpu.set_pieces(piece_of, start, nodes)
+    return sc, cpu, gpu, x0, (nx, ny, n)
+
+
+def test_two_sheets_contact_matches_oracle():
+    """The sheet-on-sheet drop of test_gpu_contact, GPU against the oracle with self-contact. The free
+    sheet slides on the sagging one under friction near its stick limit, which amplifies rounding
+    differences laterally, so the trajectory is compared substep by substep (each from the oracle's
+    state rounded to float32: the largest node error over the substep's largest displacement, median
+    under 5 %), and the free runs' resting gaps between the sheets after 60 substeps agree to 0.1 mm."""
+    sc, cpu, gpu, x0, (nx, ny, n) = two_sheets()
+    errs = []
+    for _ in range(60):
+        xs, _ = copy_state(cpu, gpu)
+        cpu.substep()
+        gpu.substep()
+        errs.append(np.abs(gpu.x.astype(np.float64) - cpu.x).max() / max(np.abs(cpu.x - xs).max(), 1e-12))
+    assert np.median(errs) < 0.05, np.round(errs, 4).tolist()
+    sc, cpu, gpu, x0, (nx, ny, n) = two_sheets()
     for _ in range(60):
         cpu.substep()
         gpu.substep()
     xc, xg = cpu.x, gpu.x.astype(np.float64)
-    moved = np.abs(xc - x0).max()
-    assert np.abs(xg - xc).max() < 0.1 * moved, (np.abs(xg - xc).max(), moved)
     gc = (xc[n:, 2] - xc[:n, 2]).reshape(ny, nx)[2:-2, 2:-2]
     gg = (xg[n:, 2] - xg[:n, 2]).reshape(ny, nx)[2:-2, 2:-2]
     assert gc.min() > HARD_CORE and gg.min() > HARD_CORE, (gc.min(), gg.min())

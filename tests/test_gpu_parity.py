@@ -183,10 +183,13 @@ def config0_pair():
 def test_config0_each_step_within_1e5_relative():
     """The plain benchmark configuration (64 x 64, dt 1/60, 4 Newton, PCG to rel-res 1e-6): from the
     same state, each of the 60 steps lands near the oracle's positions (max |x_gpu - x_cpu| /
-    max |x_cpu|, the states re-synchronised before every step). The stated bound, 1e-5 relative,
-    holds for the median step; the worst steps reach ~1e-4 (the FP32 arithmetic floor of the
-    gradient and operator: tightening the PCG stop on both sides to 1e-9 does not lower it, and the
-    oracle itself moves by 8.6e-5 between stops of 1e-6 and 1e-10), bounded here at 3e-4."""
+    max |x_cpu|, the states re-synchronised before every step). The stated bound, 1e-5 relative, holds
+    for the median step (4.4e-7 on a B200 with the FP64 operator, 3.1e-6 with the FP32 one) and for 90 %
+    of the steps; the few worst steps reach 1.0e-4 whatever the precision of the right-hand side, of the
+    operator or of the PCG stop: their Newton iterates cross the laws' kinks (the J-curve's tangent
+    switch, the projections' max(K, 0) and max(f, 0)), where the small difference the PCG tolerance seeds
+    in the first Newton iteration changes the next operator discontinuously and grows over the later
+    iterations (traced stage by stage). Bounded here at 2e-4."""
     cfg, sc, cpu, gpu = config0_pair()
     errs = []
     for _ in range(cfg["steps"]):
@@ -195,8 +198,10 @@ def test_config0_each_step_within_1e5_relative():
         gpu.substep()
         xc = cpu.x
         errs.append(np.abs(gpu.x.astype(np.float64) - xc).max() / np.abs(xc).max())
+    errs = np.array(errs)
     assert np.median(errs) < 1e-5, np.median(errs)
-    assert max(errs) < 3e-4, max(errs)
+    assert (errs > 1e-5).mean() <= 0.1, np.round(errs, 8).tolist()
+    assert errs.max() < 2e-4, errs.max()
 
 
 def test_config0_free_trajectory():
@@ -236,8 +241,10 @@ def test_config0_rebuilt_deep_hierarchy():
         xc = cpu.x
         errs.append(np.abs(gpu.x.astype(np.float64) - xc).max() / np.abs(xc).max())
     assert gpu.level_count() == cpu.level_count() == 5
+    errs = np.array(errs)
     assert np.median(errs) < 1e-5, np.median(errs)
-    assert max(errs) < 3e-4, max(errs)
+    assert (errs > 1e-5).mean() <= 0.1, np.round(errs, 8).tolist()
+    assert errs.max() < 2e-4, errs.max()
     assert abs(its_g - its_c) <= 0.25 * its_c, (its_g, its_c)
     assert its_g / newton < 25, its_g / newton
 
