@@ -126,8 +126,10 @@ def train_network(steps=1500, seed=0, verbose=True):
     1e-6) logs its coarsest operators and residuals on the plain configuration's hanging patch (64 x 64,
     seeds 1 and 3, 6 substeps each), on the yarn-damage configuration (128 x 128 with its two edge grips,
     6 substeps), on eight patches of the batch (4 substeps each, grips moving) and on configuration 4's
-    tearing patch scaled to 64 x 64 (8 substeps); then Adam over minibatches of 6 operators, each
-    configuration weighing the same. Returns (weights, loss history)."""
+    tearing patch scaled to 64 x 64 (8 substeps) and at its full 256 x 256 with another seed of its
+    break strains than the benchmark's (seed 43, 24 substeps: the grips' pull and the start of the
+    tear); then Adam over minibatches of 6 operators, each configuration weighing the same. Returns
+    (weights, loss history)."""
     from . import configs
     from .solver import GpuSolver
 
@@ -179,8 +181,13 @@ def train_network(steps=1500, seed=0, verbose=True):
     log_run(g, 8, edge(g, left, right, c4["grip_speed"], c4["h"], c4["grip_stiffness"]))
     groups.append(("config4", tr.add_log(g, 3)))
     g.close()
+    sc, left, right = configs.config4(43)
+    g = GpuSolver(sc, configs.solver_params(c4["h"], 4, 1e-6, self_contact=1))
+    log_run(g, 24, edge(g, left, right, c4["grip_speed"], c4["h"], c4["grip_stiffness"]))
+    groups.append(("config4-256", tr.add_log(g, 4)))
+    g.close()
     if verbose:
         print("logged:", groups, "operators, calls:", tr.counts(), flush=True)
-    w, hist = tr.train(init_weights(seed), steps=steps, batch_ops=6, lr=3e-3, seed=seed, group_weights=[1, 1, 1, 1])
+    w, hist = tr.train(init_weights(seed), steps=steps, batch_ops=6, lr=3e-3, seed=seed, group_weights=[1, 1, 1, 1, 1])
     tr.close()
     return w, hist
