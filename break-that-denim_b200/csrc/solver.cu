@@ -243,11 +243,12 @@ struct btd_solver {
   float* dLcW = nullptr;       // the flat FP32 weights as given (packed into dNet)
   float* lcPhi = nullptr;      // 3 M x LC_K
   uint8_t* lcCtFlag = nullptr; // per fine node
+  uint8_t* lcBasisFlags = nullptr;  // the coarsest flags of the current learned basis
   std::vector<uint8_t*> lcFlags;  // per level
   LcLog lcLog{};
   bool lcEnabled = false;
   bool lcOn() const { return lcEnabled; }
-  LcArgs lcArgs() const { return LcArgs{dLc, dNet, lcPhi, lcLog}; }
+  LcArgs lcArgs() const { return LcArgs{dLc, dNet, lcPhi, lcLog, lcBasisFlags}; }
   GripSlot* dGripSlots = nullptr;
   GripEntry* dGripEntries = nullptr;
   float4* dGripGoal = nullptr;
@@ -2039,6 +2040,7 @@ static void learnedAlloc(btd_solver* s) {
   s->dLcW = s->alloc<float>(LC_WEIGHTS);
   s->lcPhi = s->alloc<float>((size_t)3 * C.N * LC_K);
   s->lcCtFlag = s->alloc<uint8_t>(s->N);
+  s->lcBasisFlags = s->alloc<uint8_t>(C.N);
   for (const Level& L : s->levels) s->lcFlags.push_back(s->alloc<uint8_t>(L.N));
 }
 
@@ -2066,6 +2068,7 @@ extern "C" int btd_set_learned(btd_solver* s, const float* weights, int32_t coun
       s->sync();
       st.on = on ? 1 : 0;
       st.guard = (float)guard;
+      if (weights) st.basisGen = -1;  // a new network: the next solve builds its basis
       CK(cudaMemcpyAsync(s->dLc, &st, sizeof st, cudaMemcpyHostToDevice, s->stream));
     }
     // the kernels stay in the graphs while logging, so a solver that only logs keeps them too
