@@ -79,3 +79,46 @@ def test_batch_graph_equals_each_patch_alone():
     graph.close()
     for s, _ in batch:
         s.close()
+
+
+def test_batch_patches_match_the_oracle():
+    """Three patches of the batch (their seeded sizes, stiffness factors, yarn regions and grips), run
+    in the batch graph on the GPU and one by one in the oracle from the same float32 state: after 8
+    substeps every patch's positions agree to 1e-3 of its motion. (The grips' lead limit, a GPU-side
+    interaction bound that the reference's CPU grip does not have, is opened here.)"""
+    from helpers import MG
+    from oracle import Oracle
+
+    c = btd.configs.CONFIG3
+    patches = btd.configs.config3(count=3, sides=(24, 48))
+    steps = 8
+    batch = []
+    for sc, g in patches:
+        sv = btd.GpuSolver(sc, btd.configs.solver_params(c["h"], c["newton_iterations"], c["pcg_rel_tol"]))
+        anchor = sv.x[g["picked"]].astype(np.float32)
+        sv.attach_patch(0, g["picked"], g["nodes"], g["weights"], anchor, g["stiffness"], max_lead=1.0)
+        batch.append((sv, anchor))
+    graph = btd.Batch([s for s, _ in batch])
+    try:
+        for k in range(1, steps + 1):
+            for (s, anchor), (_, g) in zip(batch, patches):
+                s.set_target((anchor + k * c["h"] * g["velocity"]).astype(np.float32))
+            graph.run(1)
+        for s, _ in batch:
+            s.synchronize()
+    finally:
+        graph.close()
+    for (s, anchor), (sc, g) in zip(batch, patches):
+        o = Oracle(sc, h=c["h"], newton_iterations=c["newton_iterations"], pcg_iterations=500, pcg_rel_tol=c["pcg_rel_tol"], **MG)
+        x = sc.position.reshape(-1, 3).astype(np.float32).astype(np.float64)
+        o.set_state(x)
+        nodes = np.asarray(g["nodes"])
+        a = anchor.astype(np.float64)
+        o.add_grip(nodes, np.asarray(g["weights"], np.float64), (x[nodes] - x[g["picked"]]).reshape(-1), a, g["stiffness"])
+        for k in range(1, steps + 1):
+            o.set_grip_goal(0, (a + k * c["h"] * g["velocity"]).astype(np.float32).astype(np.float64))
+            o.substep()
+        moved = np.abs(o.x - x).max()
+        err = np.abs(s.x.astype(np.float64) - o.x).max()
+        assert moved > 0 and err < 1e-3 * moved, (sc.N, err, moved)
+        s.close()
