@@ -171,40 +171,74 @@ __global__ void k_ct_face_count(ContactArgs a) {
   if (h.y != CT_NONE) atomicAdd(&a.cells[h.y], 1u);
 }
 
-// Exclusive scan of the T cell counts in place (scan.wgsl): one CTA of 1024 threads, each a run of
-// T / 1024 consecutive slots, the run totals scanned across the block.
-constexpr int CT_SCAN_THREADS = 1024;
-__global__ void __launch_bounds__(CT_SCAN_THREADS) k_ct_scan(unsigned* cells, int T) {
-  __shared__ unsigned warpSum[CT_SCAN_THREADS / 32];
-  const int t = threadIdx.x, per = T / CT_SCAN_THREADS;
-  unsigned* run = cells + (size_t)t * per;
-  unsigned sum = 0;
-  for (int q = 0; q < per; ++q) sum += run[q];
-  // inclusive scan of the run totals: within the warp, then across warps
-  const int lane = t & 31, warp = t >> 5;
-  unsigned v = sum;
+// Exclusive scan of the T cell counts in place (scan.wgsl's result), over the whole GPU in two
+// launches: k_ct_scan_tiles sums each tile of 4,096 cells (a CTA of 1,024 threads, four consecutive
+// cells a thread, so a warp reads 512 contiguous bytes), then k_ct_scan_apply scans each tile with the
+// sum of the tiles before it as its offset. Integer sums: the same result as any order.
+constexpr int CT_SCAN_THREADS = 1024, CT_SCAN_ITEMS = 4, CT_SCAN_TILE = CT_SCAN_THREADS * CT_SCAN_ITEMS;
+constexpr int CT_SCAN_MAX_TILES = (1 << 20) / CT_SCAN_TILE;  // the largest table (cross-layer, 2^20 cells)
+
+// Exclusive scan of v over the CTA; *total gets the CTA's sum.
+__device__ __forceinline__ unsigned ctBlockScan(unsigned v, unsigned* warpSum, unsigned* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned w = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const unsigned u = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o) v += u;
+    const unsigned u = __shfl_up_sync(0xffffffffu, w, o);
+    if (lane >= o) w += u;
   }
-  if (lane == 31) warpSum[warp] = v;
+  if (lane == 31) warpSum[warp] = w;
   __syncthreads();
   if (warp == 0) {
-    unsigned w = warpSum[lane];
+    unsigned x = warpSum[lane];
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const unsigned u = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += u;
+      const unsigned u = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += u;
     }
-    warpSum[lane] = w;
+    warpSum[lane] = x;
   }
   __syncthreads();
-  unsigned off = v - sum + (warp > 0 ? warpSum[warp - 1] : 0u);
-  for (int q = 0; q < per; ++q) {
-    const unsigned c = run[q];
-    run[q] = off;
-    off += c;
+  *total = warpSum[31];
+  return w - v + (warp > 0 ? warpSum[warp - 1] : 0u);
+}
+
+__global__ void __launch_bounds__(CT_SCAN_THREADS) k_ct_scan_tiles(const unsigned* __restrict__ cells, int T, unsigned* __restrict__ tileSum) {
+  __shared__ unsigned warpSum[32];
+  const int base = blockIdx.x * CT_SCAN_TILE + threadIdx.x * CT_SCAN_ITEMS;
+  unsigned v = 0;
+#pragma unroll
+  for (int q = 0; q < CT_SCAN_ITEMS; ++q)
+    if (base + q < T) v += cells[base + q];
+  unsigned total;
+  ctBlockScan(v, warpSum, &total);
+  if (threadIdx.x == 0) tileSum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(CT_SCAN_THREADS) k_ct_scan_apply(unsigned* cells, int T, const unsigned* __restrict__ tileSum) {
+  __shared__ unsigned warpSum[32];
+  __shared__ unsigned tileOff;
+  if (threadIdx.x < 32) {
+    unsigned o = 0;
+    for (int k = threadIdx.x; k < (int)blockIdx.x; k += 32) o += tileSum[k];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) o += __shfl_down_sync(0xffffffffu, o, d);
+    if (threadIdx.x == 0) tileOff = o;
+  }
+  const int base = blockIdx.x * CT_SCAN_TILE + threadIdx.x * CT_SCAN_ITEMS;
+  unsigned c[CT_SCAN_ITEMS], v = 0;
+#pragma unroll
+  for (int q = 0; q < CT_SCAN_ITEMS; ++q) {
+    c[q] = base + q < T ? cells[base + q] : 0u;
+    v += c[q];
+  }
+  unsigned total;
+  unsigned off = ctBlockScan(v, warpSum, &total);  // its barriers also publish tileOff
+  off += tileOff;
+#pragma unroll
+  for (int q = 0; q < CT_SCAN_ITEMS; ++q) {
+    if (base + q < T) cells[base + q] = off;
+    off += c[q];
   }
 }
 

@@ -190,6 +190,7 @@ struct btd_solver {
   // self-contact (selfcontact.ts): hash table, hashed faces, candidates and bound keys, bounds,
   // fixed-point accumulators; allocated when params.self_contact
   unsigned* ctCells = nullptr;
+  unsigned* ctScanTiles = nullptr;  // the contact scan's tile sums
   float4* ctItems = nullptr;
   unsigned* ctPairs = nullptr;
   float4* cmeta = nullptr;
@@ -378,6 +379,14 @@ struct btd_solver {
     k_project_start<<<blocksFor(N, 128), 128, 0, s>>>(stepArgs());
   }
 
+  // The exclusive scan of T cell counts in place (two launches over the GPU).
+  void encScan(cudaStream_t s, unsigned* cells, int T) {
+    const int tiles = (T + CT_SCAN_TILE - 1) / CT_SCAN_TILE;
+    if (tiles > CT_SCAN_MAX_TILES) throw std::logic_error("contact table larger than the scan's tile sums");
+    k_ct_scan_tiles<<<tiles, CT_SCAN_THREADS, 0, s>>>(cells, T, ctScanTiles);
+    k_ct_scan_apply<<<tiles, CT_SCAN_THREADS, 0, s>>>(cells, T, ctScanTiles);
+  }
+
   // SelfContact.encodeClear + encodeDetect (selfcontact.ts:137-152).
   void encDetect(cudaStream_t s) {
     if (xcOn()) {  // contact.ts encodeDetect: count, scan, fill, detect on the (cell, layer) hash
@@ -385,7 +394,7 @@ struct btd_solver {
       const int T = (int)XC_MASK + 1;
       CK(cudaMemsetAsync(xcCells, 0, sizeof(unsigned) * 2 * (size_t)T, s));
       k_xc_count<<<blocksFor(N, 128), 128, 0, s>>>(a);
-      k_ct_scan<<<1, CT_SCAN_THREADS, 0, s>>>(xcCells, T);
+      encScan(s, xcCells, T);
       k_xc_fill<<<blocksFor(N, 128), 128, 0, s>>>(a);
       k_xc_detect<<<blocksFor(N, 128), 128, 0, s>>>(a, nLayers);
       return;
@@ -394,7 +403,7 @@ struct btd_solver {
     const int T = 1 << CT_TABLE_BITS;
     CK(cudaMemsetAsync(ctCells, 0, sizeof(unsigned) * 2 * (size_t)T, s));
     k_ct_face_count<<<blocksFor(N, 128), 128, 0, s>>>(a);
-    k_ct_scan<<<1, CT_SCAN_THREADS, 0, s>>>(ctCells, T);
+    encScan(s, ctCells, T);
     k_ct_face_fill<<<blocksFor(N, 128), 128, 0, s>>>(a);
     k_ct_damage_row<<<blocksFor(N, 128), 128, 0, s>>>(a);
     k_ct_detect<<<blocksFor(N, 128), 128, 0, s>>>(a);
@@ -1038,6 +1047,7 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
     s->ext = s->alloc<float4>(3 * (size_t)N);
     if (prm->self_contact) {
       s->ctCells = s->alloc<unsigned>(2 * ((size_t)1 << CT_TABLE_BITS));
+      s->ctScanTiles = s->alloc<unsigned>(CT_SCAN_MAX_TILES);
       s->ctItems = s->alloc<float4>(4 * (size_t)N);
       s->ctPairs = s->alloc<unsigned>((CT_K + 2) * (size_t)N);
       s->cmeta = s->alloc<float4>(2 * (size_t)N);
@@ -1989,16 +1999,17 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
     // held grips add their lead once per substep and their terms once per Newton iteration; the
     // assembly and every Galerkin product are followed by their level's line factorisation
     const int64_t grips = s->gripsOn() ? 1 : 0;
-    // self-contact adds detection (6 kernels) once per substep and terms + gather per Newton iteration
+    // self-contact adds detection (7 kernels, the scan two of them) once per substep and terms + gather
+    // per Newton iteration
     const int64_t contact = s->contactOn() ? 1 : 0;
     // detached pieces add rotation + frame after the assembly, start (+ the init it replaces) and curves
     const int64_t rigid = s->pieceCount > 0 ? 1 : 0;
-    const int64_t xc = s->xcOn() ? 1 : 0;  // cross-layer contact: terms in one kernel, detection in four
+    const int64_t xc = s->xcOn() ? 1 : 0;  // cross-layer contact: terms in one kernel, detection in five
     // the learned correction adds its flags (fine, then one a coarse level) and basis to every solve
     const int64_t perNewton = 2 + (1 + V + 5) + 1 + 1 + grips + (2 - xc) * contact + 4 * rigid + lc * (L + 1);
     const int64_t hierarchy = 3 * (L - 1);
     const int64_t hierPerSubstep = s->params.lag_coarse ? hierarchy : hierarchy * (newton / std::max(1, substeps));
-    const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips + (6 - 2 * xc) * contact + 2 * rigid;
+    const int64_t perSubstep = 2 + 1 + 5 + s->nLayers + 4 + grips + (7 - 2 * xc) * contact + 2 * rigid;
     // each optional (gated) Newton iteration slot adds its gate kernel, run or not
     const int64_t gates = s->gatedBound(0, 0) - s->unconditional(0);
     *out = (int64_t)substeps * (perSubstep + hierPerSubstep + gates) + (int64_t)newton * perNewton + (int64_t)(pcg - newton) * (V + 5);
