@@ -219,7 +219,6 @@ SIGNATURES = {
     "btd_set_gradient_precision": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_set_operator_precision": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_set_pcg_flexible": ([C.c_void_p, C.c_int32], C.c_int),
-    "btd_set_vcycle_tail": ([C.c_void_p, C.c_int32], C.c_int),
     "btd_set_learned": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_double], C.c_int),
     "btd_learned_stats": ([C.c_void_p, C.c_void_p], C.c_int),
     "btd_learned_basis": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),

@@ -32,7 +32,6 @@
 #include "k_rigid.cuh"
 #include "k_smooth.cuh"
 #include "k_step.cuh"
-#include "k_vtail.cuh"
 
 namespace btd {
 void setError(const std::string& msg);
@@ -175,10 +174,6 @@ struct btd_solver {
   // the fine operator in FP64, the operator PCG solves with (null when the solve takes the fp32 rows)
   double2* op64 = nullptr;
   bool opFp64 = true;
-  // the V-cycle's bottom two levels in one cluster launch (k_vtail) where they qualify; off by default:
-  // measured slower than the launch-per-pass path (whose programmatic dependent launches already overlap
-  // each pass's staging with the previous pass), 0.366 against 0.326 ms a V-cycle at 256 x 256
-  bool tailOn = false;
   float4* zPrev = nullptr;
   Seg* segs = nullptr;
   float *softening = nullptr, *failSite = nullptr, *tails = nullptr, *strain = nullptr, *strength = nullptr;
@@ -502,85 +497,6 @@ struct btd_solver {
     CK(cudaLaunchKernelEx(&cfg, k, args...));
   }
 
-  // The bottom two levels qualify for k_vtail: the upper one coarse, both of a single layer, every colour
-  // of both at most TAIL_MAX_CTAS lines; returns the cluster size (0: not eligible or switched off).
-  int tailCtas() const {
-    const int L = (int)levels.size();
-    if (!tailOn || L < 2 || 15 + 6 * params.coarse_sweeps > TAIL_MAX_PASSES) return 0;
-    int cl = 0;
-    for (int k = L - 2; k < L; ++k) {
-      const Level& v = levels[k];
-      if (v.fine || v.layers.size() != 1) return 0;
-      for (int c = 0; c < 6; ++c) {
-        if (v.geom[c].table) return 0;
-        cl = std::max(cl, v.colourStart[c + 1] - v.colourStart[c]);
-      }
-    }
-    return cl >= 1 && cl <= TAIL_MAX_CTAS ? cl : 0;
-  }
-  TailLevel tailLevel(int k) const {
-    const Level& v = levels[k];
-    TailLevel t;
-    t.L = v.dev();
-    for (int c = 0; c < 6; ++c) {
-      t.geom[c] = v.geom[c];
-      t.count[c] = v.colourStart[c + 1] - v.colourStart[c];
-    }
-    t.fac = v.fac;
-    t.T = v.tile;
-    return t;
-  }
-  void launchTail(cudaStream_t s, int lines, bool down, int from, int to, bool up) {
-    const int L = (int)levels.size();
-    TailArgs a;
-    a.lv[0] = tailLevel(L - 2);
-    a.lv[1] = tailLevel(L - 1);
-    a.passes = 0;
-    auto push = [&](int kind, int lv, int c) {
-      if (a.passes >= TAIL_MAX_PASSES) throw std::logic_error("k_vtail: too many passes");
-      a.kind[a.passes] = (int8_t)kind, a.level[a.passes] = (int8_t)lv, a.colour[a.passes] = (int8_t)c;
-      a.passes++;
-    };
-    auto sweep = [&](int lv, bool reverse) {
-      for (int q = 0; q < 6; ++q) {
-        const int c = reverse ? 5 - q : q;
-        if (a.lv[lv].count[c] > 0) push(TAIL_SWEEP, lv, c);
-      }
-    };
-    if (down) {
-      sweep(0, false);
-      push(TAIL_RESIDUAL, 0, 0);
-      push(TAIL_RESTRICT, 0, 0);
-    }
-    for (int sw = from; sw < to; ++sw) sweep(1, (sw & 1) == 1);
-    if (up) {
-      push(TAIL_PROLONG, 0, 0);
-      sweep(0, true);
-    }
-    a.err = dCounters + CNT_ERROR;
-    const Level& U = levels[L - 2];
-    const Level& B = levels[L - 1];
-    cudaLaunchConfig_t cfg = {};
-    // the transfers run over every thread of the cluster: the widest cluster and CTA (the sweeps
-    // stride by the CTA size and leave the CTAs past a colour's line count idle); `lines` (the most
-    // lines of a colour) only has to fit
-    if (lines > TAIL_MAX_CTAS) throw std::logic_error("k_vtail: more lines a colour than CTAs");
-    cfg.gridDim = dim3(TAIL_MAX_CTAS);
-    cfg.blockDim = dim3(SM_SWEEP_THREADS);
-    cfg.dynamicSmemBytes = std::max(smoothSmemBytes<CoarseRows>(U.maxLine, U.tile), smoothSmemBytes<CoarseRows>(B.maxLine, B.tile));
-    cfg.stream = s;
-    cudaLaunchAttribute at[2];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = TAIL_MAX_CTAS;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[1].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = params.overlap_launches ? 2 : 1;
-    CK(cudaLaunchKernelEx(&cfg, k_vtail, a));
-  }
-
   void encSmooth(cudaStream_t s, int k, bool reverse) {
     Level& L = levels[k];
     const size_t smem = L.fine ? smoothSmemBytes<FineRows>(L.maxLine, L.tile) : smoothSmemBytes<CoarseRows>(L.maxLine, L.tile);
@@ -607,18 +523,6 @@ struct btd_solver {
   // encodeVCycle (solver.ts:584-598): X of level k = V(B) with X zero on entry.
   void encVCycle(cudaStream_t s, int k) {
     int last = (int)levels.size() - 1;
-    const int cl = k == last - 1 ? tailCtas() : 0;
-    if (cl > 0) {  // the bottom two levels in one cluster launch (two around the learned correction)
-      if (lcOn()) {
-        const int half = params.coarse_sweeps / 2;
-        launchTail(s, cl, true, 0, half, false);
-        launch(k_lc_correct, 1, LC_THREADS, 0, s, levels[last].dev(), lcArgs());
-        launchTail(s, cl, false, half, params.coarse_sweeps, true);
-      } else {
-        launchTail(s, cl, true, 0, params.coarse_sweeps, true);
-      }
-      return;
-    }
     if (k == last) {
       if (lcOn()) {
         // the learned coarse space half-way through the coarsest sweeps, which mirror around it
@@ -1182,8 +1086,6 @@ int btd_create(const btd_scene* sc, const btd_params* prm, btd_solver** out) {
         set((const void*)k_smooth<CoarseRows, 1>);
         set((const void*)k_line_factor<FineRows>);
         set((const void*)k_line_factor<CoarseRows>);
-        set((const void*)k_vtail);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_vtail, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         smemErr = e;
       });
       CK(smemErr);
@@ -1547,18 +1449,6 @@ int btd_set_gradient_precision(btd_solver* s, int32_t fp64) {
     s->hostP.gradFp64 = fp64 ? 1 : 0;
     s->pushParams();
     s->sync();
-  });
-}
-
-static void resetGraphs(btd_solver* s);
-
-int btd_set_vcycle_tail(btd_solver* s, int32_t on) {
-  GUARD({
-    checkSolver(s);
-    if ((on != 0) != s->tailOn) {
-      s->tailOn = on != 0;
-      resetGraphs(s);
-    }
   });
 }
 
@@ -1991,9 +1881,6 @@ int btd_launch_count(btd_solver* s, int32_t substeps, int32_t newton, int32_t pc
     const int64_t lc = s->lcOn() ? 1 : 0;
     int64_t V = s->params.coarse_sweeps * colours(L - 1) + lc;
     for (int k = 0; k + 1 < L; ++k) V += 2 * colours(k) + 3;
-    // the bottom two levels in one cluster launch: their colour launches and transfers become one
-    // launch (two around the learned correction)
-    if (s->tailCtas() > 0) V -= s->params.coarse_sweeps * colours(L - 1) + 2 * colours(L - 2) + 3 - (1 + lc);
     // per Newton iteration: assembly, PCG prologue (init + V-cycle + 5), line search, apply; the
     // hierarchy (weights + RAP per coarse level) on the first iteration; V-cycle + 5 per extra PCG pass
     // held grips add their lead once per substep and their terms once per Newton iteration; the

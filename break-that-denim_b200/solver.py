@@ -157,10 +157,6 @@ class GpuSolver:
         """PCG's beta in the flexible (Polak-Ribiere) form, or the reference's form (default)."""
         check("btd_set_pcg_flexible", self._h, int(bool(on)))
 
-    def set_vcycle_tail(self, on=True):
-        """The V-cycle's bottom two levels in one cluster launch, or a launch a colour pass (default)."""
-        check("btd_set_vcycle_tail", self._h, int(bool(on)))
-
     def set_pcg(self, max_iterations, rel_tol=0.0):
         check("btd_set_pcg", self._h, int(max_iterations), float(rel_tol))
 

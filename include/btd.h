@@ -240,15 +240,6 @@ int btd_set_operator_precision(btd_solver* s, int32_t fp64);
  * when the preconditioner is applied inexactly (FP32 V-cycle, learned correction); 0 (default) the
  * reference's form r' . z' / (r . z). */
 int btd_set_pcg_flexible(btd_solver* s, int32_t on);
-/* Extension: the V-cycle's bottom two levels - the level above the coarsest (pre-sweep, residual,
- * restriction, prolongation, post-sweep) and the coarsest level's sweeps - in one launch of a
- * thread-block cluster (one CTA a line, cluster barriers between the passes) where both are single-layer
- * coarse levels of at most 16 lines a colour; 1 on, 0 (default) one launch a colour pass and transfer.
- * The arithmetic is the same either way, bit for bit. Measured on a B200 at 256 x 256 the cluster launch
- * is the slower (0.366 against 0.326 ms a V-cycle): the launches' programmatic dependent launch already
- * overlaps each pass's staging with the previous pass, and a cluster barrier costs about what a
- * launch boundary does. */
-int btd_set_vcycle_tail(btd_solver* s, int32_t on);
 /* Extension: PCG cap and relative-residual stop (0 = fixed count as the reference). */
 int btd_set_pcg(btd_solver* s, int32_t max_iterations, double rel_tol);
 
