@@ -33,3 +33,19 @@ def test_bf16_coupling_blocks_cost_few_iterations():
     print(f"PCG iterations per Newton step: coarse levels FP64 {i32:.2f}, BF16 couplings {i16:.2f}")
     assert r32 <= 1e-6 and r16 <= 1e-6
     assert i16 <= 1.1 * i32
+
+
+def test_fp32_rows_study_modes():
+    """The operator as FP32 storage would hold it (fp32_rows; the study behind PCG's FP64 operator):
+    on the hanging patch (no loose material) every mode still solves each Newton system to rel-res
+    1e-6, and keeping PCG's operator exact while the V-cycle takes FP32-rounded rows (mode 3) changes
+    the iteration count by at most one a Newton step against all-FP64 rows."""
+    sc = configs.hanging_patch(64, 0.3, seed=2)
+    i64, r64 = run(Oracle(sc, **P), 1)
+    out = {}
+    for mode in (1, 2, 3, 11, 13):
+        out[mode] = run(Oracle(sc, **P, fp32_rows=mode), 1)
+    for mode, (i, r) in out.items():
+        assert r <= 1e-6, (mode, r)
+    assert abs(out[3][0] - i64) <= 1.0, (out[3][0], i64)
+    assert abs(out[13][0] - i64) <= 1.0, (out[13][0], i64)
