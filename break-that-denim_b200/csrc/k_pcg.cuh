@@ -253,58 +253,12 @@ __global__ void k_pcg_update_p(PcgArgs a, int first) {
 }
 
 // Ap = A p (fixed rows 0), p . Ap; alpha = rz / pAp (0 and stop when pAp <= 0, as pcg() breaks).
-// Half h of fine row n's FP64 product with x (h 0: the diagonal block and couplings 0-5, h 1: couplings
-// 6-11), summed into y in FP64.
-__device__ __forceinline__ void fine64HalfApply(const PcgArgs& a, int n, int h, const float4* __restrict__ x, double& y0,
-                                                double& y1, double& y2) {
-  const DLevel& F = a.F;
-  int i, j, l;
-  nodeAt(F, n, &i, &j, &l);
-  const DLevelLayer L = layerOf(F, l);
-  if (h == 0) {
-    const float4 xn = x[n];
-    const double q[3] = {xn.x, xn.y, xn.z};
-    symDVecAdd(loadSymD(a.op64, F.N, n, 0), q, y0, y1, y2);
-  }
-#pragma unroll
-  for (int k = 0; k < FineRows::NC; ++k) {
-    if ((k < 6) != (h == 0)) continue;
-    const int2 off = FineRows::offset(k);
-    const int m = levelNode(L, i + off.x, j + off.y);
-    if (m < 0) continue;
-    const float4 xm = x[m];
-    const double q[3] = {xm.x, xm.y, xm.z};
-    symDVecAdd(fine64Block(a.op64, F.N, n, k), q, y0, y1, y2);
-  }
-}
-
 __global__ void __launch_bounds__(RED_THREADS) k_pcg_matvec(PcgArgs a) {
   pdlWait();
   pdlLaunchNext();
   double v[1] = {0.0};
   const DLevel& F = a.F;
-  if (a.op64) {
-    // the FP64 rows: two adjacent lanes a row, each half its blocks (twice the loads in flight), their
-    // sums joined by a shuffle; every lane runs the same number of rounds
-    const int t = blockIdx.x * blockDim.x + threadIdx.x, h = t & 1;
-    const int rows = (gridDim.x * blockDim.x) >> 1;
-    for (int base = 0; base < F.N; base += rows) {
-      const int n = base + (t >> 1);
-      const bool valid = n < F.N;
-      double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-      if (valid) fine64HalfApply(a, n, h, a.p, y0, y1, y2);
-      y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
-      y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
-      y2 += __shfl_xor_sync(0xffffffffu, y2, 1);
-      if (valid && h == 0) {
-        const float3 y = F.fixed[n] ? make_float3(0, 0, 0) : make_float3((float)y0, (float)y1, (float)y2);
-        a.Ap[n] = make_float4(y.x, y.y, y.z, 0.f);
-        const float3 p = f3(a.p[n]);
-        v[0] += (double)y.x * p.x + (double)y.y * p.y + (double)y.z * p.z;
-      }
-    }
-  }
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; !a.op64 && n < F.N; n += gridDim.x * blockDim.x) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < F.N; n += gridDim.x * blockDim.x) {
     // the row's loads do not wait for its fixed flag (a fixed row's product is dropped)
     float3 y = make_float3(0, 0, 0);
     const uint32_t fixedRow = F.fixed[n];
